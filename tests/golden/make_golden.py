@@ -1,0 +1,333 @@
+"""Generate the golden fixtures in this directory by running the REFERENCE's own code.
+
+Run in the development container (the reference tree is not present on GPU boxes):
+
+    python tests/golden/make_golden.py [/path/to/reference]
+
+* 1D: ``src/1D-ERK4(3)IP UPPE gas/erk43ip_method.py`` imported unmodified, with the
+  argon patch applied by importing ``gas.py`` itself (``matplotlib`` and
+  ``visualization`` are stubbed: they are plotting only).
+* 3D: ``src/3+1D-UPPE-ERK4(3)IP-envelope/{solver_3d,media_physics}.py`` imported
+  unmodified through a numpy-backed stand-in for ``cupy``/``cupyx``.  The stand-in's
+  ``RawKernel`` compiles the reference's own CUDA-C plasma kernel source string
+  (``media_physics.py:11-67``) as host C++ with g++ (output under ``oracle/_ref/``)
+  and runs each thread index serially.
+* Plugin substitutions for the 3D medium (the reference's Keldysh LUT is broken
+  and its gas n4 overflows): ``n4 = 0``; the LUT values are either the reference's
+  own ADK rate (``src/THz/2+1D-all field UPPE Argon.py:70-81``, imported through
+  the same stand-in) or a documented MPI-like test table W = W0 (I/I0)^8 that
+  makes the plasma terms non-negligible at test intensities.
+
+Every fixture is a small .npz (fields of at most 16x16x32 / Nt=1024).
+"""
+import ctypes
+import hashlib
+import importlib.util
+import os
+import subprocess
+import sys
+import types
+
+import numpy as np
+import scipy.fft
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+REF_1D = os.path.join(REF, 'src', '1D-ERK4(3)IP UPPE gas')
+REF_3D = os.path.join(REF, 'src', '3+1D-UPPE-ERK4(3)IP-envelope')
+REF_THZ = os.path.join(REF, 'src', 'THz', '2+1D-all field UPPE Argon.py')
+REF_BUILD = os.path.join(REPO, 'oracle', '_ref')
+
+
+# ---------------------------------------------------------------------------
+# numpy-backed stand-ins
+# ---------------------------------------------------------------------------
+_PRELUDE = r'''
+#include <math.h>
+struct _uppe_dim3 { unsigned x, y, z; };
+static _uppe_dim3 blockDim, blockIdx, threadIdx;
+#define __global__
+'''
+
+_LAUNCHER = r'''
+extern "C" void _launch_plasma_integration_kernel(unsigned grid, unsigned block,
+    const float* W_ion, const float* W_ava, double* rho, double* gen,
+    float rate_rec, float dt, float rho_nt, int Nt, int nsp) {
+  blockDim.x = block; blockDim.y = blockDim.z = 1;
+  for (unsigned b = 0; b < grid; ++b) {
+    blockIdx.x = b;
+    for (unsigned t = 0; t < block; ++t) {
+      threadIdx.x = t;
+      plasma_integration_kernel(W_ion, W_ava, rho, gen, rate_rec, dt, rho_nt, Nt, nsp);
+    }
+  }
+}
+'''
+
+
+class _HostRawKernel:
+    """cp.RawKernel stand-in: compiles the reference's kernel source with g++."""
+
+    def __init__(self, code, name):
+        assert name == 'plasma_integration_kernel', name
+        os.makedirs(REF_BUILD, exist_ok=True)
+        src = _PRELUDE + code + _LAUNCHER
+        tag = hashlib.sha1(src.encode()).hexdigest()[:12]
+        cpp = os.path.join(REF_BUILD, f'plasma_kernel_{tag}.cpp')
+        so = os.path.join(REF_BUILD, f'plasma_kernel_{tag}.so')
+        if not os.path.exists(so):
+            with open(cpp, 'w') as f:
+                f.write(src)
+            subprocess.check_call(['g++', '-O2', '-fPIC', '-shared', '-o', so, cpp])
+        lib = ctypes.CDLL(so)
+        fn = lib._launch_plasma_integration_kernel
+        P = ctypes.c_void_p
+        fn.argtypes = [ctypes.c_uint, ctypes.c_uint, P, P, P, P, ctypes.c_float,
+                       ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int]
+        self._fn = fn
+
+    def __call__(self, grid, block, args):
+        W_ion, W_ava, rho, gen, rr, dt, rnt, Nt, nsp = args
+        for a in (W_ion, W_ava, rho, gen):
+            assert a.flags['C_CONTIGUOUS']
+        assert W_ion.dtype == np.float32 and W_ava.dtype == np.float32
+        assert rho.dtype == np.float64 and gen.dtype == np.float64
+        self._fn(int(grid[0]), int(block[0]), W_ion.ctypes.data, W_ava.ctypes.data,
+                 rho.ctypes.data, gen.ctypes.data, float(rr), float(dt), float(rnt),
+                 int(Nt), int(nsp))
+
+
+class _Pool:
+    def free_all_blocks(self):
+        pass
+
+
+def install_stand_ins():
+    cp = types.ModuleType('cupy')
+    for k in dir(np):
+        if not k.startswith('__'):
+            setattr(cp, k, getattr(np, k))
+    cp.RawKernel = _HostRawKernel
+    cp.asnumpy = np.asarray
+    cp.get_default_memory_pool = lambda: _Pool()
+    cp_fft = types.ModuleType('cupy.fft')
+    for k in dir(np.fft):
+        if not k.startswith('__'):
+            setattr(cp_fft, k, getattr(np.fft, k))
+    cp.fft = cp_fft
+    cx = types.ModuleType('cupyx')
+    cxs = types.ModuleType('cupyx.scipy')
+    cxf = types.ModuleType('cupyx.scipy.fft')
+    for k in dir(scipy.fft):
+        if not k.startswith('__'):
+            setattr(cxf, k, getattr(scipy.fft, k))
+    cx.scipy, cxs.fft = cxs, cxf
+    mpl = types.ModuleType('matplotlib')
+    plt = types.ModuleType('matplotlib.pyplot')
+    mpl.pyplot = plt
+    vis = types.ModuleType('visualization')
+    sys.modules.update({'cupy': cp, 'cupy.fft': cp_fft, 'cupyx': cx, 'cupyx.scipy': cxs,
+                        'cupyx.scipy.fft': cxf, 'matplotlib': mpl, 'matplotlib.pyplot': plt,
+                        'visualization': vis})
+
+
+def load(path, name):
+    spec = importlib.util.spec_from_file_location(name, path)
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules[name] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def save(name, **arrays):
+    path = os.path.join(HERE, name + '.npz')
+    np.savez_compressed(path, **arrays)
+    print(f'  wrote {name}.npz ({os.path.getsize(path) / 1024:.1f} KiB)')
+
+
+def log_attempts(solver, method_name, record, h_index):
+    """Wrap solver.<method> so every attempt's (h, err) is recorded (no change to results)."""
+    inner = getattr(solver, method_name)
+
+    def wrapped(*args, **kwargs):
+        out = inner(*args, **kwargs)
+        record.append((float(args[h_index]), float(out[1])))
+        return out
+    setattr(solver, method_name, wrapped)
+
+
+# ---------------------------------------------------------------------------
+# 1D fixtures
+# ---------------------------------------------------------------------------
+def make_1d():
+    sys.path.insert(0, REF_1D)
+    erk = load(os.path.join(REF_1D, 'erk43ip_method.py'), 'erk43ip_method')
+    load(os.path.join(REF_1D, 'gas.py'), 'ref_gas')        # applies the argon patch
+    UPPE = erk.ERK43IP_UPPE
+
+    # (a) argon capillary, config-0 medium with a reduced grid and length
+    lam = 800e-9
+    Nt = 1024
+    t = np.linspace(-0.5e-12, 0.5e-12, Nt)
+    kw = dict(material='argon_gas', n2=1.0e-23, beam_radius=0.65 * 125e-6,
+              center_wavelength=lam, alpha=0.5 * np.log(10) / 10, use_raman=False,
+              use_self_steepening=True, gas_P=101325.0, gas_T=293.15)
+    s = UPPE(**kw)
+    fwhm = 30e-15
+    E = 2e9 * fwhm * np.sqrt(np.pi / (4 * np.log(2)))
+    A0 = s.generate_gaussian_pulse(t, E, fwhm)
+    rec = []
+    log_attempts(s, 'erk43_step', rec, 2)
+    zh, Ah, om = s.propagate(A0, t, L=0.3, tol=1e-6)
+    omega = 2 * np.pi * scipy.fft.fftfreq(Nt, t[1] - t[0])
+    D = s._cached_D
+    save('ref1d_argon', t=t, A0=A0, z_hist=zh, A_final=Ah[-1], A_hist_sel=Ah[::max(1, len(Ah) // 8)],
+         n_hist=len(zh), attempts=np.array(rec), D=D, n_omega=s._cached_n_omega, n0=s.n0,
+         gamma=s.gamma, omega=omega, L=0.3, tol=1e-6)
+
+    # (b) fused silica, Raman + self-steepening on (the reference defaults)
+    lam = 1064e-9
+    Nt = 512
+    t = np.linspace(-1.0e-12, 1.0e-12, Nt)
+    s = UPPE(material='fused_silica', n2=2.6e-20, beam_radius=30e-6, center_wavelength=lam)
+    A0 = s.generate_gaussian_pulse(t, 20e-9, 100e-15)
+    rec = []
+    log_attempts(s, 'erk43_step', rec, 2)
+    zh, Ah, om = s.propagate(A0, t, L=0.02, tol=1e-6)
+    att = np.array(rec)
+    # unit-level vectors of the same solver
+    rng = np.random.Generator(np.random.PCG64(11))
+    Ar = A0 * (1 + 0.05 * rng.standard_normal(Nt)) + 1j * 0.05 * np.abs(A0) * rng.standard_normal(Nt)
+    N_A = s.nonlinear_operator(Ar, om)
+    L_A = s.linear_operator(Ar, om, 1.3e-4)
+    A4, err, a5 = s.erk43_step(Ar, om, 7e-4)
+    save('ref1d_silica_raman', t=t, A0=A0, z_hist=zh, A_final=Ah[-1], n_hist=len(zh),
+         attempts=att, D=s._cached_D, n_omega=s._cached_n_omega,
+         H_R=s._cached_raman_response, n0=s.n0, gamma=s.gamma, L=0.02, tol=1e-6,
+         A_rand=Ar, N_A=N_A, L_A=L_A, h_L=1.3e-4, step_h=7e-4, step_A4=A4, step_err=err,
+         step_a5=a5)
+
+    # (c) pure SPM: dispersion forced to zero as in src/1D-ERK4(3)IP UPPE/test_3d-1d.py:52-61
+    lam = 800e-9
+    Nt = 256
+    t = np.linspace(-0.5e-12, 0.5e-12, Nt)
+    s = UPPE(material='fused_silica', n2=2.6e-20, beam_radius=50e-6, center_wavelength=lam,
+             use_raman=False, use_self_steepening=False)
+    s._compute_dispersion_operator = lambda omega_grid: np.zeros_like(omega_grid, dtype=complex)
+    s._cached_D = None
+    A0 = s.generate_gaussian_pulse(t, 5e-9, 80e-15)
+    rec = []
+    log_attempts(s, 'erk43_step', rec, 2)
+    zh, Ah, om = s.propagate(A0, t, L=0.05, tol=1e-7)
+    save('ref1d_spm', t=t, A0=A0, z_hist=zh, A_final=Ah[-1], n_hist=len(zh),
+         attempts=np.array(rec), gamma=s.gamma, L=0.05, tol=1e-7)
+    sys.path.remove(REF_1D)
+
+
+# ---------------------------------------------------------------------------
+# 3D fixtures
+# ---------------------------------------------------------------------------
+def mpi_lut(log10_I, W0=3e9, I0=5e16, K=8):
+    """Test LUT: W = W0 (I/I0)^K (documented substitution)."""
+    return W0 * (10.0 ** log10_I / I0) ** K
+
+
+def make_3d():
+    sys.path.insert(0, REF_3D)
+    media = load(os.path.join(REF_3D, 'media_physics.py'), 'media_physics')
+    solver_mod = load(os.path.join(REF_3D, 'solver_3d.py'), 'solver_3d')
+    thz = load(REF_THZ, 'ref_thz_argon')
+    adk = thz.ADK_Ionization_Argon(64)
+    c0 = 299792458.0
+    eps0 = 8.85418781e-12
+
+    class TestArgon(media.Argon):
+        """Argon with n4 = 0, the ionisation LUT values substituted and an optional
+        Taylor refractive index."""
+
+        def __init__(self, lam, precision, use_shock, lut='adk', taylor=None):
+            super().__init__(lam, 1.0, precision, use_shock)
+            self.n4 = 0.0
+            if lut == 'adk':
+                E = np.sqrt(2 * self.I_grid_cpu / (c0 * eps0 * self.n0))
+                W = adk.calculate_total_rate(E)
+            else:
+                W = mpi_lut(self.log10_I_cpu)
+            self.W_cpu = W
+            self.W_gpu = np.asarray(W, dtype=self.float_dtype)
+            self.taylor = taylor
+
+        def refractive_index(self, omega_array):
+            if self.taylor is None:
+                return super().refractive_index(omega_array)
+            n0, b2, b3 = self.taylor
+            om = omega_array.astype(np.float64)
+            omega_safe = np.where(np.abs(om) < 1e-12, 1e-12, om)
+            W = om - self.omega0
+            return n0 + self.c * (0.5 * b2 * W ** 2 + (1.0 / 6.0) * b3 * W ** 3) / omega_safe
+
+    def grids(N=16, Nt=32, half=1.5e-3, T=200e-15):
+        x = np.linspace(-half, half, N)
+        t = np.linspace(-T / 2, T / 2, Nt)
+        return x, x.copy(), t
+
+    def beam(x, y, t, w0, I_peak, fwhm):
+        X, Y = np.meshgrid(x, y, indexing='ij')
+        T0 = fwhm / (2 * np.sqrt(np.log(2)))
+        A = np.exp(-(X ** 2 + Y ** 2) / w0 ** 2)[:, :, None] * np.exp(-(t / T0) ** 2 / 2)[None, None, :]
+        return (np.sqrt(I_peak) * A).astype(np.complex128)
+
+    lam = 800e-9
+    rng = np.random.Generator(np.random.PCG64(5))
+
+    # unit vectors: the plasma kernel itself (incl. clamping at rho_nt)
+    nl, Nt = 24, 64
+    W_ion = (10 ** rng.uniform(8, 16.5, size=(nl, Nt))).astype(np.float32)
+    W_ion[:8] = (10 ** rng.uniform(6, 11, size=(8, Nt))).astype(np.float32)
+    W_ava = np.zeros_like(W_ion)
+    W_ava[20:] = (10 ** rng.uniform(10, 13, size=(4, Nt))).astype(np.float32)
+    rho = np.zeros((nl, Nt)); gen = np.zeros((nl, Nt))
+    kern = _HostRawKernel(media.PLASMA_KERNEL_CODE, 'plasma_integration_kernel')
+    kern((1,), (256,), (W_ion, W_ava, rho, gen, np.float32(1e9), np.float32(6.45e-15),
+                        np.float32(2.45e25), np.int32(Nt), np.int32(nl)))
+    save('ref_plasma_kernel', W_ion=W_ion, W_ava=W_ava, rho=rho, gen=gen, rate_rec=1e9,
+         dt=6.45e-15, rho_nt=2.45e25)
+
+    cases = [
+        # name, precision, shock, lut, taylor, I_peak, L, tol
+        ('ref3d_adk_taylor_double', 'double', True, 'adk', (1.000283, 20e-30, 0.0), 5e16, 0.05, 1e-5),
+        ('ref3d_mpi_cauchy_double', 'double', True, 'mpi', None, 5e16, 0.03, 1e-5),
+        ('ref3d_mpi_cauchy_single', 'single', True, 'mpi', None, 5e16, 0.03, 1e-4),
+        ('ref3d_noshock_double', 'double', False, 'mpi', None, 4e16, 0.02, 1e-5),
+    ]
+    for name, prec, shock, lut, taylor, Ipk, L, tol in cases:
+        x, y, t = grids()
+        med = TestArgon(lam, prec, shock, lut=lut, taylor=taylor)
+        sol = solver_mod.ERK43IP_UPPE_3D_Optimized(x, y, t, med, precision=prec)
+        A0 = beam(x, y, t, 0.5e-3, Ipk, 40e-15)
+        A0 = A0 * (1 + 0.01 * rng.standard_normal(A0.shape[:2]))[:, :, None]
+        A0 = A0.astype(sol.complex_dtype)
+        # unit: one nonlinear response and one attempt from the normalised field
+        sol.A_scale = float(np.max(np.abs(A0)))
+        An = (A0 / sol.complex_dtype(sol.A_scale + 0.0j)).astype(sol.complex_dtype)
+        Kerr, Plasma = med.calc_nonlinear_response(A0, sol.dt)
+        A4_t, err = sol.erk43_step(An, 2e-3, tol)
+        rec = []
+        log_attempts(sol, 'erk43_step', rec, 1)
+        z, freq, A_w = sol.propagate(A0, L, tol=tol, max_step=1e-2, min_step=1e-9)
+        save(name, x=x, y=y, t=t, A0=A0, lam=lam, precision=prec, shock=shock, lut=lut,
+             taylor=np.array(taylor if taylor else (0, 0, 0), dtype=float),
+             W_lut=np.asarray(med.W_cpu, dtype=np.float64), log10_I=med.log10_I_cpu,
+             Kerr=Kerr, Plasma=Plasma, step_h=2e-3, step_A4_t=A4_t, step_err=err,
+             A_scale=sol.A_scale, z=z, freq=freq, A_w=A_w, attempts=np.array(rec), L=L, tol=tol,
+             D=sol.D_operator)
+    sys.path.remove(REF_3D)
+
+
+if __name__ == '__main__':
+    install_stand_ins()
+    print('1D fixtures from', REF_1D)
+    make_1d()
+    print('3D fixtures from', REF_3D)
+    make_3d()
