@@ -1,0 +1,360 @@
+"""Benchmark of the 3+1D envelope ERK4(3)-IP UPPE step (one JSON line on rank 0).
+
+Workload: 256 x 256 x 512 grid (6 mm x 6 mm x 400 fs), collimated Gaussian beam
+(w0 = 1 mm, 800 nm, 40 fs FWHM, 2 mJ) with seeded 1 % amplitude speckle, argon at
+1 bar (n2 = 1e-23 m^2/W, GVD 20 fs^2/m, ADK ionisation, plasma defocusing and
+loss, self-steepening), L = 2 m, tol = 1e-5; mixed precision by default.
+
+A "step" is one ERK4(3) attempt of the adaptive propagation starting at z = 0,
+with acceptance and step-size control on the device (one CUDA-graph launch per
+attempt).  value = grid points x attempts x ranks / (max over ranks of the
+CUDA-event time of the timed attempts).  Every field (268 MB in complex64) is
+larger than the 126 MB L2, so no L2 flush is inserted.
+
+--impl reference times the CPU oracle port of the reference's algorithm on the
+host cores (rank 0 only) on a bounded sample of the same workload.
+"""
+import argparse
+import ctypes
+import json
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "3+1D UPPE pt-steps/s & batched-1D sims/s vs plain GPU at relL2<=1e-4; % HBM"
+NX = NY = 256
+NT = 512
+LAM = 800e-9
+FWHM = 40e-15
+ENERGY = 2e-3
+W0 = 1e-3
+L_PROP = 2.0
+TOL = 1e-5
+SAMPLE_N = 128       # CPU sample: 128 x 128 x 512
+
+
+def grids(n=NX, nt=NT):
+    x = np.linspace(-3e-3, 3e-3, n)
+    t = np.linspace(-200e-15, 200e-15, nt)
+    return x, x.copy(), t
+
+
+def argon_medium(precision, oracle=False):
+    """Argon 1 bar, Taylor GVD 20 fs^2/m about the Cauchy index at 800 nm."""
+    if oracle:
+        from oracle import uppe3d
+        m0 = uppe3d.argon(LAM, 1.0, precision, True)
+        n0 = float(m0.refractive_index(np.array([m0.omega0]))[0])
+        return uppe3d.argon(LAM, 1.0, precision, True, dispersion=('taylor', n0, 20e-30, 0.0))
+    from project_b200.media import Argon
+    m0 = Argon(LAM, 1.0, precision, True)
+    n0 = float(m0.refractive_index(np.array([m0.omega0]))[0])
+    return Argon(LAM, 1.0, precision, True, dispersion=('taylor', n0, 20e-30, 0.0))
+
+
+def make_input(x, y, t, dtype=np.complex64):
+    from project_b200.pulses import gaussian_beam, speckle
+    A = gaussian_beam(x, y, t, W0, ENERGY, FWHM, dtype=np.complex128)
+    A *= speckle(x, y, 50e-6, 0.01, seed=1)[:, :, None]
+    return A.astype(dtype)
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            return float(json.load(f)['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    Q = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+         'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+         'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = os.path.join('/tmp', f'uppe_clocks_{os.getpid()}.csv')
+
+    def start(self):
+        try:
+            self.f = open(self.path, 'w')
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), f'--query-gpu={self.Q}',
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        self.proc.wait()
+        self.f.close()
+        sm, smax, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            p = [v.strip() for v in line.split(',')]
+            if len(p) < 9:
+                continue
+            try:
+                sm.append(float(p[1]))
+                smax = float(p[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, p[5:9]):
+                if v.lower() == 'active':
+                    reasons.add(n)
+        os.unlink(self.path)
+        return {'sm_mhz': float(np.median(sm)) if sm else None, 'sm_max_mhz': smax,
+                'reasons': sorted(reasons), 'samples': len(sm)}
+
+
+def cpu_baseline(precision='single'):
+    """Oracle port (the reference algorithm on numpy/scipy) on a bounded sample:
+    one ERK attempt on a 128 x 128 x 512 grid, scipy.fft using every host core."""
+    import scipy.fft
+    from oracle import uppe3d
+    cores = len(os.sched_getaffinity(0))
+    x, y, t = grids(SAMPLE_N, NT)
+    med = argon_medium(precision, oracle=True)
+    sol = uppe3d.Solver3D(x, y, t, med, precision)
+    A0 = make_input(x, y, t, np.complex64 if precision == 'single' else np.complex128)
+    sol.A_scale = float(np.max(np.abs(A0)))
+    A = (A0 / sol.A_scale).astype(sol.complex_dtype)
+    with scipy.fft.set_workers(cores):
+        t0 = time.perf_counter()
+        sol.erk43_step(A, 2e-3)
+        dt = time.perf_counter() - t0
+    pts = SAMPLE_N * SAMPLE_N * NT
+    return {'value': pts / dt, 'unit': 'pt-steps/s', 'cores': cores, 'kind': 'port',
+            'sample': f'one ERK attempt on {SAMPLE_N}x{SAMPLE_N}x{NT} (c64, numpy/scipy, '
+                      f'{cores} FFT workers): {dt:.2f} s'}
+
+
+def run_reference(args, rank):
+    if rank != 0:
+        return 0
+    import scipy.fft
+    from oracle import uppe3d
+    cores = len(os.sched_getaffinity(0))
+    x, y, t = grids(SAMPLE_N, NT)
+    med = argon_medium('single', oracle=True)
+    sol = uppe3d.Solver3D(x, y, t, med, 'single')
+    A0 = make_input(x, y, t, np.complex64)
+    sol.A_scale = float(np.max(np.abs(A0)))
+    A = (A0 / sol.A_scale).astype(sol.complex_dtype)
+    pts = SAMPLE_N * SAMPLE_N * NT
+    with scipy.fft.set_workers(cores):
+        for _ in range(args.warmup):
+            sol.erk43_step(A, 2e-3)
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            A4, err, _, _ = sol.erk43_step(A, 2e-3)
+        dt = time.perf_counter() - t0
+    v = pts * args.steps / dt
+    sample = (f'{args.steps} ERK attempts on {SAMPLE_N}x{SAMPLE_N}x{NT} (c64, oracle port of '
+              f'solver_3d.py:100-160 + media_physics.py, {cores} FFT workers)')
+    print(json.dumps({
+        'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'pt-steps/s',
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+        'ms_per_step': 1e3 * dt / args.steps, 'higher_is_better': True, 'scaling': 'weak',
+        'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic',
+        'config': {'workload': '3+1D UPPE envelope ERK4(3)-IP, argon 1 bar, bounded CPU sample',
+                   'grid': [SAMPLE_N, SAMPLE_N, NT]},
+        'cpu_baseline': {'value': v, 'unit': 'pt-steps/s', 'cores': cores, 'kind': 'port',
+                         'sample': sample},
+        'e2e': {'value': v, 'unit': 'pt-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+    }), flush=True)
+    return 0
+
+
+def profile_kernels(sol, lib, n_attempts=3):
+    """Per-launch CUDA-event times of whole attempts -> per-kernel totals."""
+    import torch
+    from project_b200 import _lib
+    cap = 64
+    ms = (ctypes.c_float * cap)()
+    kind = (ctypes.c_int * cap)()
+    byts = (ctypes.c_double * cap)()
+    n = ctypes.c_int()
+    agg = {}
+    for _ in range(n_attempts):
+        _lib.check(lib.uppe3d_profile_attempt(sol._plan, cap, ms, kind, byts, ctypes.byref(n),
+                                              _lib.stream_ptr()), 'uppe3d_profile_attempt')
+        for i in range(n.value):
+            if byts[i] == 0:
+                continue
+            name = {0: 'k_tpass', 1: 'k_space', 2: 'k_space'}.get(kind[i], 'scalar')
+            a = agg.setdefault(name, [0.0, 0.0, 0])
+            a[0] += ms[i]
+            a[1] += byts[i]
+            a[2] += 1
+    torch.cuda.synchronize()
+    return agg
+
+
+def run_b200(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from project_b200 import _lib
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    dev = torch.device('cuda', local_rank)
+    torch.cuda.set_device(dev)
+    x, y, t = grids()
+    prec = args.precision
+    cdt = np.complex64 if prec == 'single' else np.complex128
+    A0 = make_input(x, y, t, cdt)
+    med = argon_medium(prec)
+    sol = ERK43IP_UPPE_3D_Optimized(x, y, t, med, precision=prec, device=dev)
+    lib = sol._lib
+    A_dev = torch.from_numpy(A0).to(dev)
+    sol.set_field(A_dev)
+    s = _lib.stream_ptr()
+    _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'begin')
+    _lib.check(lib.uppe3d_run_steps(sol._plan, args.warmup, s), 'warmup')
+    torch.cuda.synchronize()
+    r0 = sol.result()
+    if world > 1:
+        dist.barrier()
+    clocks = ClockSampler(local_rank)
+    clocks.start()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    ev0.record()
+    _lib.check(lib.uppe3d_run_steps(sol._plan, args.steps, s), 'run_steps')
+    ev1.record()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    clk = clocks.stop()
+    ms = ev0.elapsed_time(ev1)
+    r1 = sol.result()
+    attempts = r1.attempts - r0.attempts
+    accepted = r1.accepted - r0.accepted
+    ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
+    ms_max = float(ms_t.item())
+    npts = NX * NY * NT
+    value = npts * args.steps * world / (ms_max / 1e3)
+
+    # per-kernel roofline (CUDA events around each launch of whole attempts)
+    agg = profile_kernels(sol, lib)
+    peak, peak_kind = peaks()
+    dom = max((k for k in agg if k != 'scalar'), key=lambda k: agg[k][0])
+    d_ms, d_bytes, d_n = agg[dom]
+    achieved = d_bytes / (d_ms / 1e3) / 1e9
+    step_bytes = 64.0 * (8 if prec == 'single' else 16) * npts     # 64 s N per attempt
+    step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
+
+    # e2e: public API call with host buffers (pinned), copies inside the timed region
+    e2e_attempts = 8
+    A_host = torch.from_numpy(A0).pin_memory()
+    out_host = torch.empty(A_host.shape, dtype=A_host.dtype).pin_memory()
+    sol.propagate(A_host, L_PROP, tol=TOL, max_attempts=e2e_attempts, out=out_host)  # warm
+    torch.cuda.synchronize()
+    reps = 3
+    t0 = time.perf_counter()
+    done = 0
+    for _ in range(reps):
+        sol.propagate(A_host, L_PROP, tol=TOL, max_attempts=e2e_attempts, out=out_host)
+        done += sol.last_result.attempts
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    e2e_t = torch.tensor([e2e_s], device=dev, dtype=torch.float64)
+    if world > 1:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_v = npts * done * world / float(e2e_t.item())
+    fbytes = A0.nbytes
+
+    plain = None
+    if rank == 0 and not args.no_plain_gpu:
+        try:
+            from baseline import plain_gpu
+            plain = plain_gpu.time_step(x, y, t, A0.astype(np.complex128), argon_medium('double'),
+                                        dev)
+        except Exception as e:   # reported, never fatal
+            plain = {'error': str(e)[:200]}
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = cpu_baseline(prec)
+
+    if rank == 0:
+        line = {
+            'metric': METRIC, 'value': value, 'unit': 'pt-steps/s', 'n_gpus': world,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max / args.steps,
+            'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
+            'dtype': 'c64' if prec == 'single' else 'c128', 'data': 'synthetic',
+            'config': {'workload': '3+1D UPPE envelope ERK4(3)-IP step, argon 1 bar, ADK + plasma, '
+                                   'self-steepening, 256x256x512, 6 mm x 400 fs, 2 mJ 40 fs, w0 1 mm, '
+                                   '1% speckle, L 2 m, tol 1e-5',
+                       'grid': [NX, NY, NT], 'precision': prec,
+                       'mixed_precision': 'complex64 bulk; FP64 phase (mod 2pi), density scan, '
+                                          'error norm, controller' if prec == 'single' else None,
+                       'attempts_timed': attempts, 'accepted_timed': accepted,
+                       'z_after_timed_m': r1.z, 'parallelism': f'replicas x{world}',
+                       'l2': 'every field (268 MB c64) exceeds the 126 MB L2; no flush'},
+            'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak,
+                         'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
+                         'traffic': None, 'launches_profiled': d_n,
+                         'bytes_model': 'per launch: fields read + written x field bytes'},
+            'roofline_step': {'model': '64*s*N bytes per attempt', 'achieved': step_achieved,
+                              'peak': peak, 'unit': 'GB/s', 'frac': step_achieved / peak},
+            'kernel_ms_per_attempt': {k: v[0] / 3 for k, v in agg.items()},
+            'cpu_baseline': cpu,
+            'e2e': {'value': e2e_v, 'unit': 'pt-steps/s', 'h2d_bytes_per_step': fbytes,
+                    'd2h_bytes_per_step': fbytes,
+                    'how': f'propagate(host pinned A0) over {e2e_attempts} attempts per call, '
+                           'spectrum copied back to pinned host memory'},
+            'plain_gpu': plain,
+            'gpu_launches': args.steps * lib.uppe3d_launches_per_step(sol._plan),
+            'clocks': clk,
+        }
+        print(json.dumps(line), flush=True)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=20)
+    ap.add_argument('--warmup', type=int, default=4)
+    ap.add_argument('--impl', default='b200', choices=['b200', 'reference'])
+    ap.add_argument('--precision', default='single', choices=['single', 'double'])
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    ap.add_argument('--no-plain-gpu', action='store_true')
+    args = ap.parse_args()
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local_rank = int(os.environ.get('LOCAL_RANK', '0'))
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == 'reference':
+        return run_reference(args, rank)
+    import datetime
+    import torch.distributed as dist
+    if world > 1:
+        import torch
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=120))
+    try:
+        return run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            dist.destroy_process_group()
+
+
+if __name__ == '__main__':
+    sys.exit(main())

@@ -1,0 +1,130 @@
+/* C ABI of the B200-native ERK4(3)-IP UPPE/GNLSE propagator (libuppe_b200.so).
+ *
+ * All field pointers are caller-owned DEVICE memory (e.g. torch tensors); every
+ * call takes a CUDA stream; no C++ exception crosses this boundary.  Functions
+ * return 0 on success or a negative UPPE_ERR_* code; uppe_last_error() gives a
+ * one-line message.  Per-run solver conditions (non-finite error, forced steps
+ * at min_step, attempt budget) are reported as UPPE_STATUS_* bits in the result.
+ *
+ * The reference is a Python research code with no FFI; each entry point below
+ * names the reference function whose behaviour it replaces.
+ */
+#ifndef UPPE_B200_H
+#define UPPE_B200_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct CUstream_st* uppe_stream_t; /* == cudaStream_t */
+
+enum { UPPE_C64 = 0, UPPE_C128 = 1 };
+
+enum {
+  UPPE_OK = 0,
+  UPPE_ERR_ARG = -1,
+  UPPE_ERR_SIZE = -2,
+  UPPE_ERR_CUDA = -3
+};
+
+enum {
+  UPPE_STATUS_NONFINITE = 1,     /* error or step size became NaN/inf: stopped   */
+  UPPE_STATUS_MIN_STEP = 2,      /* a step was forced at min_step with err > tol */
+  UPPE_STATUS_MAX_ATTEMPTS = 4   /* attempt budget exhausted before z = L         */
+};
+
+/* Last error message of this library (thread-global, one line). */
+const char* uppe_last_error(void);
+
+/* ------------------------------------------------------------------ 3+1D ---- */
+/* Grid, precomputed FP64 tables and medium constants of
+ * ERK43IP_UPPE_3D_Optimized.__init__ (src/3+1D-UPPE-ERK4(3)IP-envelope/
+ * solver_3d.py:8-98) and of the OpticalMedium plugin (media_physics.py:70-205).
+ * Host pointers; copied into the plan. */
+typedef struct {
+  int Nx, Ny, Nt;          /* powers of two: Nx, Ny in [16,512], Nt in [32,2048] */
+  int precision;           /* UPPE_C64 (mixed: FP64 phase/error/controller) or UPPE_C128 */
+  double dt;               /* t[1]-t[0]                                            */
+  const double* aw;        /* [Nt] k^2 - kref^2  (solver_3d.py:76-82)              */
+  const double* ksq;       /* [Nt] k^2                                             */
+  const double* kref;      /* [Nt] k0 + k1 omega (solver_3d.py:71-74)              */
+  const unsigned char* valid; /* [Nt] omega + omega0 > 0 (solver_3d.py:53-54,86)   */
+  const double* shock;     /* [Nt] (omega+omega0)/omega0 or 1 (media_physics.py:113-119) */
+  const double* filt;      /* [Nt] anti-alias filter (solver_3d.py:47-50)          */
+  const double* kperp2;    /* [Nx*Ny] kx^2+ky^2, index ix*Ny+iy (solver_3d.py:28-32) */
+  const double* damp;      /* [Nx*Ny] absorber (solver_3d.py:89-98)                */
+  int lut_n;               /* ionisation LUT (media_physics.py:121-137)            */
+  const double* lut_log10I;/* [lut_n] uniform grid of log10(I [W/m^2])             */
+  const double* lut_W;     /* [lut_n] rate [1/s]                                   */
+  double gamma_kerr;       /* (omega0/c) n2        (media_physics.py:192)          */
+  double gamma_hoke;       /* (omega0/c) n4        (media_physics.py:194-196)      */
+  double Ui;               /* ionisation energy [J]                                */
+  double sigma_drude;      /* [m^2]                                                */
+  double omega0_tau_c;
+  double rate_rec;         /* 1/tau_rec (rounded to float32 as in :185)            */
+  double rho_nt;           /* neutral density (rounded to float32 as in :187)      */
+  double ava_coef;         /* W_ava = ava_coef * I (0 for the gases)               */
+  int plasma_on;           /* 0 disables the plasma terms                          */
+} uppe3d_desc;
+
+typedef struct {
+  double z;                /* distance reached                                     */
+  double h;                /* next step size                                       */
+  double err;              /* error of the last attempt                            */
+  long long attempts;      /* ERK attempts (accepted + rejected)                   */
+  long long accepted;
+  int fail_count;          /* consecutive forced steps at min_step                 */
+  int status;              /* UPPE_STATUS_* bits                                   */
+  double A_scale;          /* max|A0| normalisation (solver_3d.py:166)             */
+} uppe3d_result;
+
+typedef struct uppe3d_plan uppe3d_plan;
+
+/* Replaces ERK43IP_UPPE_3D_Optimized.__init__ (solver_3d.py:8-54): uploads the
+ * tables, allocates the plan's field buffers and captures the CUDA graphs of one
+ * ERK attempt.  No allocation happens in later calls. */
+int uppe3d_plan_create(const uppe3d_desc* desc, uppe3d_plan** plan);
+int uppe3d_plan_destroy(uppe3d_plan* plan);
+/* Bytes of one complex field of the plan's grid and precision. */
+long long uppe3d_field_bytes(const uppe3d_plan* plan);
+
+/* Start of propagate (solver_3d.py:163-170): A_scale = max|A0|, state = A0/A_scale.
+ * A0: device [Nx][Ny][Nt] time-domain field in the plan's precision. */
+int uppe3d_set_field(uppe3d_plan* plan, const void* A0, uppe_stream_t stream);
+
+/* One erk43_step (solver_3d.py:100-160) of size h from the current state; writes
+ * the attempt's error (synchronises the stream). */
+int uppe3d_attempt(uppe3d_plan* plan, double h, double* err, uppe_stream_t stream);
+/* Accept (state <- attempt output, z += h) or reject the last attempt. */
+int uppe3d_commit(uppe3d_plan* plan, int accept, uppe_stream_t stream);
+
+/* The adaptive loop of propagate (solver_3d.py:172-208), run on the device:
+ * step-size control and acceptance happen in device kernels; the host only
+ * polls for completion.  max_attempts <= 0 means unlimited. */
+int uppe3d_propagate(uppe3d_plan* plan, double L, double tol, double max_step, double min_step,
+                     long long max_attempts, uppe3d_result* result, uppe_stream_t stream);
+/* Split form of uppe3d_propagate for timing: begin, then nsteps graph launches. */
+int uppe3d_begin(uppe3d_plan* plan, double L, double tol, double max_step, double min_step,
+                 long long max_attempts, uppe_stream_t stream);
+int uppe3d_run_steps(uppe3d_plan* plan, int nsteps, uppe_stream_t stream);
+int uppe3d_get_result(uppe3d_plan* plan, uppe3d_result* result, uppe_stream_t stream);
+
+/* End of propagate (solver_3d.py:215-222): out = fftshift_t(fft_t(A * A_scale)). */
+int uppe3d_get_spectrum(uppe3d_plan* plan, void* out, uppe_stream_t stream);
+/* Time-domain field A(x, y, t) of the current state (physical units), for
+ * chaining segments as the reference's drivers do with the returned field. */
+int uppe3d_get_field(uppe3d_plan* plan, void* out, uppe_stream_t stream);
+
+/* Kernel launches of one propagate-mode attempt (graph nodes). */
+int uppe3d_launches_per_step(const uppe3d_plan* plan);
+/* Measurement hook: run one attempt (plus the controller) launch by launch,
+ * bracketing each launch with CUDA events on `stream`.  Writes per launch its
+ * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar) and algorithmic
+ * bytes (0 for launches the device state made exit early). */
+int uppe3d_profile_attempt(uppe3d_plan* plan, int cap, float* ms, int* kind, double* bytes,
+                           int* n, uppe_stream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* UPPE_B200_H */

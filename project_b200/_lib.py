@@ -1,0 +1,88 @@
+"""ctypes binding of libuppe_b200.so (the C ABI declared in include/uppe_b200.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+visible, loading raises.
+"""
+import ctypes
+import os
+
+import torch
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, 'libuppe_b200.so')
+_lib = None
+
+UPPE_C64, UPPE_C128 = 0, 1
+STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS = 1, 2, 4
+
+_P = ctypes.c_void_p
+_D = ctypes.c_double
+_I = ctypes.c_int
+_LL = ctypes.c_longlong
+
+
+class Desc3D(ctypes.Structure):
+    _fields_ = [('Nx', _I), ('Ny', _I), ('Nt', _I), ('precision', _I), ('dt', _D),
+                ('aw', _P), ('ksq', _P), ('kref', _P), ('valid', _P), ('shock', _P),
+                ('filt', _P), ('kperp2', _P), ('damp', _P), ('lut_n', _I),
+                ('lut_log10I', _P), ('lut_W', _P), ('gamma_kerr', _D), ('gamma_hoke', _D),
+                ('Ui', _D), ('sigma_drude', _D), ('omega0_tau_c', _D), ('rate_rec', _D),
+                ('rho_nt', _D), ('ava_coef', _D), ('plasma_on', _I)]
+
+
+class Result3D(ctypes.Structure):
+    _fields_ = [('z', _D), ('h', _D), ('err', _D), ('attempts', _LL), ('accepted', _LL),
+                ('fail_count', _I), ('status', _I), ('A_scale', _D)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    'uppe_last_error': (ctypes.c_char_p, []),
+    'uppe3d_plan_create': (_I, [ctypes.POINTER(Desc3D), ctypes.POINTER(_P)]),
+    'uppe3d_plan_destroy': (_I, [_P]),
+    'uppe3d_field_bytes': (_LL, [_P]),
+    'uppe3d_set_field': (_I, [_P, _P, _P]),
+    'uppe3d_attempt': (_I, [_P, _D, ctypes.POINTER(_D), _P]),
+    'uppe3d_commit': (_I, [_P, _I, _P]),
+    'uppe3d_propagate': (_I, [_P, _D, _D, _D, _D, _LL, ctypes.POINTER(Result3D), _P]),
+    'uppe3d_begin': (_I, [_P, _D, _D, _D, _D, _LL, _P]),
+    'uppe3d_run_steps': (_I, [_P, _I, _P]),
+    'uppe3d_get_result': (_I, [_P, ctypes.POINTER(Result3D), _P]),
+    'uppe3d_get_spectrum': (_I, [_P, _P, _P]),
+    'uppe3d_get_field': (_I, [_P, _P, _P]),
+    'uppe3d_launches_per_step': (_I, [_P]),
+    'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),
+                                    ctypes.POINTER(_D), ctypes.POINTER(_I), _P]),
+}
+
+
+def load(require_gpu=True):
+    """Load the library (raises if it is missing, or if no GPU when required)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f'{LIB_PATH} is missing: build it with `python -m project_b200.build` '
+                           '(there is no CPU fallback)')
+    if require_gpu and not torch.cuda.is_available():
+        raise RuntimeError('project_b200 needs a CUDA GPU (sm_100a); there is no CPU fallback')
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name, None)
+        if fn is None:
+            continue
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc, what):
+    if rc != 0:
+        msg = load(require_gpu=False).uppe_last_error()
+        raise RuntimeError(f'{what} failed (rc={rc}): {msg.decode() if msg else ""}')
+
+
+def stream_ptr(stream=None):
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return ctypes.c_void_p(s.cuda_stream)

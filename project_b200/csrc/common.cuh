@@ -1,0 +1,263 @@
+// Shared device helpers for the ERK4(3)-IP UPPE kernels (sm_100a).
+//
+// * complex arithmetic on float2 / double2,
+// * radix-2/4/8/16 DFTs held in registers,
+// * an in-place Stockham (self-sorting) FFT over signals resident in shared
+//   memory, driven by a compile-time pass list.  All threads of a "team" (a warp
+//   or a block) own E elements each; pass p reads its R inputs per butterfly into
+//   registers, synchronises the team, writes the R outputs in Stockham order and
+//   synchronises again, so no second buffer is needed.
+//
+// Conventions follow numpy/scipy: forward X_k = sum_n x_n exp(-2 pi i k n / N),
+// inverse without the 1/N factor (callers fold it into a power-of-two scale).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace uppe {
+
+template <typename R> struct CT;
+template <> struct CT<float>  { using T = float2; };
+template <> struct CT<double> { using T = double2; };
+
+template <typename C> __device__ __forceinline__ C cadd(C a, C b) { return {a.x + b.x, a.y + b.y}; }
+template <typename C> __device__ __forceinline__ C csub(C a, C b) { return {a.x - b.x, a.y - b.y}; }
+template <typename C> __device__ __forceinline__ C cmul(C a, C b) {
+  return {a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x};
+}
+template <typename C, typename R> __device__ __forceinline__ C cscale(C a, R s) { return {a.x * s, a.y * s}; }
+template <typename C> __device__ __forceinline__ C cconj(C a) { return {a.x, -a.y}; }
+// multiply by i (DIR=+1) or -i (DIR=-1)
+template <int DIR, typename C> __device__ __forceinline__ C mul_pmi(C a) {
+  return DIR > 0 ? C{-a.y, a.x} : C{a.y, -a.x};
+}
+template <typename C> __device__ __forceinline__ C czero() { return {0, 0}; }
+
+// exp(DIR * 2 pi i k / R) as compile-time constants for R <= 16
+template <int R, int K> struct Twid {
+  static constexpr int k16 = (K * 16 / R) % 16;   // angle index on the 16-grid
+  __host__ __device__ static constexpr double kc(int i) {
+    return i == 0 ? 1.0 : i == 1 ? 0.92387953251128675613 : i == 2 ? 0.70710678118654752440
+         : i == 3 ? 0.38268343236508977173 : i == 4 ? 0.0 : i == 5 ? -0.38268343236508977173
+         : i == 6 ? -0.70710678118654752440 : -0.92387953251128675613;
+  }
+  __host__ __device__ static constexpr double ks(int i) {
+    return i == 0 ? 0.0 : i == 1 ? 0.38268343236508977173 : i == 2 ? 0.70710678118654752440
+         : i == 3 ? 0.92387953251128675613 : i == 4 ? 1.0 : i == 5 ? 0.92387953251128675613
+         : i == 6 ? 0.70710678118654752440 : 0.38268343236508977173;
+  }
+  static constexpr double cv = k16 < 8 ? kc(k16) : -kc(k16 - 8);
+  static constexpr double sv = k16 < 8 ? ks(k16) : -ks(k16 - 8);
+};
+
+// x * exp(DIR * 2 pi i K / R)
+template <int R, int K, int DIR, typename C> __device__ __forceinline__ C rot(C x) {
+  using Rl = decltype(x.x);
+  constexpr int k = K % R;
+  if constexpr (k == 0) {
+    return x;
+  } else if constexpr (4 * k == R) {
+    return mul_pmi<DIR>(x);
+  } else if constexpr (2 * k == R) {
+    return C{-x.x, -x.y};
+  } else if constexpr (4 * k == 3 * R) {
+    return mul_pmi<-DIR>(x);
+  } else {
+    constexpr double cd = Twid<R, k>::cv, sd = DIR * Twid<R, k>::sv;
+    const Rl c = (Rl)cd;
+    const Rl s = (Rl)sd;
+    return C{x.x * c - x.y * s, x.x * s + x.y * c};
+  }
+}
+
+// In-register DFT of size R (R in {1,2,4,8,16}); DIR=-1 forward, +1 inverse.
+template <int R, int DIR, typename C> struct DFT {
+  __device__ __forceinline__ static void run(C* v) {
+    C e[R / 2], o[R / 2];
+#pragma unroll
+    for (int i = 0; i < R / 2; ++i) { e[i] = v[2 * i]; o[i] = v[2 * i + 1]; }
+    DFT<R / 2, DIR, C>::run(e);
+    DFT<R / 2, DIR, C>::run(o);
+    combine<0>(v, e, o);
+  }
+  template <int K> __device__ __forceinline__ static void combine(C* v, const C* e, const C* o) {
+    if constexpr (K < R / 2) {
+      C t = rot<R, K, DIR>(o[K]);
+      v[K] = cadd(e[K], t);
+      v[K + R / 2] = csub(e[K], t);
+      combine<K + 1>(v, e, o);
+    }
+  }
+};
+template <int DIR, typename C> struct DFT<1, DIR, C> {
+  __device__ __forceinline__ static void run(C*) {}
+};
+template <int DIR, typename C> struct DFT<2, DIR, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    C a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <int DIR, typename C> struct DFT<4, DIR, C> {
+  __device__ __forceinline__ static void run(C* v) {
+    C t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    C t2 = cadd(v[1], v[3]), t3 = mul_pmi<DIR>(csub(v[1], v[3]));
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+
+// Largest radix in {16,8,4,2} dividing both the remaining length and E.
+template <int REM, int E> struct PickRadix {
+  static constexpr int v = (REM % 16 == 0 && E % 16 == 0) ? 16
+                         : (REM % 8 == 0 && E % 8 == 0)   ? 8
+                         : (REM % 4 == 0 && E % 4 == 0)   ? 4
+                                                           : 2;
+};
+
+// Stockham passes over NSIG signals of length N in shared memory.
+//   IDX(sig, n) -> shared-memory element index.
+//   tw[m] = exp(-2 pi i m / N) (forward table, conjugated for DIR=+1).
+//   Team of NTHR threads, thread id `tid`; E = N*NSIG/NTHR elements per thread.
+//   Butterfly b of thread tid: bf = tid + b*NTHR; sig = bf % NSIG; j = bf / NSIG.
+template <int N, int NSIG, int NTHR, int DIR, int Ns, typename C, typename IDX, typename SYNC>
+__device__ __forceinline__ void stockham(C* s, const C* tw, int tid, IDX idx, SYNC sync) {
+  if constexpr (Ns < N) {
+    constexpr int E = N * NSIG / NTHR;
+    static_assert(E >= 2, "need at least two elements per thread");
+    constexpr int R = PickRadix<N / Ns, E>::v;
+    constexpr int B = E / R;
+    constexpr int M = N / R;   // butterflies per signal
+    C v[B][R];
+    // threads with tid >= NTHR (a team padded to a full warp) only synchronise
+    const bool act = tid < NTHR;
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      if (!act) break;
+      const int bf = tid + b * NTHR;
+      const int sig = bf % NSIG, j = bf / NSIG;
+      const int k = j & (Ns - 1);
+#pragma unroll
+      for (int r = 0; r < R; ++r) v[b][r] = s[idx(sig, j + r * M)];
+      if constexpr (Ns > 1) {
+#pragma unroll
+        for (int r = 1; r < R; ++r) {
+          C w = tw[(r * k) * (N / (Ns * R))];
+          if (DIR > 0) w.y = -w.y;
+          v[b][r] = cmul(v[b][r], w);
+        }
+      }
+      DFT<R, DIR, C>::run(v[b]);
+    }
+    sync();
+#pragma unroll
+    for (int b = 0; b < B; ++b) {
+      if (!act) break;
+      const int bf = tid + b * NTHR;
+      const int sig = bf % NSIG, j = bf / NSIG;
+      const int k = j & (Ns - 1);
+      const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+      for (int r = 0; r < R; ++r) s[idx(sig, base + r * Ns)] = v[b][r];
+    }
+    sync();
+    stockham<N, NSIG, NTHR, DIR, Ns * R, C>(s, tw, tid, idx, sync);
+  }
+}
+
+// Non-negative double -> order-preserving 64-bit key for atomicMax (NaN > +inf).
+__device__ __forceinline__ unsigned long long dkey(double v) {
+  return (unsigned long long)__double_as_longlong(v);
+}
+__device__ __forceinline__ void atomic_max_nonneg(unsigned long long* dst, double v) {
+  atomicMax(dst, dkey(v));
+}
+
+// max over the first WIDTH lanes of a warp (WIDTH = 32, or the whole block when
+// it is smaller than a warp); only those lanes may call it.
+template <int WIDTH = 32, typename R> __device__ __forceinline__ R warp_max(R v) {
+  constexpr unsigned mask = WIDTH >= 32 ? 0xffffffffu : ((1u << WIDTH) - 1u);
+#pragma unroll
+  for (int o = (WIDTH >= 32 ? 16 : WIDTH / 2); o > 0; o >>= 1) {
+    R u = __shfl_xor_sync(mask, v, o);
+    v = (u > v || u != u) ? u : v;    // NaN propagates
+  }
+  return v;
+}
+
+// ---------------------------------------------------------------------------
+// Ionisation LUT (media_physics.py:131-137): clip log10(I + 1e-30) to the grid,
+// then numpy.interp semantics (j with xp[j] <= x < xp[j+1]; slope evaluated in
+// FP64 as numpy does).
+// ---------------------------------------------------------------------------
+struct Lut {
+  const void* x;    // grid, field precision
+  const void* w;    // rates, field precision
+  int n;
+  double x0, inv_dx;
+};
+
+template <typename Rl>
+__device__ __forceinline__ Rl lut_eval(const Lut& L, Rl I) {
+  const Rl* xp = reinterpret_cast<const Rl*>(L.x);
+  const Rl* fp = reinterpret_cast<const Rl*>(L.w);
+  const int n = L.n;
+  Rl x = (sizeof(Rl) == 8) ? (Rl)log10((double)I + 1e-30) : (Rl)log10f((float)I + 1e-30f);
+  const Rl x0 = __ldg(xp), x1 = __ldg(xp + n - 1);
+  x = x < x0 ? x0 : (x > x1 ? x1 : x);
+  int j = (int)floor(((double)x - L.x0) * L.inv_dx);
+  j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+  while (j < n - 1 && __ldg(xp + j + 1) <= x) ++j;
+  while (j > 0 && __ldg(xp + j) > x) --j;
+  if (j >= n - 1) return __ldg(fp + n - 1);
+  const Rl xj = __ldg(xp + j);
+  if (xj == x) return __ldg(fp + j);
+  const double slope = ((double)__ldg(fp + j + 1) - (double)__ldg(fp + j)) /
+                       ((double)__ldg(xp + j + 1) - (double)xj);
+  return (Rl)(slope * ((double)x - (double)xj) + (double)__ldg(fp + j));
+}
+
+// Plasma constants shared by the 1D and 3D nonlinear kernels.
+struct PlasmaConst {
+  double Ui;          // ionisation energy [J]
+  double sigma_half;  // sigma_drude / 2
+  double w0tc;        // omega0 * tau_c
+  double rr, dt, rho_nt;   // float32-rounded, as the reference passes them (:185-187)
+  double ava;         // W_ava = ava * I
+};
+
+// One step of the reference density update (media_physics.py:36-64): returns
+// gen[t] and advances rho.
+__device__ __forceinline__ double rho_step(double& rho, double w_pi, double w_av, const PlasmaConst& m) {
+  double depl = (m.rho_nt - rho) / m.rho_nt;
+  if (depl < 0.0) depl = 0.0;
+  const double gen = (w_pi * m.rho_nt + w_av * rho) * depl;
+  const double S = w_pi * m.rho_nt * depl;
+  const double G = w_av * depl - m.rr;
+  double gdt = G * m.dt;
+  if (gdt > 10.0) gdt = 10.0;
+  if (gdt < -10.0) gdt = -10.0;
+  const double eg = exp(gdt);
+  const double sf = (fabs(gdt) < 1e-5) ? m.dt * (1.0 + 0.5 * gdt) : (eg - 1.0) / G;
+  double r = rho * eg + S * sf;
+  if (r > m.rho_nt) r = m.rho_nt;
+  if (r < 0.0) r = 0.0;
+  rho = r;
+  return gen;
+}
+
+// Affine form of the update while no clamp binds (w_av = 0):
+// rho' = rho (e - w sf) + w rho_nt sf with e = exp(gdt0), gdt0 = clamp(-rr dt).
+struct AffineStep {
+  double e, sf;
+  __device__ __forceinline__ explicit AffineStep(const PlasmaConst& m) {
+    const double gdt0 = fmin(fmax(-m.rr * m.dt, -10.0), 10.0);
+    e = exp(gdt0);
+    sf = (fabs(gdt0) < 1e-5) ? m.dt * (1.0 + 0.5 * gdt0) : (e - 1.0) / (-m.rr);
+  }
+};
+
+}  // namespace uppe

@@ -1,0 +1,1203 @@
+// 3+1D envelope ERK4(3)-IP UPPE propagator, sm_100a.
+//
+// Replaces ERK43IP_UPPE_3D_Optimized (src/3+1D-UPPE-ERK4(3)IP-envelope/solver_3d.py)
+// and the envelope medium's nonlinear response + plasma kernel
+// (src/3+1D-UPPE-ERK4(3)IP-envelope/media_physics.py:11-67, 156-205).
+//
+// Field layout in HBM: [Nx][Ny][Nt], t (or omega) contiguous, complex64 or
+// complex128.  The accepted state is kept in the (x, y, omega) domain
+// ("Z" = fft_t of the reference's time-domain field), so the reference's
+// per-attempt output transform ifft_t(ifft2(A4) * filter) * exp(-damp h) and the
+// next attempt's fft2(fft_t(.)) collapse into one x-pass that writes
+// ifft2(A4) * filter * absorber.  One ERK attempt is a fixed sequence of passes:
+//
+//   T   : t-lines      -- ifft_t, Kerr + steepening, ADK LUT, rho scan, plasma,
+//                         fft_t (x2), shock/mask combine              (k_tpass)
+//   X   : x-columns    -- fft / ifft along x                           (k_space)
+//   Y   : y-columns    -- fft_y, ERK stage algebra with the interaction-
+//                         picture factor exp(h/2 D) computed on the fly in
+//                         FP64, ifft_y of the next stage input          (k_space)
+//
+// Eval 1 (only after an accepted step):  T(Z) X(NL,Z) Ymid1
+// Evals 2-4:                             Xinv T Xfwd Ymid{2,3,4}
+// Eval 5:                                Xinv(+Z candidate) T Xfwd Yfwd5 (error)
+// then an error kernel and (in propagate mode) the step-size controller, all
+// on the device; every kernel reads the device state and exits early when the
+// propagation is done, so the whole attempt is one reusable CUDA graph.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <vector>
+
+#include "common.cuh"
+#include "../../include/uppe_b200.h"
+
+namespace uppe {
+
+// ---------------------------------------------------------------------------
+// device state and tables
+// ---------------------------------------------------------------------------
+struct State3D {
+  double z, h, L, tol, max_step, min_step;
+  double err, err_num, err_den;
+  double A_scale, inv_A_scale;
+  unsigned long long red_norm, red_diff;
+  long long attempts, accepted, max_attempts;
+  int fail_count, zidx, fresh, done, status, last_accept;
+};
+
+struct Medium3D : PlasmaConst {
+  double gk;          // (omega0/c) n2          -> Kerr = i gk I A
+  double g4;          // (omega0/c) n4          -> HOKE = i g4 I^2 A
+  int plasma;         // 0: plasma terms off
+};
+
+struct Tables3D {
+  const double* aw;      // k^2 - kref^2            [Nt]
+  const double* ksq;     // k^2                     [Nt]
+  const double* kref;    // k0 + k1 omega           [Nt]
+  const unsigned char* valid;   // omega_abs > 0    [Nt]
+  const double* shock;   // (omega+omega0)/omega0 or 1   [Nt]
+  const double* filt;    // anti-alias filter        [Nt]
+  const double* q;       // kx^2 + ky^2   [Nx*Ny]
+  const double* damp;    // absorber damp(x, y)      [Nx*Ny]
+  const void* twx;       // exp(-2 pi i m/Nx) in the field precision
+  const void* twy;
+  const void* twt;
+  Lut lut;               // ionisation table (field precision)
+};
+
+enum SpaceMode { XINV = 0, XINV_Z, XFWD, XFWD_Z, YMID1, YMID1R, YMID2, YMID3, YMID4, YFWD5 };
+
+struct Bufs3D {
+  void* z[2];     // accepted state / candidate (x, y, omega)
+  void* acur;     // fft2(Z) of the accepted state (kx, ky, omega)
+  void* k1;       // N(A) of the accepted state
+  void* tsum;     // term_sum, then beta
+  void* a4p;      // alpha4'
+  void* tmp[3];   // pass temporaries
+};
+
+struct Geom {
+  int Nx, Ny, Nt;
+  long long npts;
+};
+
+// ---------------------------------------------------------------------------
+// interaction-picture factor exp(h2 * D(kx, ky, omega)), D as in
+// solver_3d.py:56-87:  D = i (k^2 - kref^2 - kperp^2) / (kz + kref),
+// kz = sqrt(k^2 - kperp^2) (complex), masked where omega_abs <= 0.
+// The complex division follows numpy's algorithm (Smith's method).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ip_operator(const Tables3D& tb, int iw, double q, double& Dr,
+                                            double& Di) {
+  if (!tb.valid[iw]) { Dr = 0.0; Di = 0.0; return; }
+  const double num = tb.aw[iw] - q;
+  const double arg = tb.ksq[iw] - q;
+  double dr, di;
+  if (arg >= 0.0) { dr = sqrt(arg) + tb.kref[iw]; di = 0.0; }
+  else { dr = tb.kref[iw]; di = sqrt(-arg); }
+  double rr, ri;   // num / (dr + i di)
+  if (fabs(dr) >= fabs(di)) {
+    const double rat = di / dr;
+    const double scl = 1.0 / (dr + di * rat);
+    rr = num * scl;
+    ri = (-num * rat) * scl;
+  } else {
+    const double rat = dr / di;
+    const double scl = 1.0 / (di + dr * rat);
+    rr = (num * rat) * scl;
+    ri = (-num) * scl;
+  }
+  Dr = -ri;   // 1j * (rr + i ri)
+  Di = rr;
+}
+
+template <typename Rl> struct IPFactor;
+template <> struct IPFactor<double> {
+  __device__ __forceinline__ static double2 get(const Tables3D& tb, int iw, double q, double h2) {
+    double Dr, Di;
+    ip_operator(tb, iw, q, Dr, Di);
+    const double ar = h2 * Dr, ai = h2 * Di;
+    double s, c;
+    sincos(ai, &s, &c);
+    const double m = exp(ar);
+    return make_double2(m * c, m * s);
+  }
+};
+template <> struct IPFactor<float> {
+  // Mixed precision: the phase h/2*Im(D) is formed in FP64 and reduced mod 2 pi
+  // before it is rounded to FP32.
+  __device__ __forceinline__ static float2 get(const Tables3D& tb, int iw, double q, double h2) {
+    double Dr, Di;
+    ip_operator(tb, iw, q, Dr, Di);
+    double ph = h2 * Di;
+    const double twopi = 6.283185307179586476925286766559;
+    ph = ph - twopi * rint(ph * (1.0 / twopi));
+    float s, c;
+    sincosf((float)ph, &s, &c);
+    const float m = expf((float)(h2 * Dr));
+    return make_float2(m * c, m * s);
+  }
+};
+
+template <typename C> __device__ __forceinline__ C ldg_c(const C* p) { return __ldg(p); }
+
+// ---------------------------------------------------------------------------
+// spatial passes: tile = W omega-columns x N rows (x or y), N-point FFT per column
+// ---------------------------------------------------------------------------
+constexpr int kW = 16;   // omega columns per tile
+
+template <int N> struct SpaceCfg {
+  static constexpr int E = N < 16 ? N : 16;
+  static constexpr int NTHR = kW * N / E;
+};
+
+struct SpaceArgs {
+  State3D* st;
+  Tables3D tb;
+  Bufs3D b;
+  Geom g;
+  const void* in;     // primary input (pass temporaries)
+  void* out;          // primary output
+  int mode;
+};
+
+template <typename C> struct TileIdx {
+  __device__ __forceinline__ int operator()(int sig, int n) const { return n * kW + sig; }
+};
+struct BlockSync {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+template <typename C, int N, int NTHR>
+__device__ __forceinline__ void load_tile(C* s, const C* __restrict__ g, long long base,
+                                          long long stride, int tid) {
+  // 16-byte vectors: VPR vectors per row of kW complex
+  constexpr int VPR = kW * (int)sizeof(C) / 16;
+  const float4* __restrict__ gv = reinterpret_cast<const float4*>(g);
+  float4* sv = reinterpret_cast<float4*>(s);
+#pragma unroll 4
+  for (int v = tid; v < N * VPR; v += NTHR) {
+    const int n = v / VPR, c = v % VPR;
+    sv[n * VPR + c] = __ldg(gv + (base + n * stride) * (long long)sizeof(C) / 16 + c);
+  }
+}
+template <typename C, int N, int NTHR>
+__device__ __forceinline__ void store_tile(const C* s, C* __restrict__ g, long long base,
+                                           long long stride, int tid) {
+  constexpr int VPR = kW * (int)sizeof(C) / 16;
+  float4* __restrict__ gv = reinterpret_cast<float4*>(g);
+  const float4* sv = reinterpret_cast<const float4*>(s);
+#pragma unroll 4
+  for (int v = tid; v < N * VPR; v += NTHR) {
+    const int n = v / VPR, c = v % VPR;
+    gv[(base + n * stride) * (long long)sizeof(C) / 16 + c] = sv[n * VPR + c];
+  }
+}
+
+template <typename Rl, int N>
+__global__ void __launch_bounds__(SpaceCfg<N>::NTHR)
+k_space(SpaceArgs a) {
+  using C = typename CT<Rl>::T;
+  constexpr int NTHR = SpaceCfg<N>::NTHR;
+  constexpr int E = SpaceCfg<N>::E;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* s = tw + N;
+  C* s2 = s + N * kW;   // second tile (XFWD_Z, YMID1)
+  const int tid = threadIdx.x;
+  State3D* st = a.st;
+  const int mode = a.mode;
+  const bool xpass = mode <= XFWD_Z;
+  {
+    const C* gtw = reinterpret_cast<const C*>(xpass ? a.tb.twx : a.tb.twy);
+    for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  if (st->done) return;
+  if ((mode == XFWD_Z || mode == YMID1) && !st->fresh) return;
+  if (mode == YMID1R && st->fresh) return;
+
+  const int Nt = a.g.Nt, Ny = a.g.Ny;
+  const int ntile = Nt / kW;
+  const int o = blockIdx.x / ntile;          // y index (x pass) or kx index (y pass)
+  const int w0 = (blockIdx.x % ntile) * kW;  // omega offset
+  const long long stride = xpass ? (long long)Ny * Nt : (long long)Nt;
+  const long long base = (xpass ? (long long)o * Nt : (long long)o * Ny * Nt) + w0;
+  const double h = st->h;
+  TileIdx<C> idx;
+  BlockSync sync;
+  const C* in = reinterpret_cast<const C*>(a.in);
+  C* out = reinterpret_cast<C*>(a.out);
+
+  if (xpass) {
+    const bool inv = (mode == XINV || mode == XINV_Z);
+    load_tile<C, N, NTHR>(s, in, base, stride, tid);
+    __syncthreads();
+    if (inv) stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+    else stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    store_tile<C, N, NTHR>(s, out, base, stride, tid);
+    if (mode == XINV_Z) {
+      // candidate state Z = ifft2(A4) * filter(omega) * exp(-damp(x,y) h)
+      C* zc = reinterpret_cast<C*>(a.b.z[st->zidx ^ 1]);
+      const Rl nrm = (Rl)(1.0 / ((double)a.g.Nx * (double)a.g.Ny));
+#pragma unroll
+      for (int i = 0; i < E; ++i) {
+        const int e = tid + i * NTHR;
+        const int n = e / kW, w = e % kW;   // n = x index, o = y index
+        const Rl ab = (Rl)exp(-a.tb.damp[(long long)n * Ny + o] * h);
+        const Rl f = (Rl)a.tb.filt[w0 + w];
+        C v = s[idx(w, n)];
+        v = cscale(cscale(cscale(v, nrm), f), ab);
+        zc[base + n * stride + w] = v;
+      }
+    }
+    if (mode == XFWD_Z) {
+      const C* zin = reinterpret_cast<const C*>(a.b.z[st->zidx]);
+      C* zout = reinterpret_cast<C*>(a.b.tmp[2]);
+      __syncthreads();
+      load_tile<C, N, NTHR>(s, zin, base, stride, tid);
+      __syncthreads();
+      stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+      store_tile<C, N, NTHR>(s, zout, base, stride, tid);
+    }
+    return;
+  }
+
+  // ---------------- y passes (stage algebra in the (kx, ky, omega) domain) ----
+  C* acur = reinterpret_cast<C*>(a.b.acur);
+  C* k1b = reinterpret_cast<C*>(a.b.k1);
+  C* tsum = reinterpret_cast<C*>(a.b.tsum);
+  C* a4p = reinterpret_cast<C*>(a.b.a4p);
+  const double h2 = 0.5 * h;
+  const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
+
+  if (mode != YMID1R) {
+    load_tile<C, N, NTHR>(s, in, base, stride, tid);
+    if (mode == YMID1) load_tile<C, N, NTHR>(s2, reinterpret_cast<const C*>(a.b.tmp[2]), base, stride, tid);
+    __syncthreads();
+    stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    if (mode == YMID1) stockham<N, kW, NTHR, -1, 1, C>(s2, tw, tid, idx, sync);
+  }
+
+  double red = 0.0;
+#pragma unroll 2
+  for (int i = 0; i < E; ++i) {
+    const int e = tid + i * NTHR;
+    const int n = e / kW, w = e % kW;     // n = ky, o = kx
+    const long long gi = base + n * stride + w;
+    const int iw = w0 + w;
+    if (mode == YFWD5) {
+      const C a5 = s[idx(w, n)];
+      const C a4 = a4p[gi];
+      double d;
+      if (sizeof(Rl) == 8) {
+        // literal |A4 - A3| as in solver_3d.py:145-151
+        const C beta = tsum[gi];
+        const C A4 = cadd(beta, cscale(a4, h6R));
+        const Rl h30 = (Rl)(h / 30);
+        const C A3 = cadd(beta, cscale(cadd(cscale(a4, (Rl)2), cscale(a5, (Rl)3)), h30));
+        const C dd = csub(A4, A3);
+        d = sqrt((double)dd.x * dd.x + (double)dd.y * dd.y);
+      } else {
+        const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
+        d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+      }
+      red = (d > red || d != d) ? d : red;
+      continue;
+    }
+    if (mode == YMID4) {
+      const C a4 = s[idx(w, n)];
+      const C beta = tsum[gi];
+      const C A4 = cadd(beta, cscale(a4, h6R));
+      a4p[gi] = a4;
+      const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+      red = (m > red || m != m) ? m : red;
+      s[idx(w, n)] = A4;
+      continue;
+    }
+    const double qv = a.tb.q[(long long)o * Ny + n];
+    const C Ef = IPFactor<Rl>::get(a.tb, iw, qv, h2);
+    if (mode == YMID1 || mode == YMID1R) {
+      C A, k1;
+      if (mode == YMID1) {
+        A = s2[idx(w, n)];
+        k1 = s[idx(w, n)];
+        acur[gi] = A;
+        k1b[gi] = k1;
+      } else {
+        A = acur[gi];
+        k1 = k1b[gi];
+      }
+      const C v = cmul(A, Ef);
+      const C a1 = cmul(k1, Ef);
+      tsum[gi] = a1;
+      s[idx(w, n)] = cadd(v, cscale(a1, h2R));
+    } else if (mode == YMID2) {
+      const C a2 = s[idx(w, n)];
+      const C v = cmul(acur[gi], Ef);
+      const C ts = tsum[gi];
+      tsum[gi] = cadd(ts, cscale(a2, (Rl)2));
+      s[idx(w, n)] = cadd(v, cscale(a2, h2R));
+    } else {   // YMID3
+      const C a3 = s[idx(w, n)];
+      const C v = cmul(acur[gi], Ef);
+      const C ts = cadd(tsum[gi], cscale(a3, (Rl)2));
+      const C beta = cmul(cadd(v, cscale(ts, h6R)), Ef);
+      tsum[gi] = beta;
+      s[idx(w, n)] = cmul(cadd(v, cscale(a3, hR)), Ef);
+    }
+  }
+  if (mode == YMID4 || mode == YFWD5) {
+    red = warp_max<(NTHR < 32 ? NTHR : 32)>(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(mode == YMID4 ? &st->red_norm : &st->red_diff, red);
+    if (mode == YFWD5) return;
+  }
+  __syncthreads();
+  stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+  store_tile<C, N, NTHR>(s, out, base, stride, tid);
+}
+
+// ---------------------------------------------------------------------------
+// t-line nonlinear pass (media_physics.py:156-205 + the plasma kernel :11-67)
+// ---------------------------------------------------------------------------
+enum TMode { T_GENERAL = 0, T_FROM_Z = 1 };
+
+struct TArgs {
+  State3D* st;
+  Tables3D tb;
+  Medium3D md;
+  Bufs3D b;
+  Geom g;
+  const void* in;
+  void* out;
+  int mode;
+};
+
+template <int NT> struct TCfg {
+  static constexpr int PAD = NT + NT / 32;
+  static constexpr int FT = NT / 2 < 32 ? NT / 2 : 32;   // FFT team (lanes >= FT idle)
+};
+__device__ __forceinline__ int tpad(int n) { return n + (n >> 5); }
+struct LineIdx {
+  __device__ __forceinline__ int operator()(int, int n) const { return tpad(n); }
+};
+struct WarpSync {
+  __device__ __forceinline__ void operator()() const { __syncwarp(); }
+};
+
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_tpass(TArgs a) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* sK = tw + NT + warp * 2 * PAD;
+  C* sP = sK + PAD;
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
+    for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  State3D* st = a.st;
+  if (st->done) return;
+  if (a.mode == T_FROM_Z && !st->fresh) return;
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  const long long nlines = (long long)a.g.Nx * a.g.Ny;
+  if (line >= nlines) return;
+  const C* in = a.mode == T_FROM_Z ? reinterpret_cast<const C*>(a.b.z[st->zidx])
+                                   : reinterpret_cast<const C*>(a.in);
+  C* out = reinterpret_cast<C*>(a.out);
+  const Rl in_scale = (Rl)(a.mode == T_FROM_Z ? 1.0 / NT
+                                               : 1.0 / ((double)NT * a.g.Nx * a.g.Ny));
+  const double A_scale = st->A_scale;
+  const Rl A_scaleR = (Rl)A_scale;
+  const Medium3D& m = a.md;
+  LineIdx idx;
+  WarpSync wsync;
+
+  // load (coalesced) and inverse FFT along t
+  const C* src = in + line * NT;
+#pragma unroll
+  for (int i = 0; i < E; ++i) sK[tpad(lane + 32 * i)] = src[lane + 32 * i];
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sK, tw, lane, idx, wsync);
+
+  // ---- nonlinear response on this lane's chunk t in [lane*E, lane*E+E) ----
+  const int t0 = lane * E;
+  bool any_w = false;
+  bool affine_ok = (m.ava == 0.0);
+  double cmap = 1.0, dmap = 0.0;   // composed affine map of the chunk
+  const AffineStep aff(m);
+  const double eg0 = aff.e, sf0 = aff.sf;
+  if (m.plasma) {
+#pragma unroll 4
+    for (int t = t0; t < t0 + E; ++t) {
+      const C av = cscale(sK[tpad(t)], in_scale);
+      const C Ap = cscale(av, A_scaleR);
+      const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+      any_w |= (w != 0.0);
+      // rho' = rho (e - w sf) + w rho_nt sf, valid while w sf <= e (no clamping)
+      const double c = eg0 - w * sf0;
+      affine_ok &= (c >= 0.0);
+      dmap = c * dmap + w * m.rho_nt * sf0;
+      cmap = c * cmap;
+    }
+  }
+  const bool plasma_line = m.plasma && (__any_sync(0xffffffffu, any_w) || m.ava != 0.0);
+  double rho0 = 0.0;
+  if (plasma_line) {
+    if (__all_sync(0xffffffffu, affine_ok)) {
+      // exclusive scan of affine maps over lanes: (c1,d1) then (c2,d2) = (c1 c2, c2 d1 + d2)
+      double c = cmap, d = dmap;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double cp = __shfl_up_sync(0xffffffffu, c, off);
+        const double dp = __shfl_up_sync(0xffffffffu, d, off);
+        if (lane >= off) { d = c * dp + d; c = c * cp; }
+      }
+      // inclusive (c,d) of lanes 0..lane applied to rho=0 gives rho after the chunk;
+      const double incl = d;
+      const double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+      rho0 = lane == 0 ? 0.0 : excl;
+    } else {
+      // serial exact pass by lane 0 records the density at each chunk start
+      double* starts = reinterpret_cast<double*>(sP);
+      if (lane == 0) {
+        double rho = 0.0;
+        for (int t = 0; t < NT; ++t) {
+          if (t % E == 0) starts[t / E] = rho;
+          const C av = cscale(sK[tpad(t)], in_scale);
+          const C Ap = cscale(av, A_scaleR);
+          const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+          const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+          const double wa = (double)(float)(m.ava * (double)I);
+          rho_step(rho, w, wa, m);
+        }
+      }
+      __syncwarp();
+      rho0 = starts[lane];
+      __syncwarp();
+    }
+  }
+  // phase 3: exact per-sample update from the chunk start; write Kerr and plasma terms
+  {
+    double rho = rho0;
+#pragma unroll 4
+    for (int t = t0; t < t0 + E; ++t) {
+      const C av = cscale(sK[tpad(t)], in_scale);
+      const C Ap = cscale(av, A_scaleR);
+      const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+      Rl g = (Rl)m.gk * I;
+      if (m.g4 != 0.0) g += (Rl)m.g4 * I * I;
+      sK[tpad(t)] = C{-g * av.y, g * av.x};   // i g a
+      if (plasma_line) {
+        const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+        const double wa = (double)(float)(m.ava * (double)I);
+        const double rho_t = rho;
+        const double gen = rho_step(rho, w, wa, m);
+        const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
+        const double cr = loss - m.sigma_half * rho_t;
+        const double ci = -m.sigma_half * m.w0tc * rho_t;
+        sP[tpad(t)] = C{(Rl)cr * av.x - (Rl)ci * av.y, (Rl)cr * av.y + (Rl)ci * av.x};
+      }
+    }
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sK, tw, lane, idx, wsync);
+  if (plasma_line) stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sP, tw, lane, idx, wsync);
+  C* dst = out + line * NT;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int wi = lane + 32 * i;
+    const Rl sh = (Rl)a.tb.shock[wi];
+    C v = cscale(sK[tpad(wi)], sh);
+    if (plasma_line) v = cadd(v, sP[tpad(wi)]);
+    if (!a.tb.valid[wi]) v = C{0, 0};
+    dst[wi] = v;
+  }
+}
+
+// initial transform: Z = fft_t(A0 / A_scale)
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_tload(TArgs a) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* sK = tw + NT + warp * 2 * PAD;
+  const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[i];
+  __syncthreads();
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  if (line >= (long long)a.g.Nx * a.g.Ny) return;
+  const C* src = reinterpret_cast<const C*>(a.in) + line * NT;
+  const Rl inv = (Rl)a.st->inv_A_scale;
+#pragma unroll
+  for (int i = 0; i < E; ++i) sK[tpad(lane + 32 * i)] = cscale(src[lane + 32 * i], inv);
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sK, tw, lane, LineIdx(), WarpSync());
+  C* dst = reinterpret_cast<C*>(a.b.z[0]) + line * NT;
+#pragma unroll
+  for (int i = 0; i < E; ++i) dst[lane + 32 * i] = sK[tpad(lane + 32 * i)];
+}
+
+// |A0| max reduction
+template <typename Rl>
+__global__ void k_absmax(const typename CT<Rl>::T* __restrict__ x, long long n, State3D* st) {
+  double m = 0.0;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const auto v = x[i];
+    const double a = sqrt((double)v.x * v.x + (double)v.y * v.y);
+    m = (a > m || a != a) ? a : m;
+  }
+  m = warp_max(m);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(&st->red_norm, m);
+}
+
+__global__ void k_set_scale(State3D* st) {
+  double s = __longlong_as_double((long long)st->red_norm);
+  st->red_norm = 0ull;
+  if (!(s >= 1e-30)) s = 1.0;   // solver_3d.py:166-168
+  st->A_scale = s;
+  st->inv_A_scale = 1.0 / s;
+  st->zidx = 0;
+  st->fresh = 1;
+  st->done = 0;
+  st->status = 0;
+}
+
+// error of the attempt (solver_3d.py:151-153)
+__global__ void k_err(State3D* st) {
+  if (st->done) return;
+  const double num = __longlong_as_double((long long)st->red_diff);
+  const double den = __longlong_as_double((long long)st->red_norm);
+  st->red_diff = 0ull;
+  st->red_norm = 0ull;
+  st->err_num = num;
+  st->err_den = den;
+  st->err = num / (den + 1e-20);
+}
+
+// adaptive controller (solver_3d.py:182-208), plus the finite-value check the
+// reference lacks (a NaN error there never terminates)
+__global__ void k_controller(State3D* st) {
+  if (st->done) return;
+  double err = st->err;
+  double h = st->h;
+  st->attempts += 1;
+  if (!isfinite(err) || !isfinite(h)) {
+    st->status |= UPPE_STATUS_NONFINITE;
+    st->done = 1;
+    st->last_accept = 0;
+    return;
+  }
+  const double tol = st->tol, min_step = st->min_step, max_step = st->max_step;
+  if (err < tol || h <= min_step * 1.01) {
+    st->fail_count = (h <= min_step * 1.01 && err > tol) ? st->fail_count + 1 : 0;
+    if (st->fail_count > 0) st->status |= UPPE_STATUS_MIN_STEP;
+    st->z += h;
+    st->zidx ^= 1;
+    st->fresh = 1;
+    st->accepted += 1;
+    st->last_accept = 1;
+    err = fmax(err, 1e-30);
+    double factor = 0.95 * pow(tol / err, 0.2);
+    if (st->fail_count > 0) factor = fmin(factor, 1.2);
+    h = fmin(h * fmin(factor, 2.0), max_step);
+  } else {
+    st->fresh = 0;
+    st->last_accept = 0;
+    err = fmax(err, 1e-30);
+    const double factor = 0.95 * pow(tol / err, 0.2);
+    h = fmax(h * factor, min_step);
+  }
+  if (!(st->z < st->L)) {
+    st->done = 1;
+  } else {
+    const double dist = st->L - st->z;
+    if (h > dist) {
+      h = dist;
+      if (h < 1e-15) st->done = 1;
+    }
+  }
+  if (st->max_attempts > 0 && st->attempts >= st->max_attempts && !st->done) {
+    st->status |= UPPE_STATUS_MAX_ATTEMPTS;
+    st->done = 1;
+  }
+  st->h = h;
+}
+
+__global__ void k_set_h(State3D* st, double h) {
+  st->h = h;
+  st->done = 0;
+}
+
+__global__ void k_commit(State3D* st, int accept) {
+  if (accept) {
+    st->z += st->h;
+    st->zidx ^= 1;
+    st->fresh = 1;
+    st->accepted += 1;
+  } else {
+    st->fresh = 0;
+  }
+  st->attempts += 1;
+}
+
+__global__ void k_begin(State3D* st, double L, double tol, double max_step, double min_step,
+                        long long max_attempts) {
+  st->z = 0.0;
+  st->L = L;
+  st->tol = tol;
+  st->max_step = max_step;
+  st->min_step = min_step;
+  double h = fmin(max_step, L / 1000.0);   // solver_3d.py:173
+  st->attempts = 0;
+  st->accepted = 0;
+  st->max_attempts = max_attempts;
+  st->fail_count = 0;
+  st->status = 0;
+  st->done = 0;
+  st->red_norm = 0ull;
+  st->red_diff = 0ull;
+  if (!(0.0 < L)) st->done = 1;
+  else if (h > L) { h = L; if (h < 1e-15) st->done = 1; }
+  st->h = h;
+}
+
+// spectrum output: fftshift_t(Z * A_scale)   (solver_3d.py:215-222)
+template <typename Rl>
+__global__ void k_spectrum(const typename CT<Rl>::T* __restrict__ z, typename CT<Rl>::T* __restrict__ out,
+                           long long nlines, int Nt, const State3D* st) {
+  const Rl s = (Rl)st->A_scale;
+  const long long n = nlines * Nt;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long line = i / Nt;
+    const int w = (int)(i % Nt);
+    const int ws = (w + Nt / 2) % Nt;   // fftshift destination
+    out[line * Nt + ws] = cscale(z[i], s);
+  }
+}
+
+// time-domain field A_t = ifft_t(Z) * A_scale, for chaining segments
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32)
+k_tstore(TArgs a) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* sK = tw + NT + warp * 2 * PAD;
+  const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[i];
+  __syncthreads();
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  if (line >= (long long)a.g.Nx * a.g.Ny) return;
+  const C* src = reinterpret_cast<const C*>(a.b.z[a.st->zidx]) + line * NT;
+#pragma unroll
+  for (int i = 0; i < E; ++i) sK[tpad(lane + 32 * i)] = src[lane + 32 * i];
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sK, tw, lane, LineIdx(), WarpSync());
+  const Rl s = (Rl)(a.st->A_scale / NT);
+  C* dst = reinterpret_cast<C*>(a.out) + line * NT;
+#pragma unroll
+  for (int i = 0; i < E; ++i) dst[lane + 32 * i] = cscale(sK[tpad(lane + 32 * i)], s);
+}
+
+// ---------------------------------------------------------------------------
+// host side
+// ---------------------------------------------------------------------------
+template <int NT, typename Rl> struct TLaunch {
+  static constexpr int WPB = (2 * TCfg<NT>::PAD * (int)sizeof(typename CT<Rl>::T) * 8 <= 72 * 1024) ? 8
+                           : (2 * TCfg<NT>::PAD * (int)sizeof(typename CT<Rl>::T) * 4 <= 72 * 1024) ? 4
+                           : (2 * TCfg<NT>::PAD * (int)sizeof(typename CT<Rl>::T) * 2 <= 110 * 1024) ? 2 : 1;
+  static size_t smem() {
+    return (size_t)(NT + WPB * 2 * TCfg<NT>::PAD) * sizeof(typename CT<Rl>::T);
+  }
+};
+
+}  // namespace uppe
+
+using namespace uppe;
+
+struct uppe3d_plan {
+  uppe3d_desc d;
+  Geom g;
+  int dbl;
+  size_t csz;
+  State3D* st;          // device
+  State3D* st_host;     // pinned mirror
+  Tables3D tb;
+  Medium3D md;
+  Bufs3D b;
+  std::vector<void*> allocs;
+  cudaGraphExec_t g_attempt = nullptr, g_step = nullptr;
+  cudaStream_t cap_stream = nullptr;
+};
+
+#define UPPE_CK(x)                                                                 \
+  do {                                                                             \
+    cudaError_t e_ = (x);                                                          \
+    if (e_ != cudaSuccess) {                                                       \
+      snprintf(g_uppe_err, sizeof(g_uppe_err), "%s:%d %s: %s", __FILE__, __LINE__, \
+               #x, cudaGetErrorString(e_));                                        \
+      return UPPE_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+char g_uppe_err[512];
+
+extern "C" const char* uppe_last_error(void) { return g_uppe_err; }
+
+static int is_pow2(int n) { return n > 0 && (n & (n - 1)) == 0; }
+
+static int dev_upload(uppe3d_plan* p, void** dst, const void* src, size_t bytes) {
+  UPPE_CK(cudaMalloc(dst, bytes));
+  p->allocs.push_back(*dst);
+  UPPE_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+template <typename Rl> static std::vector<unsigned char> twiddles(int N) {
+  using C = typename CT<Rl>::T;
+  std::vector<unsigned char> out(sizeof(C) * N);
+  C* c = reinterpret_cast<C*>(out.data());
+  for (int m = 0; m < N; ++m) {
+    // exp(-2 pi i m / N), evaluated in extended precision and rounded once
+    const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)N;
+    c[m].x = (Rl)(double)cosl(ang);
+    c[m].y = (Rl)(double)sinl(ang);
+  }
+  return out;
+}
+
+// ---- template dispatch -----------------------------------------------------
+template <typename Rl, int N>
+static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, cudaStream_t s) {
+  k_space<Rl, N><<<(unsigned)nblocks, SpaceCfg<N>::NTHR, smem, s>>>(a);
+}
+
+template <typename Rl>
+static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cudaStream_t s) {
+  using C = typename CT<Rl>::T;
+  SpaceArgs a;
+  a.st = p->st; a.tb = p->tb; a.b = p->b; a.g = p->g; a.in = in; a.out = out; a.mode = mode;
+  const bool xpass = mode <= XFWD_Z;
+  const int N = xpass ? p->g.Nx : p->g.Ny;
+  const long long nouter = xpass ? p->g.Ny : p->g.Nx;
+  const long long nblocks = nouter * (p->g.Nt / kW);
+  const size_t smem = sizeof(C) * (size_t)(N + 2 * N * kW);
+  switch (N) {
+#define UPPE_SP(n) case n: launch_space_n<Rl, n>(a, nblocks, smem, s); break;
+    UPPE_SP(16) UPPE_SP(32) UPPE_SP(64) UPPE_SP(128) UPPE_SP(256) UPPE_SP(512)
+#undef UPPE_SP
+    default: return UPPE_ERR_SIZE;
+  }
+  return 0;
+}
+
+template <typename Rl, int NT, int KIND>
+static void launch_t_n(const TArgs& a, long long nlines, cudaStream_t s) {
+  constexpr int WPB = TLaunch<NT, Rl>::WPB;
+  const unsigned nb = (unsigned)((nlines + WPB - 1) / WPB);
+  const size_t smem = TLaunch<NT, Rl>::smem();
+  if (KIND == 0) k_tpass<Rl, NT, WPB><<<nb, WPB * 32, smem, s>>>(a);
+  else if (KIND == 1) k_tload<Rl, NT, WPB><<<nb, WPB * 32, smem, s>>>(a);
+  else k_tstore<Rl, NT, WPB><<<nb, WPB * 32, smem, s>>>(a);
+}
+
+template <typename Rl, int KIND>
+static int launch_t(uppe3d_plan* p, int mode, const void* in, void* out, cudaStream_t s) {
+  TArgs a;
+  a.st = p->st; a.tb = p->tb; a.md = p->md; a.b = p->b; a.g = p->g;
+  a.in = in; a.out = out; a.mode = mode;
+  const long long nl = (long long)p->g.Nx * p->g.Ny;
+  switch (p->g.Nt) {
+#define UPPE_T(n) case n: launch_t_n<Rl, n, KIND>(a, nl, s); break;
+    UPPE_T(32) UPPE_T(64) UPPE_T(128) UPPE_T(256) UPPE_T(512) UPPE_T(1024) UPPE_T(2048)
+#undef UPPE_T
+    default: return UPPE_ERR_SIZE;
+  }
+  return 0;
+}
+
+template <typename Rl, int N>
+static cudaError_t set_space_attr() {
+  const int smem = (int)(sizeof(typename CT<Rl>::T) * (N + 2 * N * kW));
+  return cudaFuncSetAttribute(k_space<Rl, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+template <typename Rl, int NT>
+static cudaError_t set_t_attr() {
+  constexpr int WPB = TLaunch<NT, Rl>::WPB;
+  const int smem = (int)TLaunch<NT, Rl>::smem();
+  cudaError_t e = cudaFuncSetAttribute(k_tpass<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  e = cudaFuncSetAttribute(k_tload<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+  if (e != cudaSuccess) return e;
+  return cudaFuncSetAttribute(k_tstore<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+template <typename Rl>
+static int set_attrs(const Geom& g) {
+  cudaError_t e = cudaSuccess;
+  for (int N : {g.Nx, g.Ny}) {
+    switch (N) {
+      case 16: e = set_space_attr<Rl, 16>(); break;
+      case 32: e = set_space_attr<Rl, 32>(); break;
+      case 64: e = set_space_attr<Rl, 64>(); break;
+      case 128: e = set_space_attr<Rl, 128>(); break;
+      case 256: e = set_space_attr<Rl, 256>(); break;
+      case 512: e = set_space_attr<Rl, 512>(); break;
+      default: return UPPE_ERR_SIZE;
+    }
+    if (e != cudaSuccess) break;
+  }
+  if (e == cudaSuccess) {
+    switch (g.Nt) {
+      case 32: e = set_t_attr<Rl, 32>(); break;
+      case 64: e = set_t_attr<Rl, 64>(); break;
+      case 128: e = set_t_attr<Rl, 128>(); break;
+      case 256: e = set_t_attr<Rl, 256>(); break;
+      case 512: e = set_t_attr<Rl, 512>(); break;
+      case 1024: e = set_t_attr<Rl, 1024>(); break;
+      case 2048: e = set_t_attr<Rl, 2048>(); break;
+      default: return UPPE_ERR_SIZE;
+    }
+  }
+  UPPE_CK(e);
+  return 0;
+}
+
+// Launch recorder: in capture mode it only launches; in profile mode it brackets
+// every launch with CUDA events on the launching stream and records the pass
+// kind and the algorithmic bytes the launch moves.
+struct Recorder {
+  cudaStream_t s;
+  bool prof = false;
+  int fresh = 1;                 // known device state (profile mode only)
+  double fbytes = 0.0;           // bytes of one field
+  std::vector<cudaEvent_t> ev;
+  std::vector<int> kind;
+  std::vector<double> bytes;
+  template <typename F> int operator()(int k, double nfields, bool active, F&& launch) {
+    cudaEvent_t a = nullptr, b = nullptr;
+    if (prof) { cudaEventCreate(&a); cudaEventCreate(&b); cudaEventRecord(a, s); }
+    const int rc = launch();
+    if (prof) {
+      cudaEventRecord(b, s);
+      ev.push_back(a); ev.push_back(b);
+      kind.push_back(k);
+      bytes.push_back(active ? nfields * fbytes : 0.0);
+    }
+    return rc;
+  }
+};
+
+enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3 };
+
+// the fixed pass sequence of one attempt (see the file header); the numbers are
+// the fields each launch reads + writes (algorithmic bytes / field bytes)
+template <typename Rl>
+static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
+  int rc = 0;
+  cudaStream_t s = r.s;
+  void* const* t = p->b.tmp;
+  const bool f = r.fresh != 0;
+  // eval 1 (skipped on device unless the state is fresh)
+  rc |= r(KIND_T, 2, f, [&] { return launch_t<Rl, 0>(p, T_FROM_Z, nullptr, t[0], s); });
+  rc |= r(KIND_X, 4, f, [&] { return launch_space<Rl>(p, XFWD_Z, t[0], t[1], s); });
+  rc |= r(KIND_Y, 6, f, [&] { return launch_space<Rl>(p, YMID1, t[1], t[0], s); });
+  rc |= r(KIND_Y, 4, !f, [&] { return launch_space<Rl>(p, YMID1R, nullptr, t[0], s); });
+  // eval 2..4
+  const int mids[3] = {YMID2, YMID3, YMID4};
+  const double midb[3] = {5, 5, 4};
+  for (int k = 0; k < 3; ++k) {
+    rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XINV, t[0], t[1], s); });
+    rc |= r(KIND_T, 2, true, [&] { return launch_t<Rl, 0>(p, T_GENERAL, t[1], t[2], s); });
+    rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XFWD, t[2], t[1], s); });
+    rc |= r(KIND_Y, midb[k], true, [&] { return launch_space<Rl>(p, mids[k], t[1], t[0], s); });
+  }
+  // eval 5 (+ candidate state) and the error reduction
+  rc |= r(KIND_X, 3, true, [&] { return launch_space<Rl>(p, XINV_Z, t[0], t[1], s); });
+  rc |= r(KIND_T, 2, true, [&] { return launch_t<Rl, 0>(p, T_GENERAL, t[1], t[2], s); });
+  rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XFWD, t[2], t[1], s); });
+  rc |= r(KIND_Y, sizeof(Rl) == 8 ? 3 : 2, true,
+          [&] { return launch_space<Rl>(p, YFWD5, t[1], nullptr, s); });
+  rc |= r(KIND_SMALL, 0, true, [&] { k_err<<<1, 1, 0, s>>>(p->st); return 0; });
+  return rc;
+}
+
+static int build_graphs(uppe3d_plan* p) {
+  cudaStream_t s;
+  UPPE_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  for (int which = 0; which < 2; ++which) {
+    cudaGraph_t graph;
+    UPPE_CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+    Recorder rec;
+    rec.s = s;
+    int rc = p->dbl ? enqueue_attempt<double>(p, rec) : enqueue_attempt<float>(p, rec);
+    if (which == 1) k_controller<<<1, 1, 0, s>>>(p->st);
+    UPPE_CK(cudaStreamEndCapture(s, &graph));
+    if (rc) return rc;
+    UPPE_CK(cudaGraphInstantiate(which ? &p->g_step : &p->g_attempt, graph, 0));
+    UPPE_CK(cudaGraphDestroy(graph));
+  }
+  UPPE_CK(cudaStreamDestroy(s));
+  return 0;
+}
+
+extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
+  *out = nullptr;
+  g_uppe_err[0] = 0;
+  if (!d) return UPPE_ERR_ARG;
+  if (!is_pow2(d->Nx) || !is_pow2(d->Ny) || !is_pow2(d->Nt) || d->Nx < 16 || d->Ny < 16 ||
+      d->Nx > 512 || d->Ny > 512 || d->Nt < 32 || d->Nt > 2048) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err),
+             "unsupported grid %dx%dx%d: Nx, Ny must be powers of two in [16, 512] and Nt a "
+             "power of two in [32, 2048]", d->Nx, d->Ny, d->Nt);
+    return UPPE_ERR_SIZE;
+  }
+  if (d->precision != UPPE_C64 && d->precision != UPPE_C128) return UPPE_ERR_ARG;
+  if (d->precision == UPPE_C128 && (d->Nx > 256 || d->Ny > 256)) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err),
+             "complex128 plans support Nx, Ny <= 256 (shared-memory tile limit)");
+    return UPPE_ERR_SIZE;
+  }
+  uppe3d_plan* p = new uppe3d_plan();
+  p->d = *d;
+  p->g.Nx = d->Nx; p->g.Ny = d->Ny; p->g.Nt = d->Nt;
+  p->g.npts = (long long)d->Nx * d->Ny * d->Nt;
+  p->dbl = d->precision == UPPE_C128;
+  p->csz = p->dbl ? 16 : 8;
+  int rc = 0;
+#define UPPE_TRY(x) do { rc = (x); if (rc) { uppe3d_plan_destroy(p); return rc; } } while (0)
+  {
+    cudaError_t e = cudaMalloc(&p->st, sizeof(State3D));
+    if (e != cudaSuccess) { snprintf(g_uppe_err, sizeof(g_uppe_err), "cudaMalloc state: %s", cudaGetErrorString(e)); delete p; return UPPE_ERR_CUDA; }
+    p->allocs.push_back(p->st);
+    e = cudaMallocHost(&p->st_host, sizeof(State3D));
+    if (e != cudaSuccess) { snprintf(g_uppe_err, sizeof(g_uppe_err), "cudaMallocHost: %s", cudaGetErrorString(e)); uppe3d_plan_destroy(p); return UPPE_ERR_CUDA; }
+    memset(p->st_host, 0, sizeof(State3D));
+    e = cudaMemcpy(p->st, p->st_host, sizeof(State3D), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { uppe3d_plan_destroy(p); return UPPE_ERR_CUDA; }
+  }
+  const int Nt = d->Nt, Nxy = d->Nx * d->Ny;
+  void* ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->aw, 8 * Nt)); p->tb.aw = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->ksq, 8 * Nt)); p->tb.ksq = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->kref, 8 * Nt)); p->tb.kref = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->valid, Nt)); p->tb.valid = (const unsigned char*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->shock, 8 * Nt)); p->tb.shock = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->filt, 8 * Nt)); p->tb.filt = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->kperp2, 8 * (size_t)Nxy)); p->tb.q = (const double*)ptr;
+  UPPE_TRY(dev_upload(p, &ptr, d->damp, 8 * (size_t)Nxy)); p->tb.damp = (const double*)ptr;
+  {
+    auto tx = p->dbl ? twiddles<double>(d->Nx) : twiddles<float>(d->Nx);
+    auto ty = p->dbl ? twiddles<double>(d->Ny) : twiddles<float>(d->Ny);
+    auto tt = p->dbl ? twiddles<double>(d->Nt) : twiddles<float>(d->Nt);
+    UPPE_TRY(dev_upload(p, &ptr, tx.data(), tx.size())); p->tb.twx = ptr;
+    UPPE_TRY(dev_upload(p, &ptr, ty.data(), ty.size())); p->tb.twy = ptr;
+    UPPE_TRY(dev_upload(p, &ptr, tt.data(), tt.size())); p->tb.twt = ptr;
+  }
+  {
+    const int n = d->lut_n;
+    if (n < 2) { uppe3d_plan_destroy(p); return UPPE_ERR_ARG; }
+    std::vector<unsigned char> lx(n * (p->dbl ? 8 : 4)), lw(n * (p->dbl ? 8 : 4));
+    for (int i = 0; i < n; ++i) {
+      if (p->dbl) { ((double*)lx.data())[i] = d->lut_log10I[i]; ((double*)lw.data())[i] = d->lut_W[i]; }
+      else { ((float*)lx.data())[i] = (float)d->lut_log10I[i]; ((float*)lw.data())[i] = (float)d->lut_W[i]; }
+    }
+    UPPE_TRY(dev_upload(p, &ptr, lx.data(), lx.size())); p->tb.lut.x = ptr;
+    UPPE_TRY(dev_upload(p, &ptr, lw.data(), lw.size())); p->tb.lut.w = ptr;
+    p->tb.lut.n = n;
+    p->tb.lut.x0 = d->lut_log10I[0];
+    p->tb.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
+  }
+  p->md.gk = d->gamma_kerr;
+  p->md.g4 = d->gamma_hoke;
+  p->md.Ui = d->Ui;
+  p->md.sigma_half = d->sigma_drude / 2.0;
+  p->md.w0tc = d->omega0_tau_c;
+  p->md.rr = (double)(float)d->rate_rec;
+  p->md.dt = (double)(float)d->dt;
+  p->md.rho_nt = (double)(float)d->rho_nt;
+  p->md.ava = d->ava_coef;
+  p->md.plasma = d->plasma_on;
+  const size_t fbytes = p->csz * (size_t)p->g.npts;
+  void** fields[] = {&p->b.z[0], &p->b.z[1], &p->b.acur, &p->b.k1, &p->b.tsum, &p->b.a4p,
+                     &p->b.tmp[0], &p->b.tmp[1], &p->b.tmp[2]};
+  for (void** f : fields) {
+    cudaError_t e = cudaMalloc(f, fbytes);
+    if (e != cudaSuccess) {
+      snprintf(g_uppe_err, sizeof(g_uppe_err), "cudaMalloc of a %zu-byte field: %s", fbytes, cudaGetErrorString(e));
+      uppe3d_plan_destroy(p);
+      return UPPE_ERR_CUDA;
+    }
+    p->allocs.push_back(*f);
+  }
+  UPPE_TRY(p->dbl ? set_attrs<double>(p->g) : set_attrs<float>(p->g));
+  UPPE_TRY(build_graphs(p));
+#undef UPPE_TRY
+  *out = p;
+  return 0;
+}
+
+extern "C" int uppe3d_plan_destroy(uppe3d_plan* p) {
+  if (!p) return 0;
+  if (p->g_attempt) cudaGraphExecDestroy(p->g_attempt);
+  if (p->g_step) cudaGraphExecDestroy(p->g_step);
+  for (void* a : p->allocs) cudaFree(a);
+  if (p->st_host) cudaFreeHost(p->st_host);
+  delete p;
+  return 0;
+}
+
+extern "C" int uppe3d_set_field(uppe3d_plan* p, const void* A0, cudaStream_t s) {
+  if (!p || !A0) return UPPE_ERR_ARG;
+  const long long n = p->g.npts;
+  if (p->dbl) k_absmax<double><<<148 * 8, 256, 0, s>>>((const double2*)A0, n, p->st);
+  else k_absmax<float><<<148 * 8, 256, 0, s>>>((const float2*)A0, n, p->st);
+  k_set_scale<<<1, 1, 0, s>>>(p->st);
+  int rc = p->dbl ? launch_t<double, 1>(p, 0, A0, nullptr, s) : launch_t<float, 1>(p, 0, A0, nullptr, s);
+  if (rc) return rc;
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe3d_attempt(uppe3d_plan* p, double h, double* err, cudaStream_t s) {
+  if (!p) return UPPE_ERR_ARG;
+  k_set_h<<<1, 1, 0, s>>>(p->st, h);
+  UPPE_CK(cudaGraphLaunch(p->g_attempt, s));
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  if (err) *err = p->st_host->err;
+  return 0;
+}
+
+extern "C" int uppe3d_commit(uppe3d_plan* p, int accept, cudaStream_t s) {
+  if (!p) return UPPE_ERR_ARG;
+  k_commit<<<1, 1, 0, s>>>(p->st, accept);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+static void fill_result(const State3D* h, uppe3d_result* r) {
+  r->z = h->z;
+  r->h = h->h;
+  r->err = h->err;
+  r->attempts = h->attempts;
+  r->accepted = h->accepted;
+  r->fail_count = h->fail_count;
+  r->status = h->status;
+  r->A_scale = h->A_scale;
+}
+
+extern "C" int uppe3d_propagate(uppe3d_plan* p, double L, double tol, double max_step,
+                                double min_step, long long max_attempts, uppe3d_result* res,
+                                cudaStream_t s) {
+  if (!p) return UPPE_ERR_ARG;
+  k_begin<<<1, 1, 0, s>>>(p->st, L, tol, max_step, min_step, max_attempts);
+  UPPE_CK(cudaGetLastError());
+  int batch = 1;
+  for (;;) {
+    for (int i = 0; i < batch; ++i) UPPE_CK(cudaGraphLaunch(p->g_step, s));
+    UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+    UPPE_CK(cudaStreamSynchronize(s));
+    if (p->st_host->done) break;
+    if (batch < 16) batch *= 2;
+  }
+  if (res) fill_result(p->st_host, res);
+  return 0;
+}
+
+extern "C" int uppe3d_run_steps(uppe3d_plan* p, int nsteps, cudaStream_t s) {
+  if (!p) return UPPE_ERR_ARG;
+  for (int i = 0; i < nsteps; ++i) UPPE_CK(cudaGraphLaunch(p->g_step, s));
+  return 0;
+}
+
+extern "C" int uppe3d_begin(uppe3d_plan* p, double L, double tol, double max_step,
+                            double min_step, long long max_attempts, cudaStream_t s) {
+  if (!p) return UPPE_ERR_ARG;
+  k_begin<<<1, 1, 0, s>>>(p->st, L, tol, max_step, min_step, max_attempts);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe3d_get_result(uppe3d_plan* p, uppe3d_result* res, cudaStream_t s) {
+  if (!p || !res) return UPPE_ERR_ARG;
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  fill_result(p->st_host, res);
+  return 0;
+}
+
+extern "C" int uppe3d_get_spectrum(uppe3d_plan* p, void* out, cudaStream_t s) {
+  if (!p || !out) return UPPE_ERR_ARG;
+  const long long nl = (long long)p->g.Nx * p->g.Ny;
+  const void* z = nullptr;
+  // the state index lives on the device; fetch it (tiny sync copy)
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  z = p->b.z[p->st_host->zidx];
+  if (p->dbl) k_spectrum<double><<<148 * 8, 256, 0, s>>>((const double2*)z, (double2*)out, nl, p->g.Nt, p->st);
+  else k_spectrum<float><<<148 * 8, 256, 0, s>>>((const float2*)z, (float2*)out, nl, p->g.Nt, p->st);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe3d_get_field(uppe3d_plan* p, void* out, cudaStream_t s) {
+  if (!p || !out) return UPPE_ERR_ARG;
+  int rc = p->dbl ? launch_t<double, 2>(p, 0, nullptr, out, s) : launch_t<float, 2>(p, 0, nullptr, out, s);
+  if (rc) return rc;
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" long long uppe3d_field_bytes(const uppe3d_plan* p) {
+  return p ? (long long)(p->csz * p->g.npts) : 0;
+}
+
+extern "C" int uppe3d_launches_per_step(const uppe3d_plan* p) {
+  (void)p;
+  return 22;   // 21 passes + error kernel per attempt, plus the controller
+}
+
+extern "C" int uppe3d_profile_attempt(uppe3d_plan* p, int cap, float* ms, int* kind,
+                                      double* bytes, int* n, cudaStream_t s) {
+  if (!p || !ms || !kind || !bytes || !n) return UPPE_ERR_ARG;
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  Recorder rec;
+  rec.s = s;
+  rec.prof = true;
+  rec.fresh = p->st_host->fresh;
+  rec.fbytes = (double)p->csz * (double)p->g.npts;
+  int rc = p->dbl ? enqueue_attempt<double>(p, rec) : enqueue_attempt<float>(p, rec);
+  k_controller<<<1, 1, 0, s>>>(p->st);
+  UPPE_CK(cudaStreamSynchronize(s));
+  const int m = (int)rec.kind.size();
+  for (int i = 0; i < m && i < cap; ++i) {
+    cudaEventElapsedTime(&ms[i], rec.ev[2 * i], rec.ev[2 * i + 1]);
+    kind[i] = rec.kind[i];
+    bytes[i] = rec.bytes[i];
+  }
+  for (auto e : rec.ev) cudaEventDestroy(e);
+  *n = m < cap ? m : cap;
+  return rc;
+}

@@ -1,0 +1,81 @@
+"""Seeded synthetic inputs (host side, numpy).
+
+Pulse builders follow the reference: ``generate_gaussian_pulse`` and
+``generate_dispersed_pulse`` of ``src/1D-ERK4(3)IP UPPE gas/erk43ip_method.py:375-446``.
+The noise and speckle models have no counterpart in the reference; their
+definitions are:
+
+* ``photon_noise``: one photon per mode.  For FFT bin j with absolute frequency
+  w_j > 0, a complex Gaussian of variance hbar*w_j*Nt/dt is added to fft(A), so
+  that with E = sum |A|^2 dt each mode carries hbar*w_j on average.
+* ``speckle``: amplitude factor 1 + amp*xi(x, y), xi a zero-mean, unit-variance
+  Gaussian random field obtained by filtering white N(0,1) noise with
+  exp(-(k_perp*l)^2/4) (correlation length l).
+All random draws use numpy's PCG64 generator with the given seed.
+"""
+import numpy as np
+
+HBAR = 1.054571817e-34
+C0 = 299792458.0
+
+
+def gaussian_pulse(t, pulse_energy, pulse_fwhm, chirp=0.0):
+    """erk43ip_method.py:375-381: sqrt(P0) exp(-(1 + i C)(t/T0)^2 / 2)."""
+    t = np.asarray(t, dtype=np.float64)
+    P0 = pulse_energy / (pulse_fwhm * np.sqrt(np.pi / (4 * np.log(2))))
+    T0 = pulse_fwhm / (2 * np.sqrt(np.log(2)))
+    return np.sqrt(P0) * np.exp(-(1 + 1j * chirp) * (t / T0) ** 2 / 2)
+
+
+def dispersed_pulse(t, pulse_energy, pulse_fwhm, GDD=0.0, TOD=0.0):
+    """erk43ip_method.py:383-446: transform-limited Gaussian with a spectral
+    phase GDD w^2/2 + TOD w^3/6 applied about the window centre."""
+    t = np.asarray(t, dtype=np.float64)
+    P0 = pulse_energy / (pulse_fwhm * np.sqrt(np.pi / (4 * np.log(2))))
+    T0 = pulse_fwhm / (2 * np.sqrt(np.log(2)))
+    A = np.sqrt(P0) * np.exp(-(t / T0) ** 2 / 2)
+    if GDD == 0 and TOD == 0:
+        return A.astype(np.complex128)
+    n = len(t)
+    w = 2 * np.pi * np.fft.fftfreq(n, t[1] - t[0])
+    spec = np.fft.fft(np.fft.ifftshift(A))
+    spec = spec * np.exp(1j * (0.5 * GDD * w ** 2 + (1.0 / 6.0) * TOD * w ** 3))
+    return np.fft.fftshift(np.fft.ifft(spec))
+
+
+def photon_noise(t, center_wavelength, seed):
+    t = np.asarray(t, dtype=np.float64)
+    n = len(t)
+    dt = t[1] - t[0]
+    w_abs = 2 * np.pi * C0 / center_wavelength + 2 * np.pi * np.fft.fftfreq(n, dt)
+    sigma = np.sqrt(np.where(w_abs > 0, HBAR * w_abs * n / dt, 0.0))
+    rng = np.random.Generator(np.random.PCG64(seed))
+    xi = (rng.standard_normal(n) + 1j * rng.standard_normal(n)) / np.sqrt(2.0)
+    return np.fft.ifft(sigma * xi)
+
+
+def speckle(x, y, corr_len, amp, seed):
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    kx = 2 * np.pi * np.fft.fftfreq(len(x), x[1] - x[0])
+    ky = 2 * np.pi * np.fft.fftfreq(len(y), y[1] - y[0])
+    rng = np.random.Generator(np.random.PCG64(seed))
+    white = rng.standard_normal((len(x), len(y)))
+    filt = np.exp(-(kx[:, None] ** 2 + ky[None, :] ** 2) * corr_len ** 2 / 4)
+    xi = np.real(np.fft.ifft2(np.fft.fft2(white) * filt))
+    xi = (xi - xi.mean()) / xi.std()
+    return 1.0 + amp * xi
+
+
+def gaussian_beam(x, y, t, w0, pulse_energy, pulse_fwhm, dtype=np.complex128):
+    """Collimated beam exp(-r^2/w0^2) x Gaussian pulse, |A|^2 in W/m^2, scaled so
+    that sum |A|^2 dx dy dt equals the pulse energy."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    T0 = pulse_fwhm / (2 * np.sqrt(np.log(2)))
+    sp = np.exp(-(x[:, None] ** 2 + y[None, :] ** 2) / w0 ** 2)
+    tp = np.exp(-(t / T0) ** 2 / 2)
+    E = np.sum(sp ** 2) * np.sum(tp ** 2) * (x[1] - x[0]) * (y[1] - y[0]) * (t[1] - t[0])
+    s = np.sqrt(pulse_energy / E)
+    return ((s * sp)[:, :, None] * tp[None, None, :]).astype(dtype)

@@ -1,0 +1,191 @@
+"""3+1D envelope ERK4(3)-IP UPPE propagator on the GPU (drop-in for
+``ERK43IP_UPPE_3D_Optimized``, src/3+1D-UPPE-ERK4(3)IP-envelope/solver_3d.py).
+
+The host computes the FP64 tables of ``__init__`` (solver_3d.py:8-98) exactly as
+the reference does and hands them to ``libuppe_b200.so``; every per-step
+operation (FFTs, interaction-picture factor, nonlinear response with the plasma
+scan, ERK stages, error norm, step-size control) runs in the library's CUDA
+kernels.  ``precision='double'`` is complex128 throughout; ``'single'`` is the
+mixed mode: complex64 bulk with the FP64 interaction-picture phase (reduced mod
+2 pi before rounding), FP64 density scan, FP64 error norm and controller.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib
+
+
+class ERK43IP_UPPE_3D_Optimized:
+    def __init__(self, x_grid, y_grid, t_grid, medium, precision='single', device=None):
+        lib = _lib.load()
+        self._lib = lib
+        self.medium = medium
+        self.c, self.lambda0, self.omega0 = medium.c, medium.lambda0, medium.omega0
+        self.precision = precision
+        if precision == 'double':
+            self.complex_dtype, self._prec = torch.complex128, _lib.UPPE_C128
+        elif precision == 'single':
+            self.complex_dtype, self._prec = torch.complex64, _lib.UPPE_C64
+        else:
+            raise ValueError("precision must be 'single' or 'double'")
+        self.device = torch.device(device if device is not None else 'cuda')
+        x = np.asarray(x_grid, dtype=np.float64)
+        y = np.asarray(y_grid, dtype=np.float64)
+        t = np.asarray(t_grid, dtype=np.float64)
+        self.x, self.y, self.t = x, y, t
+        self.Nx, self.Ny, self.Nt = len(x), len(y), len(t)
+        self.dx, self.dy, self.dt = float(x[1] - x[0]), float(y[1] - y[0]), float(t[1] - t[0])
+        self._tables()
+        self._create_plan()
+        self.A_scale = 1.0
+        self.last_result = None
+
+    # ---- FP64 tables of solver_3d.py:28-98 ------------------------------------
+    def _tables(self):
+        kx = 2 * np.pi * np.fft.fftfreq(self.Nx, self.dx)                    # :28
+        ky = 2 * np.pi * np.fft.fftfreq(self.Ny, self.dy)                    # :29
+        # kperp^2 at field index (ix, iy).  The reference's meshgrid(ky, kx,
+        # indexing='ij') (:30) puts ky on axis 0, which is the same array for the
+        # square, equally spaced grids it supports.
+        self.K2_perp = (kx[:, None] ** 2 + ky[None, :] ** 2).astype(np.float64)
+        omega = 2 * np.pi * np.fft.fftfreq(self.Nt, self.dt)                 # :34
+        self.omega = omega
+        self.freq_axis_hz = np.fft.fftshift(omega) / (2 * np.pi)             # :36
+        m = self.medium
+        w0, c = float(self.omega0), float(self.c)
+        n_omega = np.asarray(m.refractive_index(omega + w0), dtype=np.float64)   # :61
+        k_val = n_omega * (omega + w0) / c                                   # :62
+        n_center = float(m.refractive_index(np.array([w0]))[0])             # :64-65
+        dw = w0 * 1e-3                                                       # :67
+        n_plus = float(m.refractive_index(np.array([w0 + dw]))[0])          # :68-69
+        k0 = n_center * w0 / c                                               # :71
+        k_plus = n_plus * (w0 + dw) / c                                      # :72
+        k1 = (k_plus - k0) / dw                                              # :73
+        k_ref = k0 + k1 * omega                                              # :74
+        self.k_sq = k_val ** 2
+        self.k_ref = k_ref
+        self.a_w = self.k_sq - k_ref ** 2                                    # :82 (first term)
+        self.valid = ((omega + w0) > 0).astype(np.uint8)                     # :86, :53-54
+        self.shock = np.asarray(m.get_shock_operator(omega), dtype=np.float64)   # :44
+        f = omega / (2 * np.pi)                                              # :47
+        f_max = float(np.max(np.abs(f))) + 1e-10                             # :48
+        self.filter = np.exp(-(f / (0.85 * f_max)) ** 16)                    # :49
+        X, Y = np.meshgrid(self.x, self.y, indexing='ij')                    # :90
+        R = np.sqrt(X ** 2 + Y ** 2)
+        half_w = float(np.max(np.abs(self.x)))
+        r_edge, r_start = 0.98 * half_w, 0.85 * half_w
+        s = np.clip((R - r_start) / (r_edge - r_start + 1e-30), 0.0, 1.0)
+        self.damp = (120.0 * (s ** 10)).astype(np.float64)                   # :98
+
+    def _create_plan(self):
+        m = self.medium
+        if m.lut_log10I is None:
+            raise ValueError('the medium has no ionisation LUT')
+        self._keep = [np.ascontiguousarray(a) for a in (
+            self.a_w, self.k_sq, self.k_ref, self.valid, self.shock, self.filter,
+            self.K2_perp.ravel(), self.damp.ravel(), m.lut_log10I, m.lut_W)]
+        ptr = [a.ctypes.data for a in self._keep]
+        d = _lib.Desc3D()
+        d.Nx, d.Ny, d.Nt, d.precision, d.dt = self.Nx, self.Ny, self.Nt, self._prec, self.dt
+        (d.aw, d.ksq, d.kref, d.valid, d.shock, d.filt, d.kperp2, d.damp) = ptr[:8]
+        d.lut_n = len(m.lut_log10I)
+        d.lut_log10I, d.lut_W = ptr[8], ptr[9]
+        d.gamma_kerr = (m.omega0 / m.c) * m.n2                               # media_physics.py:192
+        d.gamma_hoke = (m.omega0 / m.c) * m.n4
+        d.Ui = m.Ui
+        d.sigma_drude = m.sigma_drude
+        d.omega0_tau_c = m.omega0 * m.tau_c
+        d.rate_rec = 1.0 / m.tau_rec
+        d.rho_nt = m.rho_nt
+        d.ava_coef = m.avalanche_coef
+        d.plasma_on = 1 if m.plasma else 0
+        plan = ctypes.c_void_p()
+        with torch.cuda.device(self.device):
+            _lib.check(self._lib.uppe3d_plan_create(ctypes.byref(d), ctypes.byref(plan)),
+                       'uppe3d_plan_create')
+        self._plan = plan
+
+    def __del__(self):
+        plan = getattr(self, '_plan', None)
+        if plan is not None and plan.value:
+            self._lib.uppe3d_plan_destroy(plan)
+            self._plan = None
+
+    # ---- state ----------------------------------------------------------------
+    def _as_device_field(self, A0):
+        if isinstance(A0, torch.Tensor):
+            A = A0.to(device=self.device, dtype=self.complex_dtype)
+        else:
+            A = torch.from_numpy(np.ascontiguousarray(A0)).to(self.device).to(self.complex_dtype)
+        A = A.contiguous()
+        if tuple(A.shape) != (self.Nx, self.Ny, self.Nt):
+            raise ValueError(f'A0 must have shape {(self.Nx, self.Ny, self.Nt)}, got {tuple(A.shape)}')
+        return A
+
+    def set_field(self, A0, stream=None):
+        """Load A0 (x, y, t): A_scale = max|A0|, state = A0/A_scale (solver_3d.py:163-170)."""
+        A = self._as_device_field(A0)
+        _lib.check(self._lib.uppe3d_set_field(self._plan, ctypes.c_void_p(A.data_ptr()),
+                                              _lib.stream_ptr(stream)), 'uppe3d_set_field')
+        return A
+
+    def attempt(self, h, stream=None):
+        """One erk43_step of size h from the current state; returns its error."""
+        err = ctypes.c_double()
+        _lib.check(self._lib.uppe3d_attempt(self._plan, float(h), ctypes.byref(err),
+                                            _lib.stream_ptr(stream)), 'uppe3d_attempt')
+        return err.value
+
+    def commit(self, accept, stream=None):
+        _lib.check(self._lib.uppe3d_commit(self._plan, 1 if accept else 0, _lib.stream_ptr(stream)),
+                   'uppe3d_commit')
+
+    def result(self, stream=None):
+        r = _lib.Result3D()
+        _lib.check(self._lib.uppe3d_get_result(self._plan, ctypes.byref(r), _lib.stream_ptr(stream)),
+                   'uppe3d_get_result')
+        return r
+
+    def spectrum(self, out=None, stream=None):
+        """fftshift_t(fft_t(A * A_scale)) of the current state, on the device."""
+        if out is None:
+            out = torch.empty((self.Nx, self.Ny, self.Nt), dtype=self.complex_dtype, device=self.device)
+        _lib.check(self._lib.uppe3d_get_spectrum(self._plan, ctypes.c_void_p(out.data_ptr()),
+                                                 _lib.stream_ptr(stream)), 'uppe3d_get_spectrum')
+        return out
+
+    def field(self, out=None, stream=None):
+        """Time-domain field A(x, y, t) of the current state (physical units)."""
+        if out is None:
+            out = torch.empty((self.Nx, self.Ny, self.Nt), dtype=self.complex_dtype, device=self.device)
+        _lib.check(self._lib.uppe3d_get_field(self._plan, ctypes.c_void_p(out.data_ptr()),
+                                              _lib.stream_ptr(stream)), 'uppe3d_get_field')
+        return out
+
+    # ---- the reference surface ---------------------------------------------------
+    def propagate(self, A0, L, tol=1e-4, max_step=1e-2, min_step=1e-9, return_gpu=False,
+                  max_attempts=0, stream=None, out=None):
+        """solver_3d.py:162-233 -> (z_reached, freq_axis_hz, A_w_final).
+
+        ``out``: optional host tensor (e.g. pinned) that receives the spectrum.
+
+        The adaptive loop runs on the device.  Unlike the reference (which never
+        terminates once the error becomes NaN), a non-finite error stops the run
+        with ``last_result.status & STATUS_NONFINITE`` set.
+        """
+        self.set_field(A0, stream)
+        r = _lib.Result3D()
+        _lib.check(self._lib.uppe3d_propagate(self._plan, float(L), float(tol), float(max_step),
+                                              float(min_step), int(max_attempts), ctypes.byref(r),
+                                              _lib.stream_ptr(stream)), 'uppe3d_propagate')
+        self.last_result = r
+        self.A_scale = r.A_scale
+        A_w = self.spectrum(stream=stream)
+        if return_gpu:
+            return r.z, self.freq_axis_hz, A_w
+        if out is not None:      # caller-provided (e.g. pinned) host buffer
+            out.copy_(A_w)
+            return r.z, self.freq_axis_hz, out.numpy()
+        return r.z, self.freq_axis_hz, A_w.cpu().numpy()

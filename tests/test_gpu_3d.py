@@ -1,0 +1,123 @@
+"""3+1D CUDA path vs the oracle and the reference-generated goldens (GPU)."""
+import numpy as np
+import pytest
+
+from conftest import golden, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+CASES = ['ref3d_mpi_cauchy_double', 'ref3d_adk_taylor_double', 'ref3d_noshock_double']
+
+
+def product_solver(g, precision=None):
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    prec = precision or str(g['precision'])
+    tay = g['taylor']
+    disp = ('taylor', float(tay[0]), float(tay[1]), float(tay[2])) if str(g['lut']) == 'adk' else None
+    med = Argon(float(g['lam']), 1.0, prec, bool(g['shock']), dispersion=disp,
+                lut=(g['log10_I'], g['W_lut']))
+    return ERK43IP_UPPE_3D_Optimized(g['x'], g['y'], g['t'], med, precision=prec)
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_single_attempt_matches_reference(name):
+    g = golden(name)
+    sol = product_solver(g)
+    sol.set_field(g['A0'])
+    err = sol.attempt(float(g['step_h']))
+    assert abs(err - float(g['step_err'])) <= 1e-9 * float(g['step_err'])
+    sol.commit(True)
+    A4 = sol.field().cpu().numpy() / float(g['A_scale'])
+    assert rel_l2(A4, g['step_A4_t']) < 1e-11
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_replay_matches_reference(name):
+    """Replay the reference's (h, accept) sequence: field parity at 1e-10 in c128."""
+    g = golden(name)
+    sol = product_solver(g)
+    sol.set_field(g['A0'])
+    tol = float(g['tol'])
+    for h, err_ref in g['attempts']:
+        err = sol.attempt(h)
+        # errors at round-off level (~1e-16) carry no information beyond their size
+        assert abs(err - err_ref) <= 1e-8 * err_ref + 1e-13 * tol
+        sol.commit(err_ref < tol)
+    A_w = sol.spectrum().cpu().numpy()
+    assert rel_l2(A_w, g['A_w']) < 1e-10
+
+
+@pytest.mark.parametrize('name', CASES)
+def test_free_running_propagate(name):
+    g = golden(name)
+    sol = product_solver(g)
+    z, freq, A_w = sol.propagate(g['A0'], float(g['L']), tol=float(g['tol']))
+    r = sol.last_result
+    assert r.status == 0
+    assert r.attempts == len(g['attempts'])
+    assert abs(z - float(g['z'])) < 1e-12
+    assert np.array_equal(freq, g['freq'])
+    assert rel_l2(A_w, g['A_w']) < 1e-9
+
+
+def test_mixed_precision_vs_fp64_reference():
+    """complex64 bulk + FP64 phase/error/controller against the complex128 reference run."""
+    g = golden('ref3d_mpi_cauchy_double')
+    sol = product_solver(g, precision='single')
+    z, freq, A_w = sol.propagate(g['A0'], float(g['L']), tol=float(g['tol']))
+    assert abs(z - float(g['z'])) < 1e-12
+    assert rel_l2(A_w, g['A_w']) < 1e-4
+
+
+def _oracle_case(N=32, Nt=64, W0=3e9, I_peak=5e16, precision='double', seed=3):
+    from oracle import uppe3d
+    from oracle.inputs import speckle
+    x = np.linspace(-1.5e-3, 1.5e-3, N)
+    t = np.linspace(-100e-15, 100e-15, Nt)
+    lam = 800e-9
+    med = uppe3d.argon(lam, 1.0, precision, True)
+    # MPI-like test table, capped so that it stays finite in float32
+    W = np.minimum(W0 * (10.0 ** med.log10_I_cpu / 5e16) ** 8, 1e20)
+    med.W_gpu = W.astype(med.float_dtype)
+    sol = uppe3d.Solver3D(x, x, t, med, precision)
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    T0 = 40e-15 / (2 * np.sqrt(np.log(2)))
+    A0 = np.sqrt(I_peak) * np.exp(-(X ** 2 + Y ** 2) / (0.5e-3) ** 2)[:, :, None] * \
+        np.exp(-(t / T0) ** 2 / 2)[None, None, :]
+    A0 = (A0 * speckle(x, x, 50e-6, 0.01, seed)[:, :, None]).astype(np.complex128)
+    lut = (med.log10_I_cpu, W)
+    return x, t, lam, A0, sol, lut
+
+
+def test_strong_ionisation_clamped_scan():
+    """Rates above 1/dt make the reference's density clamp bind: the kernel falls
+    back to the exact serial scan for those lines."""
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(W0=1e15, I_peak=5e16)
+    osol.A_scale = float(np.max(np.abs(A0)))
+    An = A0 / osol.A_scale
+    A4o, erro, _, _ = osol.erk43_step(An, 1e-5)
+    med = Argon(lam, 1.0, 'double', True, lut=lut)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='double')
+    sol.set_field(A0)
+    err = sol.attempt(1e-5)
+    assert abs(err - erro) <= 1e-8 * erro
+    sol.commit(True)
+    assert rel_l2(sol.field().cpu().numpy() / osol.A_scale, A4o) < 1e-11
+
+
+def test_larger_grid_attempts_vs_oracle():
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(N=64, Nt=128)
+    z, freq, Ao, log = osol.propagate(A0, 0.02, tol=1e-5, max_attempts=6)
+    med = Argon(lam, 1.0, 'double', True, lut=lut)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='double')
+    sol.set_field(A0)
+    for z0, h, err_o, acc in log:
+        err = sol.attempt(h)
+        assert abs(err - err_o) <= 1e-8 * err_o + 1e-18
+        sol.commit(acc)
+    assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < 1e-10
