@@ -33,6 +33,10 @@ enum {
   UPPE_STATUS_MAX_ATTEMPTS = 4   /* attempt budget exhausted before z = L         */
 };
 
+/* Attempt budget used when a caller passes max_attempts <= 0: every propagation
+ * on the device is bounded.  min_step must be > 0. */
+#define UPPE_DEFAULT_MAX_ATTEMPTS 2000000LL
+
 /* Last error message of this library (thread-global, one line). */
 const char* uppe_last_error(void);
 
@@ -100,7 +104,8 @@ int uppe3d_commit(uppe3d_plan* plan, int accept, uppe_stream_t stream);
 
 /* The adaptive loop of propagate (solver_3d.py:172-208), run on the device:
  * step-size control and acceptance happen in device kernels; the host only
- * polls for completion.  max_attempts <= 0 means unlimited. */
+ * polls for completion.  max_attempts <= 0 means UPPE_DEFAULT_MAX_ATTEMPTS;
+ * tol, max_step and min_step must be > 0. */
 int uppe3d_propagate(uppe3d_plan* plan, double L, double tol, double max_step, double min_step,
                      long long max_attempts, uppe3d_result* result, uppe_stream_t stream);
 /* Split form of uppe3d_propagate for timing: begin, then nsteps graph launches. */
@@ -114,6 +119,59 @@ int uppe3d_get_spectrum(uppe3d_plan* plan, void* out, uppe_stream_t stream);
 /* Time-domain field A(x, y, t) of the current state (physical units), for
  * chaining segments as the reference's drivers do with the returned field. */
 int uppe3d_get_field(uppe3d_plan* plan, void* out, uppe_stream_t stream);
+
+/* -------------------------------------------------------------------- 1D ---- */
+/* One propagation of ERK43IP_UPPE.propagate (src/1D-ERK4(3)IP UPPE gas/
+ * erk43ip_method.py:288-369).  Many instances with different Nt and parameters
+ * run in one persistent launch. */
+typedef struct {
+  int Nt;                  /* power of two: [64,16384] complex64, [64,8192] complex128 */
+  double dt;               /* t[1]-t[0]                                                */
+  double L, tol, max_step, min_step;   /* propagate() arguments (:288)                */
+  long long max_attempts;  /* <= 0: UPPE_DEFAULT_MAX_ATTEMPTS                          */
+  int raman;               /* Raman convolution with H_R (erk43ip_method.py:150-179, 208-215) */
+  int plasma;              /* envelope plasma term with I = |A|^2 / A_eff              */
+  double f_R;
+  double A_eff;            /* [m^2] for the plasma intensity                          */
+  double Ui, sigma_drude, omega0_tau_c, rate_rec, rho_nt, ava_coef;   /* plasma constants */
+  int hist_cap;            /* history slots (the reference saves <= 1501); 0 = none   */
+} uppe1d_inst_desc;
+
+typedef struct {
+  int n_inst;
+  int precision;           /* UPPE_C64 (mixed: FP64 phase/error/controller) or UPPE_C128 */
+  const uppe1d_inst_desc* inst;
+  const double* D;         /* packed complex [sum Nt]: D(omega) = i(k - k0 - k1 w) - alpha/2 (:104-148) */
+  const double* G;         /* packed [sum Nt]: gamma * (w_abs/w0)(n0/n(w)) or gamma (:244-255) */
+  const double* H;         /* packed complex [sum Nt]: H_R(omega), required if any raman */
+  int lut_n;               /* ionisation LUT for the plasma term                       */
+  const double* lut_log10I;
+  const double* lut_W;
+} uppe1d_desc;
+
+typedef struct {
+  double z, h, err;
+  long long attempts, accepted;
+  int status;              /* UPPE_STATUS_* bits; 8 = history capacity reached          */
+  int hist_count;          /* saved history slots (slot 0 = A0)                        */
+} uppe1d_result;
+
+typedef struct uppe1d_plan uppe1d_plan;
+
+/* Replaces ERK43IP_UPPE.__init__ + the cached tables of linear_operator /
+ * nonlinear_operator (erk43ip_method.py:21-70, 104-179): uploads the packed
+ * FP64 tables and allocates the per-CTA scratch. */
+int uppe1d_plan_create(const uppe1d_desc* desc, uppe1d_plan** plan);
+int uppe1d_plan_destroy(uppe1d_plan* plan);
+long long uppe1d_field_elems(const uppe1d_plan* plan);   /* sum Nt                   */
+long long uppe1d_hist_elems(const uppe1d_plan* plan);    /* sum hist_cap * Nt        */
+long long uppe1d_hist_slots(const uppe1d_plan* plan);    /* sum hist_cap             */
+/* propagate (erk43ip_method.py:288-369) for every instance.  field: device,
+ * packed time-domain A0 in, final A out; hist/zhist: device history fields and z
+ * values (NULL when no instance keeps history); results: host array [n_inst]
+ * (the call synchronises the stream when results is not NULL). */
+int uppe1d_propagate(uppe1d_plan* plan, void* field, void* hist, double* zhist,
+                     uppe1d_result* results, uppe_stream_t stream);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);

@@ -35,6 +35,26 @@ class Result3D(ctypes.Structure):
                 ('fail_count', _I), ('status', _I), ('A_scale', _D)]
 
 
+class InstDesc1D(ctypes.Structure):
+    _fields_ = [('Nt', _I), ('dt', _D), ('L', _D), ('tol', _D), ('max_step', _D),
+                ('min_step', _D), ('max_attempts', _LL), ('raman', _I), ('plasma', _I),
+                ('f_R', _D), ('A_eff', _D), ('Ui', _D), ('sigma_drude', _D),
+                ('omega0_tau_c', _D), ('rate_rec', _D), ('rho_nt', _D), ('ava_coef', _D),
+                ('hist_cap', _I)]
+
+
+class Desc1D(ctypes.Structure):
+    _fields_ = [('n_inst', _I), ('precision', _I), ('inst', ctypes.POINTER(InstDesc1D)),
+                ('D', _P), ('G', _P), ('H', _P), ('lut_n', _I), ('lut_log10I', _P), ('lut_W', _P)]
+
+
+class Result1D(ctypes.Structure):
+    _fields_ = [('z', _D), ('h', _D), ('err', _D), ('attempts', _LL), ('accepted', _LL),
+                ('status', _I), ('hist_count', _I)]
+
+
+STATUS_HIST_FULL = 8
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     'uppe_last_error': (ctypes.c_char_p, []),
@@ -51,6 +71,12 @@ SIGNATURES = {
     'uppe3d_get_spectrum': (_I, [_P, _P, _P]),
     'uppe3d_get_field': (_I, [_P, _P, _P]),
     'uppe3d_launches_per_step': (_I, [_P]),
+    'uppe1d_plan_create': (_I, [ctypes.POINTER(Desc1D), ctypes.POINTER(_P)]),
+    'uppe1d_plan_destroy': (_I, [_P]),
+    'uppe1d_field_elems': (_LL, [_P]),
+    'uppe1d_hist_elems': (_LL, [_P]),
+    'uppe1d_hist_slots': (_LL, [_P]),
+    'uppe1d_propagate': (_I, [_P, _P, _P, _P, ctypes.POINTER(Result1D), _P]),
     'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),
                                     ctypes.POINTER(_D), ctypes.POINTER(_I), _P]),
 }

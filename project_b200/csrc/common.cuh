@@ -132,11 +132,11 @@ __device__ __forceinline__ void stockham(C* s, const C* tw, int tid, IDX idx, SY
     constexpr int B = E / R;
     constexpr int M = N / R;   // butterflies per signal
     C v[B][R];
-    // threads with tid >= NTHR (a team padded to a full warp) only synchronise
+    // threads with tid >= NTHR (a team padded to a full warp/block) only synchronise
     const bool act = tid < NTHR;
+    if (act) {
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      if (!act) break;
       const int bf = tid + b * NTHR;
       const int sig = bf % NSIG, j = bf / NSIG;
       const int k = j & (Ns - 1);
@@ -152,16 +152,18 @@ __device__ __forceinline__ void stockham(C* s, const C* tw, int tid, IDX idx, SY
       }
       DFT<R, DIR, C>::run(v[b]);
     }
+    }
     sync();
+    if (act) {
 #pragma unroll
     for (int b = 0; b < B; ++b) {
-      if (!act) break;
       const int bf = tid + b * NTHR;
       const int sig = bf % NSIG, j = bf / NSIG;
       const int k = j & (Ns - 1);
       const int base = (j / Ns) * Ns * R + k;
 #pragma unroll
       for (int r = 0; r < R; ++r) s[idx(sig, base + r * Ns)] = v[b][r];
+    }
     }
     sync();
     stockham<N, NSIG, NTHR, DIR, Ns * R, C>(s, tw, tid, idx, sync);

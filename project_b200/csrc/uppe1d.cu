@@ -1,0 +1,205 @@
+// Host side of the 1D propagator: plan (tables, twiddles, scratch) and launch.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "uppe1d_kernel.cuh"
+
+extern char g_uppe_err[512];
+
+using namespace uppe;
+
+struct uppe1d_plan {
+  int dbl;
+  size_t csz;
+  int ninst;
+  int nmax;
+  long long ftotal;       // sum Nt
+  long long htotal;       // sum hist_cap * Nt
+  long long zhtotal;      // sum hist_cap
+  int nblocks;
+  size_t smem;
+  Batch1D b;
+  Inst1D* d_inst;
+  std::vector<Inst1D> h_inst;
+  std::vector<void*> allocs;
+  Res1D* h_res;
+};
+
+#define UPPE1_CK(x)                                                                \
+  do {                                                                             \
+    cudaError_t e_ = (x);                                                          \
+    if (e_ != cudaSuccess) {                                                       \
+      snprintf(g_uppe_err, sizeof(g_uppe_err), "%s:%d %s: %s", __FILE__, __LINE__, \
+               #x, cudaGetErrorString(e_));                                        \
+      return UPPE_ERR_CUDA;                                                        \
+    }                                                                              \
+  } while (0)
+
+static int up1(uppe1d_plan* p, void** dst, const void* src, size_t bytes) {
+  UPPE1_CK(cudaMalloc(dst, bytes));
+  p->allocs.push_back(*dst);
+  if (src) UPPE1_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  return 0;
+}
+
+extern "C" int uppe1d_plan_destroy(uppe1d_plan* p) {
+  if (!p) return 0;
+  for (void* a : p->allocs) cudaFree(a);
+  if (p->h_res) cudaFreeHost(p->h_res);
+  delete p;
+  return 0;
+}
+
+extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
+  *out = nullptr;
+  g_uppe_err[0] = 0;
+  if (!d || d->n_inst <= 0 || !d->inst || !d->D || !d->G) return UPPE_ERR_ARG;
+  if (d->precision != UPPE_C64 && d->precision != UPPE_C128) return UPPE_ERR_ARG;
+  const int dbl = d->precision == UPPE_C128;
+  const int nmax_allowed = dbl ? 8192 : 16384;
+  uppe1d_plan* p = new uppe1d_plan();
+  p->dbl = dbl;
+  p->csz = dbl ? 16 : 8;
+  p->ninst = d->n_inst;
+  p->h_inst.resize(d->n_inst);
+  long long off = 0, hoff = 0, zoff = 0;
+  int nmax = 0;
+  bool any_raman = false;
+  for (int i = 0; i < d->n_inst; ++i) {
+    const uppe1d_inst_desc& s = d->inst[i];
+    const int n = s.Nt;
+    if (n < 64 || n > nmax_allowed || (n & (n - 1))) {
+      snprintf(g_uppe_err, sizeof(g_uppe_err),
+               "instance %d: Nt=%d unsupported (power of two in [64, %d] for this precision)", i, n,
+               nmax_allowed);
+      delete p;
+      return UPPE_ERR_SIZE;
+    }
+    if (!(s.L >= 0.0) || !(s.tol > 0.0) || !(s.max_step > 0.0) || !(s.min_step > 0.0) ||
+        s.hist_cap < 0 || (s.plasma && !(s.A_eff > 0.0))) {
+      snprintf(g_uppe_err, sizeof(g_uppe_err), "instance %d: invalid L/tol/step/history/A_eff", i);
+      delete p;
+      return UPPE_ERR_ARG;
+    }
+    Inst1D& q = p->h_inst[i];
+    q.Nt = n;
+    q.log2n = 31 - __builtin_clz((unsigned)n);
+    q.dt = s.dt; q.L = s.L; q.tol = s.tol; q.max_step = s.max_step; q.min_step = s.min_step;
+    q.off = off; q.hist_off = hoff; q.zh_off = zoff; q.hist_cap = s.hist_cap;
+    // a bounded run: the device loop always ends (default cap when none is given)
+    q.max_attempts = s.max_attempts > 0 ? s.max_attempts : UPPE_DEFAULT_MAX_ATTEMPTS;
+    q.raman = s.raman; q.plasma = s.plasma; q.f_R = s.f_R; q.A_eff = s.A_eff;
+    q.pc.Ui = s.Ui; q.pc.sigma_half = s.sigma_drude / 2.0; q.pc.w0tc = s.omega0_tau_c;
+    q.pc.rr = (double)(float)s.rate_rec; q.pc.dt = (double)(float)s.dt;
+    q.pc.rho_nt = (double)(float)s.rho_nt; q.pc.ava = s.ava_coef;
+    any_raman |= s.raman != 0;
+    off += n;
+    hoff += (long long)s.hist_cap * n;
+    zoff += s.hist_cap;
+    nmax = std::max(nmax, n);
+  }
+  if (any_raman && !d->H) { delete p; return UPPE_ERR_ARG; }
+  for (int i = 0; i < d->n_inst; ++i)
+    if (d->inst[i].plasma && (d->lut_n < 2 || !d->lut_log10I || !d->lut_W)) { delete p; return UPPE_ERR_ARG; }
+  p->ftotal = off; p->htotal = hoff; p->zhtotal = zoff; p->nmax = nmax;
+  int rc;
+#define TRY1(x) do { rc = (x); if (rc) { uppe1d_plan_destroy(p); return rc; } } while (0)
+  void* ptr;
+  TRY1(up1(p, &ptr, p->h_inst.data(), sizeof(Inst1D) * p->ninst)); p->d_inst = (Inst1D*)ptr;
+  TRY1(up1(p, &ptr, d->D, 16 * (size_t)off)); p->b.D = (const double2*)ptr;
+  TRY1(up1(p, &ptr, d->G, 8 * (size_t)off)); p->b.G = (const double*)ptr;
+  p->b.H = nullptr;
+  if (any_raman) { TRY1(up1(p, &ptr, d->H, 16 * (size_t)off)); p->b.H = (const double2*)ptr; }
+  // order: longest instances first (largest Nt, then longest L)
+  std::vector<int> order(p->ninst);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b2) {
+    const double ca = (double)p->h_inst[a].Nt * p->h_inst[a].L, cb = (double)p->h_inst[b2].Nt * p->h_inst[b2].L;
+    return ca > cb;
+  });
+  TRY1(up1(p, &ptr, order.data(), sizeof(int) * p->ninst)); p->b.order = (const int*)ptr;
+  TRY1(up1(p, &ptr, nullptr, sizeof(int))); p->b.counter = (int*)ptr;
+  TRY1(up1(p, &ptr, nullptr, sizeof(Res1D) * p->ninst)); p->b.res = (Res1D*)ptr;
+  {
+    cudaError_t e = cudaMallocHost(&p->h_res, sizeof(Res1D) * p->ninst);
+    if (e != cudaSuccess) { uppe1d_plan_destroy(p); return UPPE_ERR_CUDA; }
+  }
+  // packed twiddles: for every N = 2^k <= nmax, exp(-2 pi i m / N) at offset N - 1
+  {
+    std::vector<unsigned char> tw(p->csz * (size_t)(2 * nmax));
+    for (int n = 1; n <= nmax; n *= 2) {
+      for (int m = 0; m < n; ++m) {
+        const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
+        const double cr = (double)cosl(ang), ci = (double)sinl(ang);
+        if (dbl) { ((double2*)tw.data())[n - 1 + m] = make_double2(cr, ci); }
+        else { ((float2*)tw.data())[n - 1 + m] = make_float2((float)cr, (float)ci); }
+      }
+    }
+    TRY1(up1(p, &ptr, tw.data(), tw.size())); p->b.tw = ptr;
+  }
+  if (d->lut_n >= 2 && d->lut_log10I && d->lut_W) {
+    const int n = d->lut_n;
+    std::vector<unsigned char> lx(n * (dbl ? 8 : 4)), lw(n * (dbl ? 8 : 4));
+    for (int i = 0; i < n; ++i) {
+      if (dbl) { ((double*)lx.data())[i] = d->lut_log10I[i]; ((double*)lw.data())[i] = d->lut_W[i]; }
+      else { ((float*)lx.data())[i] = (float)d->lut_log10I[i]; ((float*)lw.data())[i] = (float)d->lut_W[i]; }
+    }
+    TRY1(up1(p, &ptr, lx.data(), lx.size())); p->b.lut.x = ptr;
+    TRY1(up1(p, &ptr, lw.data(), lw.size())); p->b.lut.w = ptr;
+    p->b.lut.n = n;
+    p->b.lut.x0 = d->lut_log10I[0];
+    p->b.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
+  } else {
+    p->b.lut.x = p->b.lut.w = nullptr;
+    p->b.lut.n = 0;
+  }
+  int dev = 0, nsm = 148;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  p->nblocks = std::min(p->ninst, nsm);
+  p->b.scratch_per_block = 7LL * nmax;
+  TRY1(up1(p, &ptr, nullptr, p->csz * (size_t)p->b.scratch_per_block * p->nblocks)); p->b.scratch = ptr;
+  p->smem = p->csz * (size_t)(nmax + nmax / 32) + sizeof(double) * (64 + T1);
+  p->b.inst = p->d_inst;
+  p->b.ninst = p->ninst;
+#undef TRY1
+  *out = p;
+  return 0;
+}
+
+extern "C" long long uppe1d_field_elems(const uppe1d_plan* p) { return p ? p->ftotal : 0; }
+extern "C" long long uppe1d_hist_elems(const uppe1d_plan* p) { return p ? p->htotal : 0; }
+extern "C" long long uppe1d_hist_slots(const uppe1d_plan* p) { return p ? p->zhtotal : 0; }
+
+extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double* zhist,
+                                uppe1d_result* results, cudaStream_t s) {
+  if (!p || !field) return UPPE_ERR_ARG;
+  if (p->htotal > 0 && (!hist || !zhist)) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err), "plan has history slots: hist and zhist are required");
+    return UPPE_ERR_ARG;
+  }
+  Batch1D b = p->b;
+  b.field = field;
+  b.hist = hist;
+  b.zhist = zhist;
+  UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
+  UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s)
+                   : launch_uppe1d<float>(b, p->nblocks, p->smem, s));
+  if (results) {
+    UPPE1_CK(cudaMemcpyAsync(p->h_res, p->b.res, sizeof(Res1D) * p->ninst, cudaMemcpyDeviceToHost, s));
+    UPPE1_CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < p->ninst; ++i) {
+      const Res1D& r = p->h_res[i];
+      results[i].z = r.z; results[i].h = r.h; results[i].err = r.err;
+      results[i].attempts = r.attempts; results[i].accepted = r.accepted;
+      results[i].status = r.status; results[i].hist_count = r.hist_count;
+    }
+  }
+  return 0;
+}

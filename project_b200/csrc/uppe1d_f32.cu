@@ -1,0 +1,13 @@
+// float instantiation of the 1D persistent kernel (compiled separately so the
+// two precisions build in parallel).
+#include "uppe1d_kernel.cuh"
+
+namespace uppe {
+template <>
+cudaError_t launch_uppe1d<float>(const Batch1D& b, int nblocks, size_t smem, cudaStream_t s) {
+  cudaError_t e = cudaFuncSetAttribute(k_uppe1d<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  k_uppe1d<float><<<nblocks, T1, smem, s>>>(b);
+  return cudaGetLastError();
+}
+}  // namespace uppe

@@ -1,0 +1,493 @@
+#pragma once
+// 1D ERK4(3)-IP UPPE/GNLSE propagator, batched and persistent, sm_100a.
+//
+// Replaces ERK43IP_UPPE.propagate / erk43_step / linear_operator /
+// nonlinear_operator (src/1D-ERK4(3)IP UPPE gas/erk43ip_method.py:181-369).
+//
+// One launch propagates a whole batch: each CTA pulls instances from a device
+// work queue (longest first) and runs the complete adaptive loop of one
+// instance on the device -- no host round trip per step.  The state is held in
+// the omega domain, so exp(h/2 D) is a diagonal factor computed on the fly from
+// the FP64 D(omega) table, and each nonlinear evaluation is one inverse FFT,
+// the pointwise Kerr (+ Raman, + plasma) term and one forward FFT, all on a line
+// resident in shared memory (Stockham, Nt <= 16384 complex64 / 8192 complex128).
+// The stage arrays live in a per-CTA global scratch that stays in L2.
+// FSAL: alpha5 of an accepted step is the next step's N(A) (bit-identical to
+// recomputing it, which the reference does whenever h changes).
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <numeric>
+#include <vector>
+
+#include "common.cuh"
+#include "../../include/uppe_b200.h"
+
+namespace uppe {
+
+constexpr int T1 = 512;   // threads per CTA
+
+struct Inst1D {
+  int Nt, log2n;
+  double dt, L, tol, max_step, min_step;
+  long long off;         // element offset in the packed field/table arrays
+  long long hist_off;    // element offset of the history slots
+  long long zh_off;      // offset of the history z values
+  int hist_cap;
+  long long max_attempts;
+  int raman, plasma;
+  double f_R, A_eff;
+  PlasmaConst pc;
+};
+
+struct Res1D {
+  double z, h, err;
+  long long attempts, accepted;
+  int status, hist_count;
+};
+
+struct Batch1D {
+  const Inst1D* inst;
+  Res1D* res;
+  const int* order;
+  int* counter;
+  int ninst;
+  const double2* D;
+  const double* G;
+  const double2* H;
+  void* field;
+  void* hist;
+  double* zhist;
+  void* scratch;
+  long long scratch_per_block;   // complex elements
+  const void* tw;                // packed twiddles: size N at offset N-1
+  Lut lut;
+};
+
+template <int N> struct Cfg1 {
+  static constexpr int FT = N / 2 < T1 ? N / 2 : T1;   // FFT team size
+  static constexpr int PAD = N + N / 32;
+  static constexpr int CH = N >= T1 ? N / T1 : 1;      // density-scan chunk per thread
+  static constexpr int NA = N / CH;                    // threads owning a chunk
+};
+
+static __device__ __forceinline__ int pad1(int n) { return n + (n >> 5); }
+struct Idx1 {
+  __device__ __forceinline__ int operator()(int, int n) const { return pad1(n); }
+};
+struct Sync1 {
+  __device__ __forceinline__ void operator()() const { __syncthreads(); }
+};
+
+static __device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// deterministic block sum (fixed order)
+static __device__ double block_sum(double v, double* red) {
+  const int tid = threadIdx.x;
+  v = warp_sum(v);
+  if ((tid & 31) == 0) red[tid >> 5] = v;
+  __syncthreads();
+  if (tid < 32) {
+    double t = tid < T1 / 32 ? red[tid] : 0.0;
+    t = warp_sum(t);
+    if (tid == 0) red[T1 / 32] = t;
+  }
+  __syncthreads();
+  const double r = red[T1 / 32];
+  __syncthreads();
+  return r;
+}
+
+// exp(hh * D[w]) with D the FP64 dispersion table (erk43ip_method.py:194)
+template <typename Rl> struct EFac;
+template <> struct EFac<double> {
+  __device__ __forceinline__ static double2 get(double2 D, double hh) {
+    double s, c;
+    sincos(hh * D.y, &s, &c);
+    const double m = exp(hh * D.x);
+    return make_double2(m * c, m * s);
+  }
+};
+template <> struct EFac<float> {
+  __device__ __forceinline__ static float2 get(double2 D, double hh) {
+    double ph = hh * D.y;
+    const double twopi = 6.283185307179586476925286766559;
+    ph = ph - twopi * rint(ph * (1.0 / twopi));
+    float s, c;
+    sincosf((float)ph, &s, &c);
+    const float m = expf((float)(hh * D.x));
+    return make_float2(m * c, m * s);
+  }
+};
+
+enum In1 { IN_A = 0, IN_2, IN_3, IN_4, IN_5 };
+
+template <typename Rl> struct Ctx1 {
+  using C = typename CT<Rl>::T;
+  C* s;
+  double* red;
+  double* starts;
+  const C* tw;
+  C *A, *K1, *T, *O, *A4, *A4P, *GA;
+  const double2* D;
+  const double* G;
+  const double2* H;
+  const Inst1D* in;
+  Lut lut;
+};
+
+// plasma term P(t) = (loss + defocus)(t) * a(t) into the shared line, from the
+// time-domain field in GA (media_physics.py:156-203 with I = |A|^2 / A_eff).
+// Returns false (nothing written) when the whole line has W_ion = 0 and no
+// avalanche, i.e. the term is identically zero.
+template <typename Rl, int N>
+__device__ bool plasma_line(Ctx1<Rl>& c) {
+  using C = typename CT<Rl>::T;
+  constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
+  const int tid = threadIdx.x;
+  const PlasmaConst& m = c.in->pc;
+  const double Aeff = c.in->A_eff;
+  const AffineStep aff(m);
+  bool any_w = false, ok = (m.ava == 0.0);
+  double cm = 1.0, dm = 0.0;
+  if (tid < NA) {
+    for (int t = tid * CH; t < tid * CH + CH; ++t) {
+      const C a = c.GA[t];
+      const Rl I = (Rl)(((double)a.x * a.x + (double)a.y * a.y) / Aeff);
+      const double w = (double)(float)lut_eval<Rl>(c.lut, I);
+      any_w |= (w != 0.0);
+      const double cc = aff.e - w * aff.sf;
+      ok &= (cc >= 0.0);
+      dm = cc * dm + w * m.rho_nt * aff.sf;
+      cm = cc * cm;
+    }
+  }
+  const bool any_block = __syncthreads_or(any_w) || m.ava != 0.0;
+  if (!any_block) return false;
+  const bool all_ok = __syncthreads_and(ok);
+  double rho0;
+  if (all_ok) {
+    // block exclusive scan of affine maps (c1,d1) then (c2,d2) = (c1 c2, c2 d1 + d2)
+    const int lane = tid & 31, warp = tid >> 5;
+    double cc = cm, dd = dm;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double cp = __shfl_up_sync(0xffffffffu, cc, off);
+      const double dp = __shfl_up_sync(0xffffffffu, dd, off);
+      if (lane >= off) { dd = cc * dp + dd; cc = cc * cp; }
+    }
+    double* wc = c.starts;            // warp totals
+    double* wd = c.starts + T1 / 32;
+    if (lane == 31) { wc[warp] = cc; wd[warp] = dd; }
+    __syncthreads();
+    if (tid == 0) {
+      double C0 = 1.0, D0 = 0.0;      // exclusive prefix over warps (applied to rho = 0)
+      for (int w = 0; w < T1 / 32; ++w) {
+        const double c2 = wc[w], d2 = wd[w];
+        wc[w] = C0; wd[w] = D0;
+        D0 = c2 * D0 + d2;
+        C0 = C0 * c2;
+      }
+    }
+    __syncthreads();
+    double ce = __shfl_up_sync(0xffffffffu, cc, 1);
+    double de = __shfl_up_sync(0xffffffffu, dd, 1);
+    if (lane == 0) { ce = 1.0; de = 0.0; }
+    rho0 = ce * wd[warp] + de;
+    __syncthreads();
+  } else {
+    if (tid == 0) {
+      double rho = 0.0;
+      for (int t = 0; t < N; ++t) {
+        if (t % CH == 0) c.starts[t / CH] = rho;
+        const C a = c.GA[t];
+        const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
+        const double w = (double)(float)lut_eval<Rl>(c.lut, (Rl)Id);
+        const double wa = (double)(float)(m.ava * (double)(Rl)Id);
+        rho_step(rho, w, wa, m);
+      }
+    }
+    __syncthreads();
+    rho0 = tid < NA ? c.starts[tid] : 0.0;
+    __syncthreads();
+  }
+  if (tid < NA) {
+    double rho = rho0;
+    for (int t = tid * CH; t < tid * CH + CH; ++t) {
+      const C a = c.GA[t];
+      const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
+      const Rl I = (Rl)Id;
+      const double w = (double)(float)lut_eval<Rl>(c.lut, I);
+      const double wa = (double)(float)(m.ava * (double)I);
+      const double rho_t = rho;
+      const double gen = rho_step(rho, w, wa, m);
+      const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
+      const double cr = loss - m.sigma_half * rho_t;
+      const double ci = -m.sigma_half * m.w0tc * rho_t;
+      c.s[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
+    }
+  }
+  __syncthreads();
+  return true;
+}
+
+// One nonlinear evaluation N(u) in the omega domain (erk43ip_method.py:197-255
+// plus the plasma term), with the stage input u formed on the fly.
+// Returns sum |u|^2 for IN_5 (else 0).
+template <typename Rl, int N>
+__device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename CT<Rl>::T* out,
+                          typename CT<Rl>::T* hist_t) {
+  using C = typename CT<Rl>::T;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const Rl hR = (Rl)h, h2 = (Rl)(h / 2), h6 = (Rl)(h / 6);
+  double nrm = 0.0;
+  for (int w = tid; w < N; w += T1) {
+    C u;
+    if (mode == IN_A) {
+      u = c.A[w];
+    } else if (mode == IN_5) {
+      u = cadd(c.T[w], cscale(c.A4P[w], h6));
+      c.A4[w] = u;
+      nrm += (double)u.x * u.x + (double)u.y * u.y;
+    } else {
+      const C E = EFac<Rl>::get(c.D[w], 0.5 * h);
+      const C v = cmul(c.A[w], E);
+      if (mode == IN_2) {
+        const C a1 = cmul(c.K1[w], E);
+        c.T[w] = a1;
+        u = cadd(v, cscale(a1, h2));
+      } else if (mode == IN_3) {
+        const C o = c.O[w];
+        c.T[w] = cadd(c.T[w], cscale(o, (Rl)2));
+        u = cadd(v, cscale(o, h2));
+      } else {   // IN_4
+        const C o = c.O[w];
+        const C ts = cadd(c.T[w], cscale(o, (Rl)2));
+        c.T[w] = cmul(cadd(v, cscale(ts, h6)), E);    // beta
+        u = cmul(cadd(v, cscale(o, hR)), E);
+      }
+    }
+    c.s[pad1(w)] = u;
+  }
+  __syncthreads();
+  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  const Rl invN = (Rl)(1.0 / N);
+  const bool raman = c.in->raman, plasma = c.in->plasma;
+  for (int t = tid; t < N; t += T1) {
+    const C a = cscale(c.s[pad1(t)], invN);
+    if (raman || plasma) c.GA[t] = a;
+    if (hist_t) hist_t[t] = a;
+    if (raman) {
+      c.s[pad1(t)] = C{a.x * a.x + a.y * a.y, (Rl)0};
+    } else {
+      const Rl I = a.x * a.x + a.y * a.y;
+      c.s[pad1(t)] = cscale(a, I);
+    }
+  }
+  __syncthreads();
+  if (raman) {
+    // I_eff = (1 - f_R) I + f_R ifft(H_R fft(I))   (erk43ip_method.py:208-215)
+    stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    for (int w = tid; w < N; w += T1) {
+      const double2 Hw = c.H[w];
+      c.s[pad1(w)] = cmul(c.s[pad1(w)], C{(Rl)Hw.x, (Rl)Hw.y});
+    }
+    __syncthreads();
+    stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    const Rl fR = (Rl)c.in->f_R, g1 = (Rl)(1.0 - c.in->f_R);
+    for (int t = tid; t < N; t += T1) {
+      const C a = c.GA[t];
+      const Rl I = a.x * a.x + a.y * a.y;
+      const C Id = cscale(c.s[pad1(t)], invN);
+      const C Ieff = C{g1 * I + fR * Id.x, fR * Id.y};
+      c.s[pad1(t)] = cmul(a, Ieff);
+    }
+    __syncthreads();
+  }
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) {
+    const C p = c.s[pad1(w)];
+    const Rl g = (Rl)c.G[w];
+    out[w] = C{-g * p.y, g * p.x};     // i gamma U(w) P_NL(w)
+  }
+  __syncthreads();
+  if (plasma) {
+    if (plasma_line<Rl, N>(c)) {
+      stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+      for (int w = tid; w < N; w += T1) out[w] = cadd(out[w], c.s[pad1(w)]);
+      __syncthreads();
+    }
+  }
+  return mode == IN_5 ? block_sum(nrm, c.red) : 0.0;
+}
+
+// one erk43_step from the state (A, K1); leaves A4, a4' (A4P), a5 (O), beta (T);
+// returns the error of erk43ip_method.py:279-284
+template <typename Rl, int N>
+__device__ __noinline__ double attempt1(Ctx1<Rl>& c, double h, typename CT<Rl>::T* hist_t) {
+  using C = typename CT<Rl>::T;
+  const int tid = threadIdx.x;
+  nl_eval<Rl, N>(c, IN_2, h, c.O, nullptr);     // alpha2
+  nl_eval<Rl, N>(c, IN_3, h, c.O, nullptr);     // alpha3
+  nl_eval<Rl, N>(c, IN_4, h, c.A4P, nullptr);   // alpha4'
+  const double nrm = nl_eval<Rl, N>(c, IN_5, h, c.O, hist_t);   // alpha5' = N(A4)
+  double acc = 0.0;
+  const Rl h30 = (Rl)(h / 30);
+  for (int w = tid; w < N; w += T1) {
+    if (sizeof(Rl) == 8) {
+      const C a4 = c.A4P[w], a5 = c.O[w];
+      const C A3 = cadd(c.T[w], cscale(cadd(cscale(a4, (Rl)2), cscale(a5, (Rl)3)), h30));
+      const C d = csub(c.A4[w], A3);
+      acc += (double)d.x * d.x + (double)d.y * d.y;
+    } else {
+      const C a4 = c.A4P[w], a5 = c.O[w];
+      const double dx = (double)a4.x - a5.x, dy = (double)a4.y - a5.y;
+      acc += dx * dx + dy * dy;
+    }
+  }
+  double num = block_sum(acc, c.red);
+  if (sizeof(Rl) != 8) num *= (h / 10.0) * (h / 10.0);
+  double normA = sqrt(nrm / N);          // time-domain norm by Parseval
+  if (normA < 1e-20) normA = 1.0;
+  return sqrt(num / N) / normA;
+}
+
+template <typename Rl, int N>
+__device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
+  using C = typename CT<Rl>::T;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const Inst1D& in = b.inst[i];
+  Ctx1<Rl> c;
+  c.s = reinterpret_cast<C*>(smem);
+  c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
+  c.starts = c.red + 64;
+  c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
+  C* sc = reinterpret_cast<C*>(b.scratch) + (long long)blockIdx.x * b.scratch_per_block;
+  c.A = sc; c.K1 = sc + N; c.T = sc + 2 * N; c.O = sc + 3 * N;
+  c.A4 = sc + 4 * N; c.A4P = sc + 5 * N; c.GA = sc + 6 * N;
+  c.D = b.D + in.off;
+  c.G = b.G + in.off;
+  c.H = b.H ? b.H + in.off : nullptr;
+  c.in = &in;
+  c.lut = b.lut;
+  C* field = reinterpret_cast<C*>(b.field) + in.off;
+  C* hist = in.hist_cap > 0 ? reinterpret_cast<C*>(b.hist) + in.hist_off : nullptr;
+  double* zh = in.hist_cap > 0 ? b.zhist + in.zh_off : nullptr;
+
+  // A0 -> history slot 0, state = fft(A0)
+  for (int t = tid; t < N; t += T1) {
+    const C a = field[t];
+    c.s[pad1(t)] = a;
+    if (hist) hist[t] = a;
+  }
+  if (zh && tid == 0) zh[0] = 0.0;
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
+  __syncthreads();
+  nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr);   // k1 = N(A)
+
+  // adaptive loop (erk43ip_method.py:294-367), evaluated identically by all threads
+  const double L = in.L, tol = in.tol, max_step = in.max_step, min_step = in.min_step;
+  double z = 0.0, h = max_step / 100, err = 0.0, err_prev = -1.0, zlast = 0.0;
+  long long attempts = 0, accepted = 0;
+  int status = 0, hcount = 1;
+  auto cand = [&]() -> C* { return (hist && hcount < in.hist_cap) ? hist + (long long)hcount * N : nullptr; };
+  auto accept = [&](double hh) {
+    z += hh;
+    C* t0 = c.A; c.A = c.A4; c.A4 = t0;     // state <- A4
+    C* t1 = c.K1; c.K1 = c.O; c.O = t1;     // k1 <- alpha5' (FSAL)
+    accepted += 1;
+    if (hcount < 1000 || (z - zlast) > L / 500) {   // :327
+      if (hist && hcount < in.hist_cap) {
+        if (tid == 0) zh[hcount] = z;
+        hcount += 1;
+        zlast = z;
+      } else if (hist) {
+        status |= 8;   // history capacity exhausted
+      }
+    }
+  };
+  while (z < L) {
+    if (z + h > L) h = L - z;
+    err = attempt1<Rl, N>(c, h, cand());
+    attempts += 1;
+    if (!isfinite(err) || !isfinite(h)) { status |= UPPE_STATUS_NONFINITE; break; }
+    if (err < tol) {
+      accept(h);
+      double factor = 0.95 * pow(tol / (err + 1e-30), 0.25);
+      if (err_prev >= 0.0 && err_prev > 1e-30) factor *= pow(err_prev / (err + 1e-30), 0.1);
+      err_prev = err;
+      h = fmin(h * fmin(factor, 2.0), max_step);
+    } else {
+      const double factor = 0.95 * pow(tol / (err + 1e-30), 0.25);
+      h = fmax(h * fmax(factor, 0.1), min_step);
+      if (h <= min_step) {   // forced step (:345-367)
+        err = attempt1<Rl, N>(c, h, cand());
+        attempts += 1;
+        status |= UPPE_STATUS_MIN_STEP;
+        if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
+        accept(h);
+        err_prev = -1.0;
+      }
+    }
+    if (in.max_attempts > 0 && attempts >= in.max_attempts && z < L) {
+      status |= UPPE_STATUS_MAX_ATTEMPTS;
+      break;
+    }
+  }
+  // final state back to the time domain
+  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+  __syncthreads();
+  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  const Rl invN = (Rl)(1.0 / N);
+  for (int t = tid; t < N; t += T1) field[t] = cscale(c.s[pad1(t)], invN);
+  if (tid == 0) {
+    Res1D r;
+    r.z = z; r.h = h; r.err = err; r.attempts = attempts; r.accepted = accepted;
+    r.status = status; r.hist_count = hist ? hcount : 0;
+    b.res[i] = r;
+  }
+  __syncthreads();
+}
+
+template <typename Rl>
+__global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ int s_k;
+  for (;;) {
+    if (threadIdx.x == 0) s_k = atomicAdd(b.counter, 1);
+    __syncthreads();
+    const int k = s_k;
+    __syncthreads();
+    if (k >= b.ninst) return;
+    const int i = b.order[k];
+    switch (b.inst[i].log2n) {
+      case 6: run_instance<Rl, 64>(b, i, smem); break;
+      case 7: run_instance<Rl, 128>(b, i, smem); break;
+      case 8: run_instance<Rl, 256>(b, i, smem); break;
+      case 9: run_instance<Rl, 512>(b, i, smem); break;
+      case 10: run_instance<Rl, 1024>(b, i, smem); break;
+      case 11: run_instance<Rl, 2048>(b, i, smem); break;
+      case 12: run_instance<Rl, 4096>(b, i, smem); break;
+      case 13: run_instance<Rl, 8192>(b, i, smem); break;
+      case 14: if (sizeof(Rl) == 4) run_instance<Rl, 16384>(b, i, smem); break;
+      default: break;
+    }
+  }
+}
+
+// launcher implemented once per precision (uppe1d_f32.cu / uppe1d_f64.cu)
+template <typename Rl> cudaError_t launch_uppe1d(const Batch1D& b, int nblocks, size_t smem, cudaStream_t s);
+
+}  // namespace uppe
+

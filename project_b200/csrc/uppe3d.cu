@@ -1110,7 +1110,8 @@ static void fill_result(const State3D* h, uppe3d_result* r) {
 extern "C" int uppe3d_propagate(uppe3d_plan* p, double L, double tol, double max_step,
                                 double min_step, long long max_attempts, uppe3d_result* res,
                                 cudaStream_t s) {
-  if (!p) return UPPE_ERR_ARG;
+  if (!p || !(tol > 0.0) || !(max_step > 0.0) || !(min_step > 0.0) || !(L >= 0.0)) return UPPE_ERR_ARG;
+  if (max_attempts <= 0) max_attempts = UPPE_DEFAULT_MAX_ATTEMPTS;
   k_begin<<<1, 1, 0, s>>>(p->st, L, tol, max_step, min_step, max_attempts);
   UPPE_CK(cudaGetLastError());
   int batch = 1;
@@ -1133,7 +1134,8 @@ extern "C" int uppe3d_run_steps(uppe3d_plan* p, int nsteps, cudaStream_t s) {
 
 extern "C" int uppe3d_begin(uppe3d_plan* p, double L, double tol, double max_step,
                             double min_step, long long max_attempts, cudaStream_t s) {
-  if (!p) return UPPE_ERR_ARG;
+  if (!p || !(tol > 0.0) || !(max_step > 0.0) || !(min_step > 0.0) || !(L >= 0.0)) return UPPE_ERR_ARG;
+  if (max_attempts <= 0) max_attempts = UPPE_DEFAULT_MAX_ATTEMPTS;
   k_begin<<<1, 1, 0, s>>>(p->st, L, tol, max_step, min_step, max_attempts);
   UPPE_CK(cudaGetLastError());
   return 0;

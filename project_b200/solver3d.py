@@ -42,42 +42,10 @@ class ERK43IP_UPPE_3D_Optimized:
         self.A_scale = 1.0
         self.last_result = None
 
-    # ---- FP64 tables of solver_3d.py:28-98 ------------------------------------
     def _tables(self):
-        kx = 2 * np.pi * np.fft.fftfreq(self.Nx, self.dx)                    # :28
-        ky = 2 * np.pi * np.fft.fftfreq(self.Ny, self.dy)                    # :29
-        # kperp^2 at field index (ix, iy).  The reference's meshgrid(ky, kx,
-        # indexing='ij') (:30) puts ky on axis 0, which is the same array for the
-        # square, equally spaced grids it supports.
-        self.K2_perp = (kx[:, None] ** 2 + ky[None, :] ** 2).astype(np.float64)
-        omega = 2 * np.pi * np.fft.fftfreq(self.Nt, self.dt)                 # :34
-        self.omega = omega
-        self.freq_axis_hz = np.fft.fftshift(omega) / (2 * np.pi)             # :36
-        m = self.medium
-        w0, c = float(self.omega0), float(self.c)
-        n_omega = np.asarray(m.refractive_index(omega + w0), dtype=np.float64)   # :61
-        k_val = n_omega * (omega + w0) / c                                   # :62
-        n_center = float(m.refractive_index(np.array([w0]))[0])             # :64-65
-        dw = w0 * 1e-3                                                       # :67
-        n_plus = float(m.refractive_index(np.array([w0 + dw]))[0])          # :68-69
-        k0 = n_center * w0 / c                                               # :71
-        k_plus = n_plus * (w0 + dw) / c                                      # :72
-        k1 = (k_plus - k0) / dw                                              # :73
-        k_ref = k0 + k1 * omega                                              # :74
-        self.k_sq = k_val ** 2
-        self.k_ref = k_ref
-        self.a_w = self.k_sq - k_ref ** 2                                    # :82 (first term)
-        self.valid = ((omega + w0) > 0).astype(np.uint8)                     # :86, :53-54
-        self.shock = np.asarray(m.get_shock_operator(omega), dtype=np.float64)   # :44
-        f = omega / (2 * np.pi)                                              # :47
-        f_max = float(np.max(np.abs(f))) + 1e-10                             # :48
-        self.filter = np.exp(-(f / (0.85 * f_max)) ** 16)                    # :49
-        X, Y = np.meshgrid(self.x, self.y, indexing='ij')                    # :90
-        R = np.sqrt(X ** 2 + Y ** 2)
-        half_w = float(np.max(np.abs(self.x)))
-        r_edge, r_start = 0.98 * half_w, 0.85 * half_w
-        s = np.clip((R - r_start) / (r_edge - r_start + 1e-30), 0.0, 1.0)
-        self.damp = (120.0 * (s ** 10)).astype(np.float64)                   # :98
+        tb = tables3d(self.x, self.y, self.t, self.medium)
+        for k, v in tb.items():
+            setattr(self, k, v)
 
     def _create_plan(self):
         m = self.medium
@@ -189,3 +157,57 @@ class ERK43IP_UPPE_3D_Optimized:
             out.copy_(A_w)
             return r.z, self.freq_axis_hz, out.numpy()
         return r.z, self.freq_axis_hz, A_w.cpu().numpy()
+
+
+def tables3d(x, y, t, medium):
+    """FP64 tables of ERK43IP_UPPE_3D_Optimized.__init__ (solver_3d.py:28-98)."""
+    x = np.asarray(x, dtype=np.float64)
+    y = np.asarray(y, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    Nx, Ny, Nt = len(x), len(y), len(t)
+    dx, dy, dt = float(x[1] - x[0]), float(y[1] - y[0]), float(t[1] - t[0])
+    kx = 2 * np.pi * np.fft.fftfreq(Nx, dx)                                  # :28
+    ky = 2 * np.pi * np.fft.fftfreq(Ny, dy)                                  # :29
+    # kperp^2 at field index (ix, iy).  The reference's meshgrid(ky, kx,
+    # indexing='ij') (:30) puts ky on axis 0, which is the same array for the
+    # square, equally spaced grids it supports.
+    K2_perp = (kx[:, None] ** 2 + ky[None, :] ** 2).astype(np.float64)
+    omega = 2 * np.pi * np.fft.fftfreq(Nt, dt)                               # :34
+    m = medium
+    w0, c = float(m.omega0), float(m.c)
+    n_omega = np.asarray(m.refractive_index(omega + w0), dtype=np.float64)   # :61
+    k_val = n_omega * (omega + w0) / c                                       # :62
+    n_center = float(m.refractive_index(np.array([w0]))[0])                 # :64-65
+    dw = w0 * 1e-3                                                           # :67
+    n_plus = float(m.refractive_index(np.array([w0 + dw]))[0])              # :68-69
+    k0 = n_center * w0 / c                                                   # :71
+    k_plus = n_plus * (w0 + dw) / c                                          # :72
+    k1 = (k_plus - k0) / dw                                                  # :73
+    k_ref = k0 + k1 * omega                                                  # :74
+    k_sq = k_val ** 2
+    f = omega / (2 * np.pi)                                                  # :47
+    f_max = float(np.max(np.abs(f))) + 1e-10                                 # :48
+    X, Y = np.meshgrid(x, y, indexing='ij')                                  # :90
+    R = np.sqrt(X ** 2 + Y ** 2)
+    half_w = float(np.max(np.abs(x)))
+    r_edge, r_start = 0.98 * half_w, 0.85 * half_w
+    s = np.clip((R - r_start) / (r_edge - r_start + 1e-30), 0.0, 1.0)
+    return {
+        'K2_perp': K2_perp, 'omega': omega,
+        'freq_axis_hz': np.fft.fftshift(omega) / (2 * np.pi),                # :36
+        'k_sq': k_sq, 'k_ref': k_ref,
+        'a_w': k_sq - k_ref ** 2,                                            # :82 first term
+        'valid': ((omega + w0) > 0).astype(np.uint8),                        # :86, :53-54
+        'shock': np.asarray(m.get_shock_operator(omega), dtype=np.float64),  # :44
+        'filter': np.exp(-(f / (0.85 * f_max)) ** 16),                       # :49
+        'damp': (120.0 * (s ** 10)).astype(np.float64),                      # :98
+    }
+
+
+def ip_operator_host(tb, kx_index=None):
+    """numpy restatement of the device's D(kx, ky, omega) from the tables (for checks)."""
+    q = tb['K2_perp'][:, :, None]
+    num = tb['a_w'][None, None, :] - q
+    kz = np.sqrt((tb['k_sq'][None, None, :] - q).astype(np.complex128))
+    D = 1j * (num / (kz + tb['k_ref'][None, None, :]))
+    return D * tb['valid'][None, None, :]

@@ -1,0 +1,133 @@
+"""Host-side logic without a GPU: table construction, input generators, ADK,
+batch partitioning (world size 2 over gloo)."""
+import os
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+from conftest import golden, rel_l2
+
+
+def test_3d_tables_reproduce_reference_operator():
+    from oracle import uppe3d
+    from project_b200.media import Argon
+    from project_b200.solver3d import ip_operator_host, tables3d
+    for name, disp in (('ref3d_mpi_cauchy_double', None),
+                       ('ref3d_adk_taylor_double', ('taylor', 1.000283, 20e-30, 0.0))):
+        g = golden(name)
+        med = Argon(float(g['lam']), 1.0, 'double', bool(g['shock']), dispersion=disp,
+                    lut=(g['log10_I'], g['W_lut']))
+        tb = tables3d(g['x'], g['y'], g['t'], med)
+        D = ip_operator_host(tb)
+        assert rel_l2(D, g['D']) < 1e-15
+        om = uppe3d.argon(float(g['lam']), 1.0, 'double', bool(g['shock']), dispersion=disp)
+        osol = uppe3d.Solver3D(g['x'], g['y'], g['t'], om, 'double')
+        assert np.array_equal(tb['damp'], osol.damp_space[:, :, 0])
+        assert np.array_equal(tb['filter'], osol.anti_alias_filter[0, 0].real)
+        assert np.array_equal(tb['shock'], osol.shock_operator[0, 0].real)
+        assert np.array_equal(tb['freq_axis_hz'], g['freq'])
+
+
+def test_1d_tables_match_reference():
+    from project_b200.solver1d import ERK43IP_UPPE
+    g = golden('ref1d_argon')
+    s = ERK43IP_UPPE(material='argon_gas', n2=1.0e-23, beam_radius=0.65 * 125e-6,
+                     center_wavelength=800e-9, alpha=0.5 * np.log(10) / 10, use_raman=False)
+    D, G, H, om = s.tables(g['t'])
+    assert np.array_equal(D, g['D'])
+    assert np.array_equal(om, g['omega'])
+    assert s.gamma == float(g['gamma']) and s.n0 == float(g['n0'])
+    g = golden('ref1d_silica_raman')
+    s = ERK43IP_UPPE(material='fused_silica', n2=2.6e-20, beam_radius=30e-6, center_wavelength=1064e-9)
+    D, G, H, om = s.tables(g['t'])
+    assert np.array_equal(D, g['D'])
+    assert rel_l2(H, g['H_R']) < 1e-15
+
+
+def test_1d_uppe_factor_matches_oracle():
+    from oracle import uppe1d as o1
+    from project_b200.solver1d import ERK43IP_UPPE
+    t = np.linspace(-0.5e-12, 0.5e-12, 512)
+    kw = dict(material='argon_gas', n2=1e-23, beam_radius=80e-6, center_wavelength=800e-9)
+    o = o1.Solver1D(use_raman=False, **kw)
+    om = 2 * np.pi * np.fft.fftfreq(512, t[1] - t[0])
+    o.setup(om, t[1] - t[0])
+    D, G, H, _ = ERK43IP_UPPE(use_raman=False, **kw).tables(t)
+    assert np.allclose(G, o.gamma * o._U, rtol=1e-15, atol=0)
+
+
+def test_inputs_match_oracle_definitions():
+    from oracle import inputs as oi
+    from project_b200 import pulses as pp
+    t = np.linspace(-0.5e-12, 0.5e-12, 1024)
+    assert np.allclose(pp.gaussian_pulse(t, 1e-4, 30e-15), oi.gaussian_pulse(t, 1e-4, 30e-15), rtol=1e-14)
+    assert rel_l2(pp.dispersed_pulse(t, 1e-4, 30e-15, GDD=200e-30, TOD=100e-45),
+                  oi.dispersed_pulse(t, 1e-4, 30e-15, GDD=200e-30, TOD=100e-45)) < 1e-13
+    assert rel_l2(pp.photon_noise(t, 800e-9, 0), oi.photon_noise(t, 800e-9, 0)) < 1e-13
+    x = np.linspace(-3e-3, 3e-3, 64)
+    assert rel_l2(pp.speckle(x, x, 50e-6, 0.01, 1), oi.speckle(x, x, 50e-6, 0.01, 1)) < 1e-13
+    # one photon per mode: mean |A_j|^2 over many seeds ~ hbar w_j Nt / dt
+    n = np.mean([np.abs(np.fft.fft(pp.photon_noise(t, 800e-9, s))) ** 2 for s in range(200)], axis=0)
+    w = 2 * np.pi * 299792458.0 / 800e-9 + 2 * np.pi * np.fft.fftfreq(1024, t[1] - t[0])
+    expect = np.where(w > 0, 1.054571817e-34 * w * 1024 / (t[1] - t[0]), 0)
+    sel = w > 0
+    assert abs(np.mean(n[sel] / expect[sel]) - 1) < 0.05
+    sp = pp.speckle(x, x, 50e-6, 0.01, 1)
+    assert abs(np.std(sp) - 0.01) < 1e-12 and abs(np.mean(sp) - 1) < 1e-12
+
+
+def test_adk_matches_oracle():
+    from oracle import adk as oa
+    from project_b200.media import Argon, adk_rate
+    E = np.logspace(6, 12, 200)
+    Ui = 15.76 * 1.60217663e-19
+    assert np.array_equal(adk_rate(E, Ui), oa.adk_rate(E, Ui))
+    m = Argon(800e-9, 1.0, 'double', True)
+    x, W = oa.ionization_lut(Ui)
+    assert np.array_equal(m.lut_log10I, x) and np.array_equal(m.lut_W, W)
+
+
+def test_partition_instances_is_balanced_cover():
+    from project_b200.distributed import instance_cost, partition_instances
+    rng = np.random.Generator(np.random.PCG64(2))
+    Nt = rng.choice([2048, 4096, 8192, 16384], size=256)
+    costs = [instance_cost(int(n), 1.0) for n in Nt]
+    parts = partition_instances(costs, 8)
+    flat = sorted(i for p in parts for i in p)
+    assert flat == list(range(256))
+    loads = [sum(costs[i] for i in p) for p in parts]
+    assert max(loads) / (sum(loads) / 8) < 1.05
+
+
+def _worker(rank, world, port, q):
+    import torch.distributed as dist
+    from project_b200.distributed import gather_results, partition_instances
+    os.environ['MASTER_ADDR'] = '127.0.0.1'
+    os.environ['MASTER_PORT'] = str(port)
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    costs = [float(c) for c in range(1, 11)]
+    parts = partition_instances(costs, world)
+    mine = parts[rank]
+    local = [(i, {'z': 1.0, 'rank': rank}) for i in mine]
+    merged = gather_results(local)
+    if rank == 0:
+        q.put((sorted(merged), [merged[i]['rank'] for i in range(10)], parts))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharded_batch_gather_gloo_world2():
+    ctx = mp.get_context('spawn')
+    q = ctx.Queue()
+    port = 29500 + os.getpid() % 1000
+    procs = [ctx.Process(target=_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    keys, owners, parts = q.get(timeout=120)
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    assert keys == list(range(10))
+    for r, part in enumerate(parts):
+        assert all(owners[i] == r for i in part)
