@@ -326,6 +326,30 @@ def run_b200(args, rank, world, local_rank):
     return 0
 
 
+def run_profile_case(args):
+    """Only the propagator: set up, warm up, run the timed attempts, print timing."""
+    import torch
+    from project_b200 import _lib
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, y, t = grids()
+    cdt = np.complex64 if args.precision == 'single' else np.complex128
+    sol = ERK43IP_UPPE_3D_Optimized(x, y, t, argon_medium(args.precision), precision=args.precision)
+    sol.set_field(torch.from_numpy(make_input(x, y, t, cdt)).cuda())
+    lib, s = sol._lib, _lib.stream_ptr()
+    _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'begin')
+    _lib.check(lib.uppe3d_run_steps(sol._plan, args.warmup, s), 'warmup')
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    _lib.check(lib.uppe3d_run_steps(sol._plan, args.steps, s), 'run')
+    e1.record()
+    torch.cuda.synchronize()
+    r = sol.result()
+    print(json.dumps({'ms_per_attempt': e0.elapsed_time(e1) / args.steps, 'attempts': r.attempts,
+                      'accepted': r.accepted, 'z': r.z, 'status': r.status}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -335,6 +359,8 @@ def main():
     ap.add_argument('--precision', default='single', choices=['single', 'double'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-plain-gpu', action='store_true')
+    ap.add_argument('--profile-case', action='store_true',
+                    help='only the solver: warm-up + timed attempts (a short command for ncu)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -343,6 +369,8 @@ def main():
         args.warmup = 3
     if args.impl == 'reference':
         return run_reference(args, rank)
+    if args.profile_case:
+        return run_profile_case(args)
     import datetime
     import torch.distributed as dist
     if world > 1:

@@ -200,6 +200,7 @@ struct Lut {
   const void* w;    // rates, field precision
   int n;
   double x0, inv_dx;
+  double zero_x;    // W is exactly 0 for clipped log10(I) <= zero_x (-inf if none)
 };
 
 template <typename Rl>
@@ -210,6 +211,8 @@ __device__ __forceinline__ Rl lut_eval(const Lut& L, Rl I) {
   Rl x = (sizeof(Rl) == 8) ? (Rl)log10((double)I + 1e-30) : (Rl)log10f((float)I + 1e-30f);
   const Rl x0 = __ldg(xp), x1 = __ldg(xp + n - 1);
   x = x < x0 ? x0 : (x > x1 ? x1 : x);
+  // below the last leading zero of the table the interpolant is exactly 0
+  if ((double)x <= L.zero_x) return (Rl)0;
   int j = (int)floor(((double)x - L.x0) * L.inv_dx);
   j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
   while (j < n - 1 && __ldg(xp + j + 1) <= x) ++j;

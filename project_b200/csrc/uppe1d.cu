@@ -155,9 +155,22 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     p->b.lut.n = n;
     p->b.lut.x0 = d->lut_log10I[0];
     p->b.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
+    {
+      // leading run of zero rates (as stored in the field precision)
+      int j0 = -1;
+      for (int i = 0; i < n; ++i) {
+        const double wv = dbl ? d->lut_W[i] : (double)(float)d->lut_W[i];
+        if (wv != 0.0) break;
+        j0 = i;
+      }
+      p->b.lut.zero_x = j0 < 0 ? -INFINITY
+                       : (dbl ? d->lut_log10I[j0] : (double)(float)d->lut_log10I[j0]);
+      if (j0 == n - 1) p->b.lut.zero_x = INFINITY;
+    }
   } else {
     p->b.lut.x = p->b.lut.w = nullptr;
     p->b.lut.n = 0;
+    p->b.lut.zero_x = INFINITY;
   }
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);

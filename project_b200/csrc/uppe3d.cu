@@ -116,9 +116,20 @@ __device__ __forceinline__ void ip_operator(const Tables3D& tb, int iw, double q
   Di = rr;
 }
 
+// Per-omega constants of the operator, loaded once per thread (each thread of a
+// y-pass tile owns one omega column).
+struct OmegaCol {
+  double aw, ksq, kref;
+  bool valid;
+  __device__ __forceinline__ OmegaCol(const Tables3D& tb, int iw)
+      : aw(tb.aw[iw]), ksq(tb.ksq[iw]), kref(tb.kref[iw]), valid(tb.valid[iw] != 0) {}
+};
+
 template <typename Rl> struct IPFactor;
 template <> struct IPFactor<double> {
-  __device__ __forceinline__ static double2 get(const Tables3D& tb, int iw, double q, double h2) {
+  // complex128: the reference's formula (solver_3d.py:80-87) and numpy's exp
+  __device__ __forceinline__ static double2 get(const Tables3D& tb, const OmegaCol&, int iw,
+                                                double q, double h2) {
     double Dr, Di;
     ip_operator(tb, iw, q, Dr, Di);
     const double ar = h2 * Dr, ai = h2 * Di;
@@ -129,17 +140,31 @@ template <> struct IPFactor<double> {
   }
 };
 template <> struct IPFactor<float> {
-  // Mixed precision: the phase h/2*Im(D) is formed in FP64 and reduced mod 2 pi
-  // before it is rounded to FP32.
-  __device__ __forceinline__ static float2 get(const Tables3D& tb, int iw, double q, double h2) {
-    double Dr, Di;
-    ip_operator(tb, iw, q, Dr, Di);
-    double ph = h2 * Di;
+  // Mixed precision.  D = i (k_z - k_ref): the same operator as the reference's
+  // i (k^2 - k_ref^2 - k_perp^2)/(k_z + k_ref); in FP64 the direct difference
+  // loses ~1e-16 * k ~ 1e-9 rad/m, far below FP32 resolution of the field, and
+  // needs no division.  k_z comes from an FP32 square root refined by one FP64
+  // Newton step (error ~1e-8 1/m).  The phase h/2*Im(D) is formed in FP64 and
+  // reduced mod 2 pi before it is rounded to FP32; __sincosf then works on [-pi, pi].
+  __device__ __forceinline__ static float2 get(const Tables3D&, const OmegaCol& oc, int,
+                                               double q, double h2) {
+    if (!oc.valid) return make_float2(1.f, 0.f);
+    const double arg = oc.ksq - q;
+    double ph;
+    float m = 1.f;
+    if (arg >= 0.0) {
+      const float kf = sqrtf((float)arg);
+      const double k0 = (double)kf;
+      const double kz = fma(fma(-k0, k0, arg), (double)(0.5f / kf), k0);
+      ph = h2 * (kz - oc.kref);
+    } else {   // evanescent: k_z = i sqrt(-arg) -> D = -sqrt(-arg) - i k_ref
+      m = expf((float)(-h2 * sqrt(-arg)));
+      ph = -h2 * oc.kref;
+    }
     const double twopi = 6.283185307179586476925286766559;
-    ph = ph - twopi * rint(ph * (1.0 / twopi));
+    ph = fma(-twopi, rint(ph * (1.0 / twopi)), ph);
     float s, c;
-    sincosf((float)ph, &s, &c);
-    const float m = expf((float)(h2 * Dr));
+    __sincosf((float)ph, &s, &c);
     return make_float2(m * c, m * s);
   }
 };
@@ -176,15 +201,22 @@ struct BlockSync {
 template <typename C, int N, int NTHR>
 __device__ __forceinline__ void load_tile(C* s, const C* __restrict__ g, long long base,
                                           long long stride, int tid) {
-  // 16-byte vectors: VPR vectors per row of kW complex
+  // 16-byte vectors: VPR vectors per row of kW complex; all of a thread's loads
+  // are issued before its shared-memory stores
   constexpr int VPR = kW * (int)sizeof(C) / 16;
+  constexpr int NV = N * VPR / NTHR;
+  static_assert(N * VPR % NTHR == 0, "tile/threads mismatch");
   const float4* __restrict__ gv = reinterpret_cast<const float4*>(g);
   float4* sv = reinterpret_cast<float4*>(s);
-#pragma unroll 4
-  for (int v = tid; v < N * VPR; v += NTHR) {
+  float4 r[NV];
+#pragma unroll
+  for (int k = 0; k < NV; ++k) {
+    const int v = tid + k * NTHR;
     const int n = v / VPR, c = v % VPR;
-    sv[n * VPR + c] = __ldg(gv + (base + n * stride) * (long long)sizeof(C) / 16 + c);
+    r[k] = __ldg(gv + (base + n * stride) * (long long)sizeof(C) / 16 + c);
   }
+#pragma unroll
+  for (int k = 0; k < NV; ++k) sv[tid + k * NTHR] = r[k];
 }
 template <typename C, int N, int NTHR>
 __device__ __forceinline__ void store_tile(const C* s, C* __restrict__ g, long long base,
@@ -200,7 +232,7 @@ __device__ __forceinline__ void store_tile(const C* s, C* __restrict__ g, long l
 }
 
 template <typename Rl, int N>
-__global__ void __launch_bounds__(SpaceCfg<N>::NTHR)
+__global__ void __launch_bounds__(SpaceCfg<N>::NTHR, (sizeof(Rl) == 4 && N == 256) ? 2 : 1)
 k_space(SpaceArgs a) {
   using C = typename CT<Rl>::T;
   constexpr int NTHR = SpaceCfg<N>::NTHR;
@@ -269,12 +301,35 @@ k_space(SpaceArgs a) {
   }
 
   // ---------------- y passes (stage algebra in the (kx, ky, omega) domain) ----
-  C* acur = reinterpret_cast<C*>(a.b.acur);
-  C* k1b = reinterpret_cast<C*>(a.b.k1);
-  C* tsum = reinterpret_cast<C*>(a.b.tsum);
-  C* a4p = reinterpret_cast<C*>(a.b.a4p);
+  C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
+  C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
+  C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
+  C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
   const double h2 = 0.5 * h;
   const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
+  // stage operands of this thread's elements, prefetched before the tile FFT so
+  // their latency overlaps it (element i: e = tid + i*NTHR)
+  C opA[E], opB[E];
+  auto eidx = [&](int i) {
+    const int e = tid + i * NTHR;
+    return base + (long long)(e / kW) * stride + (e % kW);
+  };
+  if (mode == YMID1R) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) { opA[i] = __ldg(acur + eidx(i)); opB[i] = __ldg(k1b + eidx(i)); }
+  } else if (mode == YMID2 || mode == YMID3) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) { opA[i] = __ldg(acur + eidx(i)); opB[i] = __ldg(tsum + eidx(i)); }
+  } else if (mode == YMID4) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) opB[i] = __ldg(tsum + eidx(i));
+  } else if (mode == YFWD5) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      opA[i] = __ldg(a4p + eidx(i));
+      if (sizeof(Rl) == 8) opB[i] = __ldg(tsum + eidx(i));
+    }
+  }
 
   if (mode != YMID1R) {
     load_tile<C, N, NTHR>(s, in, base, stride, tid);
@@ -285,7 +340,10 @@ k_space(SpaceArgs a) {
   }
 
   double red = 0.0;
-#pragma unroll 2
+  // every element of this thread has omega column w0 + tid % kW (NTHR is a
+  // multiple of kW), so the per-omega tables are read once
+  const OmegaCol oc(a.tb, w0 + tid % kW);
+#pragma unroll
   for (int i = 0; i < E; ++i) {
     const int e = tid + i * NTHR;
     const int n = e / kW, w = e % kW;     // n = ky, o = kx
@@ -293,11 +351,11 @@ k_space(SpaceArgs a) {
     const int iw = w0 + w;
     if (mode == YFWD5) {
       const C a5 = s[idx(w, n)];
-      const C a4 = a4p[gi];
+      const C a4 = opA[i];
       double d;
       if (sizeof(Rl) == 8) {
         // literal |A4 - A3| as in solver_3d.py:145-151
-        const C beta = tsum[gi];
+        const C beta = opB[i];
         const C A4 = cadd(beta, cscale(a4, h6R));
         const Rl h30 = (Rl)(h / 30);
         const C A3 = cadd(beta, cscale(cadd(cscale(a4, (Rl)2), cscale(a5, (Rl)3)), h30));
@@ -312,7 +370,7 @@ k_space(SpaceArgs a) {
     }
     if (mode == YMID4) {
       const C a4 = s[idx(w, n)];
-      const C beta = tsum[gi];
+      const C beta = opB[i];
       const C A4 = cadd(beta, cscale(a4, h6R));
       a4p[gi] = a4;
       const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
@@ -321,7 +379,7 @@ k_space(SpaceArgs a) {
       continue;
     }
     const double qv = a.tb.q[(long long)o * Ny + n];
-    const C Ef = IPFactor<Rl>::get(a.tb, iw, qv, h2);
+    const C Ef = IPFactor<Rl>::get(a.tb, oc, iw, qv, h2);
     if (mode == YMID1 || mode == YMID1R) {
       C A, k1;
       if (mode == YMID1) {
@@ -330,8 +388,8 @@ k_space(SpaceArgs a) {
         acur[gi] = A;
         k1b[gi] = k1;
       } else {
-        A = acur[gi];
-        k1 = k1b[gi];
+        A = opA[i];
+        k1 = opB[i];
       }
       const C v = cmul(A, Ef);
       const C a1 = cmul(k1, Ef);
@@ -339,14 +397,14 @@ k_space(SpaceArgs a) {
       s[idx(w, n)] = cadd(v, cscale(a1, h2R));
     } else if (mode == YMID2) {
       const C a2 = s[idx(w, n)];
-      const C v = cmul(acur[gi], Ef);
-      const C ts = tsum[gi];
+      const C v = cmul(opA[i], Ef);
+      const C ts = opB[i];
       tsum[gi] = cadd(ts, cscale(a2, (Rl)2));
       s[idx(w, n)] = cadd(v, cscale(a2, h2R));
     } else {   // YMID3
       const C a3 = s[idx(w, n)];
-      const C v = cmul(acur[gi], Ef);
-      const C ts = cadd(tsum[gi], cscale(a3, (Rl)2));
+      const C v = cmul(opA[i], Ef);
+      const C ts = cadd(opB[i], cscale(a3, (Rl)2));
       const C beta = cmul(cadd(v, cscale(ts, h6R)), Ef);
       tsum[gi] = beta;
       s[idx(w, n)] = cmul(cadd(v, cscale(a3, hR)), Ef);
@@ -360,6 +418,93 @@ k_space(SpaceArgs a) {
   __syncthreads();
   stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
   store_tile<C, N, NTHR>(s, out, base, stride, tid);
+}
+
+// ---------------------------------------------------------------------------
+// x passes for square sizes N = R*R (16, 64, 256): register four-step FFT.
+// Thread (w, j) of a tile (kW omega-columns, N rows) holds rows j + R*i, i < R,
+// both in natural order and in the four-step output order (X[k1 + R k2] with
+// k1 = j), so loads and stores go directly between registers and HBM (a
+// half-warp covers 16 consecutive omega = 128 contiguous bytes per row).
+// One FFT = R-point DFT in registers, twiddle, one shared-memory transpose,
+// R-point DFT; the inverse is the same with conjugated roots.
+// ---------------------------------------------------------------------------
+template <int R, int DIR, typename C>
+__device__ __forceinline__ void fft_sq(C (&v)[R], C* T, const C* tw, int j, int w) {
+  DFT<R, DIR, C>::run(v);
+#pragma unroll
+  for (int k = 1; k < R; ++k) {
+    C t = tw[j * k];                 // exp(-2 pi i j k / N), j k < N
+    if (DIR > 0) t.y = -t.y;
+    v[k] = cmul(v[k], t);
+  }
+#pragma unroll
+  for (int k = 0; k < R; ++k) T[(k * R + j) * kW + w] = v[k];
+  __syncthreads();
+#pragma unroll
+  for (int k = 0; k < R; ++k) v[k] = T[(j * R + k) * kW + w];
+  __syncthreads();
+  DFT<R, DIR, C>::run(v);
+}
+
+template <typename Rl, int R>
+__global__ void __launch_bounds__(kW * R, (sizeof(Rl) == 4 && R == 16) ? 3 : 1)
+k_xpass_sq(SpaceArgs a) {
+  using C = typename CT<Rl>::T;
+  constexpr int N = R * R;
+  constexpr int NTHR = kW * R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* T = tw + N;
+  const int tid = threadIdx.x, w = tid % kW, j = tid / kW;
+  State3D* st = a.st;
+  const int mode = a.mode;
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twx);
+    for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  if (st->done) return;
+  if (mode == XFWD_Z && !st->fresh) return;
+  const int Nt = a.g.Nt, Ny = a.g.Ny;
+  const int ntile = Nt / kW;
+  const int o = blockIdx.x / ntile;          // y index
+  const int w0 = (blockIdx.x % ntile) * kW;  // omega offset
+  const long long stride = (long long)Ny * Nt;
+  const long long base = (long long)o * Nt + w0 + w;
+  const double h = st->h;
+  const C* __restrict__ in = reinterpret_cast<const C*>(a.in);
+  C* __restrict__ out = reinterpret_cast<C*>(a.out);
+  C v[R];
+  auto gidx = [&](int i) { return base + (long long)(j + R * i) * stride; };
+  const bool inv = (mode == XINV || mode == XINV_Z);
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = __ldg(in + gidx(i));
+  if (inv) fft_sq<R, +1>(v, T, tw, j, w);
+  else fft_sq<R, -1>(v, T, tw, j, w);
+#pragma unroll
+  for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
+  if (mode == XINV_Z) {
+    // candidate state Z = ifft2(A4) * filter(omega) * exp(-damp(x,y) h)
+    C* __restrict__ zc = reinterpret_cast<C*>(a.b.z[st->zidx ^ 1]);
+    const Rl nrm = (Rl)(1.0 / ((double)a.g.Nx * (double)a.g.Ny));
+    const Rl f = (Rl)a.tb.filt[w0 + w];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int x = j + R * i;   // output row = x index, o = y index
+      const Rl ab = (Rl)exp(-a.tb.damp[(long long)x * Ny + o] * h);
+      zc[gidx(i)] = cscale(cscale(cscale(v[i], nrm), f), ab);
+    }
+  }
+  if (mode == XFWD_Z) {
+    const C* __restrict__ zin = reinterpret_cast<const C*>(a.b.z[st->zidx]);
+    C* __restrict__ zout = reinterpret_cast<C*>(a.b.tmp[2]);
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = __ldg(zin + gidx(i));
+    fft_sq<R, -1>(v, T, tw, j, w);
+#pragma unroll
+    for (int i = 0; i < R; ++i) zout[gidx(i)] = v[i];
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -379,10 +524,33 @@ struct TArgs {
 };
 
 template <int NT> struct TCfg {
-  static constexpr int PAD = NT + NT / 32;
+  static constexpr int PAD = NT + NT / 16;
   static constexpr int FT = NT / 2 < 32 ? NT / 2 : 32;   // FFT team (lanes >= FT idle)
 };
-__device__ __forceinline__ int tpad(int n) { return n + (n >> 5); }
+// one padding element per 16: conflict-free for the per-lane chunk accesses
+// (lane l at 17 l) and for the Stockham writes of 8-byte elements
+__device__ __forceinline__ int tpad(int n) { return n + (n >> 4); }
+
+template <typename C, int NT>
+__device__ __forceinline__ void load_line(C* s, const C* __restrict__ src, int lane) {
+  // 16-byte vector loads, all issued before the shared stores
+  constexpr int EPV = 16 / (int)sizeof(C);          // elements per vector
+  if constexpr (NT >= 32 * EPV) {
+    constexpr int NV = NT / (32 * EPV);
+    const float4* __restrict__ v = reinterpret_cast<const float4*>(src);
+    float4 r[NV];
+#pragma unroll
+    for (int k = 0; k < NV; ++k) r[k] = __ldg(v + lane + 32 * k);
+#pragma unroll
+    for (int k = 0; k < NV; ++k) {
+      const C* e = reinterpret_cast<const C*>(&r[k]);
+#pragma unroll
+      for (int q = 0; q < EPV; ++q) s[tpad((lane + 32 * k) * EPV + q)] = e[q];
+    }
+  } else {
+    for (int n = lane; n < NT; n += 32) s[tpad(n)] = src[n];
+  }
+}
 struct LineIdx {
   __device__ __forceinline__ int operator()(int, int n) const { return tpad(n); }
 };
@@ -391,11 +559,12 @@ struct WarpSync {
 };
 
 template <typename Rl, int NT, int WPB>
-__global__ void __launch_bounds__(WPB * 32)
+__global__ void __launch_bounds__(WPB * 32, (sizeof(Rl) == 4 && NT <= 512) ? 3 : 1)
 k_tpass(TArgs a) {
   using C = typename CT<Rl>::T;
   constexpr int PAD = TCfg<NT>::PAD;
-  constexpr int E = NT / 32;
+  constexpr int E = NT / 32;                  // samples per lane (one contiguous chunk)
+  constexpr bool KEEP_W = E <= 16;            // keep the rates in registers
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -417,45 +586,52 @@ k_tpass(TArgs a) {
   C* out = reinterpret_cast<C*>(a.out);
   const Rl in_scale = (Rl)(a.mode == T_FROM_Z ? 1.0 / NT
                                                : 1.0 / ((double)NT * a.g.Nx * a.g.Ny));
-  const double A_scale = st->A_scale;
-  const Rl A_scaleR = (Rl)A_scale;
+  const Rl A_scaleR = (Rl)st->A_scale;
   const Medium3D& m = a.md;
   LineIdx idx;
   WarpSync wsync;
 
-  // load (coalesced) and inverse FFT along t
-  const C* src = in + line * NT;
-#pragma unroll
-  for (int i = 0; i < E; ++i) sK[tpad(lane + 32 * i)] = src[lane + 32 * i];
+  // load (16-byte vectors, coalesced) and inverse FFT along t
+  load_line<C, NT>(sK, in + line * NT, lane);
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sK, tw, lane, idx, wsync);
 
   // ---- nonlinear response on this lane's chunk t in [lane*E, lane*E+E) ----
   const int t0 = lane * E;
+  float Wr[KEEP_W ? E : 1];
   bool any_w = false;
-  bool affine_ok = (m.ava == 0.0);
-  double cmap = 1.0, dmap = 0.0;   // composed affine map of the chunk
-  const AffineStep aff(m);
-  const double eg0 = aff.e, sf0 = aff.sf;
   if (m.plasma) {
-#pragma unroll 4
-    for (int t = t0; t < t0 + E; ++t) {
-      const C av = cscale(sK[tpad(t)], in_scale);
-      const C Ap = cscale(av, A_scaleR);
-      const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
-      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
-      any_w |= (w != 0.0);
-      // rho' = rho (e - w sf) + w rho_nt sf, valid while w sf <= e (no clamping)
-      const double c = eg0 - w * sf0;
-      affine_ok &= (c >= 0.0);
-      dmap = c * dmap + w * m.rho_nt * sf0;
-      cmap = c * cmap;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const C Ap = cscale(cscale(sK[tpad(t0 + i)], in_scale), A_scaleR);
+      const float w = (float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+      any_w |= (w != 0.f);
+      if constexpr (KEEP_W) Wr[i] = w;
     }
   }
   const bool plasma_line = m.plasma && (__any_sync(0xffffffffu, any_w) || m.ava != 0.0);
   double rho0 = 0.0;
   if (plasma_line) {
-    if (__all_sync(0xffffffffu, affine_ok)) {
+    // composed affine map of the chunk: rho' = rho (e - w sf) + w rho_nt sf,
+    // valid while no clamp binds (w sf <= e, no avalanche)
+    const AffineStep aff(m);
+    bool ok = (m.ava == 0.0);
+    double cmap = 1.0, dmap = 0.0;
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      double w;
+      if constexpr (KEEP_W) {
+        w = (double)Wr[i];
+      } else {
+        const C Ap = cscale(cscale(sK[tpad(t0 + i)], in_scale), A_scaleR);
+        w = (double)(float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+      }
+      const double c = aff.e - w * aff.sf;
+      ok &= (c >= 0.0);
+      dmap = c * dmap + w * m.rho_nt * aff.sf;
+      cmap = c * cmap;
+    }
+    if (__all_sync(0xffffffffu, ok)) {
       // exclusive scan of affine maps over lanes: (c1,d1) then (c2,d2) = (c1 c2, c2 d1 + d2)
       double c = cmap, d = dmap;
 #pragma unroll
@@ -464,19 +640,17 @@ k_tpass(TArgs a) {
         const double dp = __shfl_up_sync(0xffffffffu, d, off);
         if (lane >= off) { d = c * dp + d; c = c * cp; }
       }
-      // inclusive (c,d) of lanes 0..lane applied to rho=0 gives rho after the chunk;
-      const double incl = d;
-      const double excl = __shfl_up_sync(0xffffffffu, incl, 1);
+      const double excl = __shfl_up_sync(0xffffffffu, d, 1);
       rho0 = lane == 0 ? 0.0 : excl;
     } else {
-      // serial exact pass by lane 0 records the density at each chunk start
+      // a clamp binds on this line: lane 0 runs the exact serial update and
+      // records the density at each chunk start
       double* starts = reinterpret_cast<double*>(sP);
       if (lane == 0) {
         double rho = 0.0;
         for (int t = 0; t < NT; ++t) {
           if (t % E == 0) starts[t / E] = rho;
-          const C av = cscale(sK[tpad(t)], in_scale);
-          const C Ap = cscale(av, A_scaleR);
+          const C Ap = cscale(cscale(sK[tpad(t)], in_scale), A_scaleR);
           const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
           const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
           const double wa = (double)(float)(m.ava * (double)I);
@@ -488,11 +662,12 @@ k_tpass(TArgs a) {
       __syncwarp();
     }
   }
-  // phase 3: exact per-sample update from the chunk start; write Kerr and plasma terms
+  // Kerr (+ plasma) terms; exact per-sample density update from the chunk start
   {
     double rho = rho0;
-#pragma unroll 4
-    for (int t = t0; t < t0 + E; ++t) {
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int t = t0 + i;
       const C av = cscale(sK[tpad(t)], in_scale);
       const C Ap = cscale(av, A_scaleR);
       const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
@@ -500,7 +675,9 @@ k_tpass(TArgs a) {
       if (m.g4 != 0.0) g += (Rl)m.g4 * I * I;
       sK[tpad(t)] = C{-g * av.y, g * av.x};   // i g a
       if (plasma_line) {
-        const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+        double w;
+        if constexpr (KEEP_W) w = (double)Wr[i];
+        else w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
         const double wa = (double)(float)(m.ava * (double)I);
         const double rho_t = rho;
         const double gen = rho_step(rho, w, wa, m);
@@ -788,8 +965,21 @@ template <typename Rl> static std::vector<unsigned char> twiddles(int N) {
 }
 
 // ---- template dispatch -----------------------------------------------------
+template <int N> struct SqRoot {
+  static constexpr int v = N == 16 ? 4 : N == 64 ? 8 : N == 256 ? 16 : 0;
+};
+
 template <typename Rl, int N>
 static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, cudaStream_t s) {
+  constexpr int R = SqRoot<N>::v;
+  if constexpr (R > 0) {
+    if (a.mode <= XFWD_Z) {   // x passes of square sizes: register four-step kernel
+      using C = typename CT<Rl>::T;
+      const size_t sm = sizeof(C) * (size_t)(N + N * kW);
+      k_xpass_sq<Rl, R><<<(unsigned)nblocks, kW * R, sm, s>>>(a);
+      return;
+    }
+  }
   k_space<Rl, N><<<(unsigned)nblocks, SpaceCfg<N>::NTHR, smem, s>>>(a);
 }
 
@@ -802,7 +992,9 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   const int N = xpass ? p->g.Nx : p->g.Ny;
   const long long nouter = xpass ? p->g.Ny : p->g.Nx;
   const long long nblocks = nouter * (p->g.Nt / kW);
-  const size_t smem = sizeof(C) * (size_t)(N + 2 * N * kW);
+  // the second tile is only used by the passes that transform two fields
+  const int ntiles = (mode == YMID1 || mode == XFWD_Z) ? 2 : 1;
+  const size_t smem = sizeof(C) * (size_t)(N + ntiles * N * kW);
   switch (N) {
 #define UPPE_SP(n) case n: launch_space_n<Rl, n>(a, nblocks, smem, s); break;
     UPPE_SP(16) UPPE_SP(32) UPPE_SP(64) UPPE_SP(128) UPPE_SP(256) UPPE_SP(512)
@@ -839,6 +1031,12 @@ static int launch_t(uppe3d_plan* p, int mode, const void* in, void* out, cudaStr
 
 template <typename Rl, int N>
 static cudaError_t set_space_attr() {
+  constexpr int R = SqRoot<N>::v;
+  if constexpr (R > 0) {
+    const int sm = (int)(sizeof(typename CT<Rl>::T) * (N + N * kW));
+    const cudaError_t e = cudaFuncSetAttribute(k_xpass_sq<Rl, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e != cudaSuccess) return e;
+  }
   const int smem = (int)(sizeof(typename CT<Rl>::T) * (N + 2 * N * kW));
   return cudaFuncSetAttribute(k_space<Rl, N>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
 }
@@ -1016,6 +1214,7 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
   }
   {
     const int n = d->lut_n;
+    const int dbl = p->dbl;
     if (n < 2) { uppe3d_plan_destroy(p); return UPPE_ERR_ARG; }
     std::vector<unsigned char> lx(n * (p->dbl ? 8 : 4)), lw(n * (p->dbl ? 8 : 4));
     for (int i = 0; i < n; ++i) {
@@ -1027,6 +1226,18 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
     p->tb.lut.n = n;
     p->tb.lut.x0 = d->lut_log10I[0];
     p->tb.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
+    {
+      // leading run of zero rates (as stored in the field precision)
+      int j0 = -1;
+      for (int i = 0; i < n; ++i) {
+        const double wv = dbl ? d->lut_W[i] : (double)(float)d->lut_W[i];
+        if (wv != 0.0) break;
+        j0 = i;
+      }
+      p->tb.lut.zero_x = j0 < 0 ? -INFINITY
+                       : (dbl ? d->lut_log10I[j0] : (double)(float)d->lut_log10I[j0]);
+      if (j0 == n - 1) p->tb.lut.zero_x = INFINITY;
+    }
   }
   p->md.gk = d->gamma_kerr;
   p->md.g4 = d->gamma_hoke;
