@@ -173,6 +173,28 @@ long long uppe1d_hist_slots(const uppe1d_plan* plan);    /* sum hist_cap        
 int uppe1d_propagate(uppe1d_plan* plan, void* field, void* hist, double* zhist,
                      uppe1d_result* results, uppe_stream_t stream);
 
+/* Allocation-free single propagation, for callers that cannot allocate device
+ * memory (a host framework that owns the CUDA allocator and forbids cudaMalloc
+ * from plug-ins, a real-time host that must not allocate after start-up, or code
+ * holding only device pointers lent by another runtime).  No counterpart in the
+ * reference.  It runs the same kernel as uppe1d_propagate for one instance
+ * without a plan: the caller passes the FP64 tables D, G (and H when raman, all
+ * device memory, packed as in uppe1d_desc), the ionisation table in the field
+ * precision (device, only when plasma) and the device field (A0 in, final A out,
+ * time domain).  The per-call device state lives in one static device array of
+ * UPPE_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until exit;
+ * Nt above UPPE_NOALLOC_MAX_NT_C64 / _C128 is rejected with UPPE_ERR_SIZE, and
+ * hist_cap must be 0.  The first call on a device looks up the array's address
+ * (make it before any stream capture).  Calls share the array: calls that overlap
+ * on the GPU race.  Synchronises the stream when result is not NULL. */
+#define UPPE_NOALLOC_MAX_NT_C64 16384
+#define UPPE_NOALLOC_MAX_NT_C128 8192
+#define UPPE_NOALLOC_SCRATCH_BYTES (1024ull + 9ull * UPPE_NOALLOC_MAX_NT_C128 * 16ull)
+int uppe1d_propagate_noalloc(const uppe1d_inst_desc* inst, int precision, const double* D,
+                             const double* G, const double* H, int lut_n,
+                             const void* lut_log10I, const void* lut_W, void* field,
+                             uppe1d_result* result, uppe_stream_t stream);
+
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,
