@@ -703,6 +703,235 @@ k_tpass(TArgs a) {
   }
 }
 
+// ---------------------------------------------------------------------------
+// Warp FFT of a t-line of NT = 32*E points held in registers (E = 16 or 32).
+// Natural layout: lane l holds x[l + 32 m], m < E.  Four-step layout: lane L
+// holds X[out_index(L, k)], k < E.  fwd_like: DFT_E in registers, twiddle
+// W_NT^(l k1), transpose through a padded shared buffer S, DFT_E, then (E = 16)
+// a radix-2 combine with the partner lane L^1.  bwd_like is the transposed
+// sequence (four-step -> natural).  With DIR=-1 fwd_like is the forward FFT;
+// with DIR=+1 bwd_like is the unnormalised inverse.
+// ---------------------------------------------------------------------------
+template <int E> struct WarpFFT {
+  static constexpr int G = 32 / E;                   // lanes per second-stage DFT
+  static constexpr int SP = 32 + (G == 2 ? 2 : 1);   // padded row stride of S
+  static constexpr int NT = 32 * E;
+  static constexpr int SBUF = E * SP;
+  __device__ __forceinline__ static int out_index(int lane, int k) {
+    return (lane / G) + E * (k + E * (lane % G));
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void pair_fwd(C (&v)[E], const C* tw, int lane) {
+    if constexpr (G == 2) {
+      const bool r0 = (lane & 1) == 0;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        C t = tw[k * E];                               // W_32^k = W_NT^(k E)
+        if (DIR > 0) t.y = -t.y;
+        const C own = v[k];
+        C oth;
+        oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
+        oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
+        v[k] = r0 ? cadd(own, cmul(t, oth)) : csub(oth, cmul(t, own));
+      }
+    }
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void pair_bwd(C (&v)[E], const C* tw, int lane) {
+    if constexpr (G == 2) {
+      const bool r0 = (lane & 1) == 0;
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        C t = tw[k * E];
+        if (DIR > 0) t.y = -t.y;
+        const C own = v[k];
+        C oth;
+        oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
+        oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
+        v[k] = r0 ? cadd(own, oth) : cmul(t, csub(oth, own));
+      }
+    }
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void fwd_like(C (&v)[E], C* S, const C* tw, int lane) {
+    DFT<E, DIR, C>::run(v);
+#pragma unroll
+    for (int k = 1; k < E; ++k) {
+      C t = tw[lane * k];
+      if (DIR > 0) t.y = -t.y;
+      v[k] = cmul(v[k], t);
+    }
+#pragma unroll
+    for (int k = 0; k < E; ++k) S[k * SP + lane] = v[k];
+    __syncwarp();
+    const int d = lane / G, r = lane % G;
+#pragma unroll
+    for (int i = 0; i < E; ++i) v[i] = S[d * SP + r + G * i];
+    __syncwarp();
+    DFT<E, DIR, C>::run(v);
+    pair_fwd<DIR>(v, tw, lane);
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void bwd_like(C (&v)[E], C* S, const C* tw, int lane) {
+    pair_bwd<DIR>(v, tw, lane);
+    DFT<E, DIR, C>::run(v);
+    const int d = lane / G, r = lane % G;
+#pragma unroll
+    for (int i = 0; i < E; ++i) S[d * SP + r + G * i] = v[i];
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E; ++k) v[k] = S[k * SP + lane];
+    __syncwarp();
+#pragma unroll
+    for (int k = 1; k < E; ++k) {
+      C t = tw[lane * k];
+      if (DIR > 0) t.y = -t.y;
+      v[k] = cmul(v[k], t);
+    }
+    DFT<E, DIR, C>::run(v);
+  }
+};
+
+// t-line nonlinear pass with the register warp FFT (NT = 512, and NT = 1024 in
+// complex64).  Same physics and operation order as k_tpass; the frequency-domain
+// line is read and written in the four-step order (coalesced: each half-warp
+// covers 16 consecutive omega), the time-domain samples stay in registers, and
+// only lines that ionise go through shared memory in time order for the scan.
+template <typename Rl, int E, int WPB>
+__global__ void __launch_bounds__(WPB * 32, (sizeof(Rl) == 4 && E == 16) ? 3 : 1)
+k_tpass_w(TArgs a) {
+  using C = typename CT<Rl>::T;
+  using W = WarpFFT<E>;
+  constexpr int NT = 32 * E;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int BUF = W::SBUF > PAD ? W::SBUF : PAD;    // transpose buffer / time-order line
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* S = tw + NT + warp * BUF;
+  double* starts = reinterpret_cast<double*>(tw + NT + WPB * BUF) + warp * 32;
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
+    for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  State3D* st = a.st;
+  if (st->done) return;
+  if (a.mode == T_FROM_Z && !st->fresh) return;
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  const long long nlines = (long long)a.g.Nx * a.g.Ny;
+  if (line >= nlines) return;
+  const C* __restrict__ src = (a.mode == T_FROM_Z ? reinterpret_cast<const C*>(a.b.z[st->zidx])
+                                                 : reinterpret_cast<const C*>(a.in)) + line * NT;
+  C* __restrict__ dst = reinterpret_cast<C*>(a.out) + line * NT;
+  const Rl in_scale = (Rl)(a.mode == T_FROM_Z ? 1.0 / NT
+                                               : 1.0 / ((double)NT * a.g.Nx * a.g.Ny));
+  const Rl A_scaleR = (Rl)st->A_scale;
+  const Medium3D& m = a.md;
+
+  C v[E];
+#pragma unroll
+  for (int k = 0; k < E; ++k) v[k] = __ldg(src + W::out_index(lane, k));
+  W::template bwd_like<+1>(v, S, tw, lane);          // time domain, natural layout
+#pragma unroll
+  for (int k = 0; k < E; ++k) v[k] = cscale(v[k], in_scale);
+
+  bool any_w = false;
+  if (m.plasma) {
+#pragma unroll
+    for (int k = 0; k < E; ++k) {
+      const C Ap = cscale(v[k], A_scaleR);
+      any_w |= (lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y) != (Rl)0);
+    }
+  }
+  const bool plasma_line = m.plasma && (__any_sync(0xffffffffu, any_w) || m.ava != 0.0);
+  C pv[E];
+  if (plasma_line) {
+    // time-ordered copy for the density scan: lane owns t in [lane E, lane E + E)
+#pragma unroll
+    for (int k = 0; k < E; ++k) S[tpad(lane + 32 * k)] = v[k];
+    __syncwarp();
+    const int t0 = lane * E;
+    const AffineStep aff(m);
+    bool ok = (m.ava == 0.0);
+    double cmap = 1.0, dmap = 0.0;
+    for (int i = 0; i < E; ++i) {
+      const C Ap = cscale(S[tpad(t0 + i)], A_scaleR);
+      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+      const double c = aff.e - w * aff.sf;
+      ok &= (c >= 0.0);
+      dmap = c * dmap + w * m.rho_nt * aff.sf;
+      cmap = c * cmap;
+    }
+    double rho0;
+    if (__all_sync(0xffffffffu, ok)) {
+      double c = cmap, d = dmap;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double cp = __shfl_up_sync(0xffffffffu, c, off);
+        const double dp = __shfl_up_sync(0xffffffffu, d, off);
+        if (lane >= off) { d = c * dp + d; c = c * cp; }
+      }
+      const double excl = __shfl_up_sync(0xffffffffu, d, 1);
+      rho0 = lane == 0 ? 0.0 : excl;
+    } else {
+      if (lane == 0) {
+        double rho = 0.0;
+        for (int t = 0; t < NT; ++t) {
+          if (t % E == 0) starts[t / E] = rho;
+          const C Ap = cscale(S[tpad(t)], A_scaleR);
+          const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+          const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+          const double wa = (double)(float)(m.ava * (double)I);
+          rho_step(rho, w, wa, m);
+        }
+      }
+      __syncwarp();
+      rho0 = starts[lane];
+    }
+    __syncwarp();
+    double rho = rho0;
+    for (int i = 0; i < E; ++i) {
+      const int t = t0 + i;
+      const C av = S[tpad(t)];
+      const C Ap = cscale(av, A_scaleR);
+      const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+      const double wa = (double)(float)(m.ava * (double)I);
+      const double rho_t = rho;
+      const double gen = rho_step(rho, w, wa, m);
+      const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
+      const double cr = loss - m.sigma_half * rho_t;
+      const double ci = -m.sigma_half * m.w0tc * rho_t;
+      S[tpad(t)] = C{(Rl)cr * av.x - (Rl)ci * av.y, (Rl)cr * av.y + (Rl)ci * av.x};
+    }
+    __syncwarp();
+#pragma unroll
+    for (int k = 0; k < E; ++k) pv[k] = S[tpad(lane + 32 * k)];
+    __syncwarp();
+  }
+  // Kerr term i (gk I + g4 I^2) a, in place
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    const C av = v[k];
+    const C Ap = cscale(av, A_scaleR);
+    const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
+    Rl g = (Rl)m.gk * I;
+    if (m.g4 != 0.0) g += (Rl)m.g4 * I * I;
+    v[k] = C{-g * av.y, g * av.x};
+  }
+  W::template fwd_like<-1>(v, S, tw, lane);
+  if (plasma_line) W::template fwd_like<-1>(pv, S, tw, lane);
+#pragma unroll
+  for (int k = 0; k < E; ++k) {
+    const int wi = W::out_index(lane, k);
+    C o = cscale(v[k], (Rl)a.tb.shock[wi]);
+    if (plasma_line) o = cadd(o, pv[k]);
+    if (!a.tb.valid[wi]) o = C{0, 0};
+    dst[wi] = o;
+  }
+}
+
 // initial transform: Z = fft_t(A0 / A_scale)
 template <typename Rl, int NT, int WPB>
 __global__ void __launch_bounds__(WPB * 32)
@@ -1004,8 +1233,25 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   return 0;
 }
 
+template <int NT, typename Rl> struct TWarp {
+  static constexpr bool use = NT == 512 || (NT == 1024 && sizeof(Rl) == 4);
+  static constexpr int E = NT / 32;
+  static constexpr int WPB = 8;
+  static constexpr int BUF = WarpFFT<(E < 16 ? 16 : E)>::SBUF > TCfg<NT>::PAD
+                                 ? WarpFFT<(E < 16 ? 16 : E)>::SBUF : TCfg<NT>::PAD;
+  static size_t smem() {
+    return (size_t)(NT + WPB * BUF) * sizeof(typename CT<Rl>::T) + (size_t)WPB * 32 * sizeof(double);
+  }
+};
+
 template <typename Rl, int NT, int KIND>
 static void launch_t_n(const TArgs& a, long long nlines, cudaStream_t s) {
+  if constexpr (KIND == 0 && TWarp<NT, Rl>::use) {
+    constexpr int WPB = TWarp<NT, Rl>::WPB;
+    const unsigned nb = (unsigned)((nlines + WPB - 1) / WPB);
+    k_tpass_w<Rl, NT / 32, WPB><<<nb, WPB * 32, TWarp<NT, Rl>::smem(), s>>>(a);
+    return;
+  }
   constexpr int WPB = TLaunch<NT, Rl>::WPB;
   const unsigned nb = (unsigned)((nlines + WPB - 1) / WPB);
   const size_t smem = TLaunch<NT, Rl>::smem();
@@ -1046,6 +1292,11 @@ static cudaError_t set_t_attr() {
   const int smem = (int)TLaunch<NT, Rl>::smem();
   cudaError_t e = cudaFuncSetAttribute(k_tpass<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
+  if constexpr (TWarp<NT, Rl>::use) {
+    e = cudaFuncSetAttribute(k_tpass_w<Rl, NT / 32, TWarp<NT, Rl>::WPB>,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TWarp<NT, Rl>::smem());
+    if (e != cudaSuccess) return e;
+  }
   e = cudaFuncSetAttribute(k_tload<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   return cudaFuncSetAttribute(k_tstore<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);

@@ -121,3 +121,24 @@ def test_larger_grid_attempts_vs_oracle():
         assert abs(err - err_o) <= 1e-8 * err_o + 1e-18
         sol.commit(acc)
     assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < 1e-10
+
+
+@pytest.mark.parametrize('Nt,precision,W0', [(512, 'double', 3e9), (512, 'double', 1e15),
+                                              (512, 'single', 3e9), (1024, 'single', 3e9)])
+def test_long_lines_vs_oracle(Nt, precision, W0):
+    """t-lines of 512 / 1024 samples (the register warp-FFT kernel): attempts from the
+    oracle's schedule; W0 = 1e15 makes the density clamp bind (serial scan path)."""
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(N=16, Nt=Nt, W0=W0, I_peak=5e16)
+    z, freq, Ao, log = osol.propagate(A0, 0.01, tol=1e-5, max_attempts=4)
+    med = Argon(lam, 1.0, precision, True, lut=lut)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision=precision)
+    sol.set_field(A0)
+    for z0, h, err_o, acc in log:
+        err = sol.attempt(h)
+        if precision == 'double':
+            assert abs(err - err_o) <= 1e-8 * err_o + 1e-18
+        sol.commit(acc)
+    tol = 1e-10 if precision == 'double' else 1e-4
+    assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < tol
