@@ -194,7 +194,7 @@ def profile_kernels(sol, lib, n_attempts=3):
         for i in range(n.value):
             if byts[i] == 0:
                 continue
-            name = {0: 'k_tpass', 1: 'k_space', 2: 'k_space'}.get(kind[i], 'scalar')
+            name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space'}.get(kind[i], 'scalar')
             a = agg.setdefault(name, [0.0, 0.0, 0])
             a[0] += ms[i]
             a[1] += byts[i]
@@ -256,6 +256,12 @@ def run_b200(args, rank, world, local_rank):
     dom = max((k for k in agg if k != 'scalar'), key=lambda k: agg[k][0])
     d_ms, d_bytes, d_n = agg[dom]
     achieved = d_bytes / (d_ms / 1e3) / 1e9
+    traffic = None
+    try:   # DRAM bytes from the committed ncu capture of the same kernel, per launch
+        with open(os.path.join(ROOT, 'profiles', 'ncu_traffic.json')) as f:
+            traffic = json.load(f)[dom]['measured_over_algorithmic'] * d_bytes / d_n
+    except Exception:
+        traffic = None
     step_bytes = 64.0 * (8 if prec == 'single' else 16) * npts     # 64 s N per attempt
     step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
 
@@ -308,7 +314,8 @@ def run_b200(args, rank, world, local_rank):
                        'l2': 'every field (268 MB c64) exceeds the 126 MB L2; no flush'},
             'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak,
                          'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
-                         'traffic': None, 'launches_profiled': d_n,
+                         'traffic': traffic, 'traffic_unit': 'bytes per launch',
+                         'launches_profiled': d_n,
                          'bytes_model': 'per launch: fields read + written x field bytes'},
             'roofline_step': {'model': '64*s*N bytes per attempt', 'achieved': step_achieved,
                               'peak': peak, 'unit': 'GB/s', 'frac': step_achieved / peak},
