@@ -37,6 +37,7 @@ W0 = 1e-3
 L_PROP = 2.0
 TOL = 1e-5
 SAMPLE_N = 128       # CPU sample: 128 x 128 x 512
+LAM_1D = 800e-9
 
 
 def grids(n=NX, nt=NT):
@@ -178,6 +179,74 @@ def run_reference(args, rank):
     return 0
 
 
+def batched1d_instances(n=256, seed=2, L=1.0):
+    """Batched 1D sweep (seeded): Nt in {2048..16384} with dt = 1 ps/4095, E log-uniform in
+    10 uJ..1 mJ, pressure U(0.2, 3) bar (n2, beta2, beta3, plasma scale with it), GDD
+    U(-500, 500) fs^2; argon capillary a = 125 um, A_eff = pi (0.65 a)^2, loss 0.5 dB/m,
+    beta2 15 fs^2/m, beta3 15 fs^3/m per bar, ADK plasma, one-photon-per-mode noise."""
+    from project_b200.pulses import dispersed_pulse, photon_noise
+    from project_b200.solver1d import ERK43IP_UPPE, GasPlasma1D
+    rng = np.random.Generator(np.random.PCG64(seed))
+    Aeff = np.pi * (0.65 * 125e-6) ** 2
+    insts, fields = [], []
+    for k in range(n):
+        Nt = int(rng.choice([2048, 4096, 8192, 16384]))
+        E = float(np.exp(rng.uniform(np.log(10e-6), np.log(1e-3))))
+        P = float(rng.uniform(0.2, 3.0))
+        GDD = float(rng.uniform(-500e-30, 500e-30))
+        t = (np.arange(Nt) - (Nt - 1) / 2) * (1e-12 / 4095)
+        s = ERK43IP_UPPE(material='argon_gas', n2=1e-23 * P, beam_radius=0.65 * 125e-6,
+                         center_wavelength=LAM_1D, alpha=0.5 * np.log(10) / 10, use_raman=False,
+                         taylor=(15e-30 * P, 15e-45 * P), plasma=GasPlasma1D(Aeff, pressure_atm=P),
+                         precision='single')
+        insts.append(s.instance(t, L, tol=1e-6))
+        fields.append(dispersed_pulse(t, E, 30e-15, GDD=GDD) + photon_noise(t, LAM_1D, 1000 + k))
+    return insts, fields
+
+
+def run_batched1d(dev):
+    """Whole sweep in one persistent launch; sims/s over CUDA events."""
+    import torch
+    from project_b200.solver1d import BatchedPropagator
+    insts, fields = batched1d_instances()
+    bp = BatchedPropagator(insts, precision='single', device=dev)
+    packed0 = bp.pack(fields)
+    work = packed0.clone()
+    bp.run_packed(work)                      # warm-up (first launch)
+    work.copy_(packed0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    res = bp.run_packed(work)
+    e1.record()
+    torch.cuda.synchronize()
+    sec = e0.elapsed_time(e1) / 1e3
+    att = [r.attempts for r in res]
+    return {'value': len(insts) / sec, 'unit': 'sims/s', 'n_instances': len(insts), 'seconds': sec,
+            'attempts_total': int(sum(att)), 'attempts_max': int(max(att)),
+            'status_nonzero': int(sum(1 for r in res if r.status)), 'dtype': 'c64',
+            'workload': 'batched 1D sweep, 256 argon-capillary instances, L = 1 m, tol 1e-6, '
+                        'one persistent launch'}
+
+
+def cpu_baseline_1d():
+    """Oracle port of the reference 1D solver on one config-0 instance (Nt 4096, 2 GW 30 fs,
+    argon 1 bar, 1 m, tol 1e-6, with the plasma term) on the host."""
+    from oracle import uppe1d as o1
+    from oracle.inputs import gaussian_pulse
+    Aeff = np.pi * (0.65 * 125e-6) ** 2
+    t = np.linspace(-0.5e-12, 0.5e-12, 4096)
+    fw = 30e-15
+    s = o1.Solver1D(material='argon_gas', n2=1e-23, beam_radius=0.65 * 125e-6, center_wavelength=LAM_1D,
+                    alpha=0.5 * np.log(10) / 10, use_raman=False, taylor=(15e-30, 15e-45),
+                    plasma=o1.Plasma1D(Aeff, center_wavelength=LAM_1D))
+    t0 = time.perf_counter()
+    _, _, _, log = s.propagate(gaussian_pulse(t, 2e9 * fw * np.sqrt(np.pi / (4 * np.log(2))), fw), t, 1.0, tol=1e-6)
+    dt = time.perf_counter() - t0
+    return {'value': 1.0 / dt, 'unit': 'sims/s', 'cores': 1, 'kind': 'port',
+            'sample': f'one config-0 instance (Nt 4096, 1 m, {len(log)} attempts) on numpy/scipy: {dt:.2f} s'}
+
+
 def profile_kernels(sol, lib, n_attempts=3):
     """Per-launch CUDA-event times of whole attempts -> per-kernel totals."""
     import torch
@@ -296,6 +365,11 @@ def run_b200(args, rank, world, local_rank):
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = cpu_baseline(prec)
+    b1d = None
+    if not args.no_batched_1d:
+        b1d = run_batched1d(dev)
+        if rank == 0 and world == 1 and not args.no_cpu_baseline:
+            b1d['cpu_baseline'] = cpu_baseline_1d()
 
     if rank == 0:
         line = {
@@ -326,6 +400,7 @@ def run_b200(args, rank, world, local_rank):
                     'how': f'propagate(host pinned A0) over {e2e_attempts} attempts per call, '
                            'spectrum copied back to pinned host memory'},
             'plain_gpu': plain,
+            'batched_1d': b1d,
             'gpu_launches': args.steps * lib.uppe3d_launches_per_step(sol._plan),
             'clocks': clk,
         }
@@ -366,6 +441,7 @@ def main():
     ap.add_argument('--precision', default='single', choices=['single', 'double'])
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-plain-gpu', action='store_true')
+    ap.add_argument('--no-batched-1d', action='store_true')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
     args = ap.parse_args()
