@@ -173,6 +173,30 @@ long long uppe1d_hist_slots(const uppe1d_plan* plan);    /* sum hist_cap        
 int uppe1d_propagate(uppe1d_plan* plan, void* field, void* hist, double* zhist,
                      uppe1d_result* results, uppe_stream_t stream);
 
+/* propagate with the accepted step sizes written to hlog (device, hlog_cap per
+ * instance in instance order; result.accepted tells how many; status bit 16 when
+ * the log overflowed).  The record the adjoint needs (no reference counterpart:
+ * the reference has no differentiation). */
+int uppe1d_propagate_logged(uppe1d_plan* plan, void* field, double* hlog, int hlog_cap,
+                            uppe1d_result* results, uppe_stream_t stream);
+/* Replay: every instance takes the nsched step sizes hsched[i*nsched + k] (device),
+ * each accepted, no step control -- the frozen-schedule forward map that the adjoint
+ * differentiates (used for finite-difference checks).  No reference counterpart. */
+int uppe1d_propagate_schedule(uppe1d_plan* plan, void* field, const double* hsched, int nsched,
+                              uppe1d_result* results, uppe_stream_t stream);
+/* Workspace of uppe1d_adjoint, in complex128 elements. */
+long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K);
+/* Reverse-mode derivative of one instance's frozen-schedule propagation (complex128
+ * plan; Kerr + self-steepening + dispersion + loss; no Raman/plasma).  Replays the
+ * forward with a checkpoint every K steps and recomputes within segments.  Inputs
+ * (device): hlog[nsteps], A0 (time domain), Abar = dL/dA_L in the omega domain
+ * (dL = Re sum conj(Abar) dA).  Outputs (device): A0bar = dL/dfft(A0), gD = dL/dD,
+ * gG = dL/dG (the tables of uppe1d_desc), rhs = D A_L + N(A_L) (so dL/dL = Re
+ * sum conj(Abar) rhs).  No reference counterpart (the reference is not differentiable). */
+int uppe1d_adjoint(uppe1d_plan* plan, int inst, const double* hlog, int nsteps, int K,
+                   const void* A0, const void* Abar, void* A0bar, void* gD, double* gG, void* rhs,
+                   void* work, uppe_stream_t stream);
+
 /* Allocation-free single propagation, for callers that cannot allocate device
  * memory (a host framework that owns the CUDA allocator and forbids cudaMalloc
  * from plug-ins, a real-time host that must not allocate after start-up, or code

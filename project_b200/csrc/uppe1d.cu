@@ -216,3 +216,81 @@ extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double*
   }
   return 0;
 }
+
+// ---- step log, replay and adjoint ------------------------------------------
+static int run1(uppe1d_plan* p, Batch1D& b, uppe1d_result* results, cudaStream_t s) {
+  UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
+  UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s)
+                   : launch_uppe1d<float>(b, p->nblocks, p->smem, s));
+  if (results) {
+    UPPE1_CK(cudaMemcpyAsync(p->h_res, p->b.res, sizeof(Res1D) * p->ninst, cudaMemcpyDeviceToHost, s));
+    UPPE1_CK(cudaStreamSynchronize(s));
+    for (int i = 0; i < p->ninst; ++i) {
+      const Res1D& r = p->h_res[i];
+      results[i].z = r.z; results[i].h = r.h; results[i].err = r.err;
+      results[i].attempts = r.attempts; results[i].accepted = r.accepted;
+      results[i].status = r.status; results[i].hist_count = r.hist_count;
+    }
+  }
+  return 0;
+}
+
+extern "C" int uppe1d_propagate_logged(uppe1d_plan* p, void* field, double* hlog, int hlog_cap,
+                                       uppe1d_result* results, cudaStream_t s) {
+  if (!p || !field || !hlog || hlog_cap <= 0 || p->htotal > 0) return UPPE_ERR_ARG;
+  Batch1D b = p->b;
+  b.field = field;
+  b.hlog = hlog;
+  b.hlog_cap = hlog_cap;
+  return run1(p, b, results, s);
+}
+
+extern "C" int uppe1d_propagate_schedule(uppe1d_plan* p, void* field, const double* hsched,
+                                         int nsched, uppe1d_result* results, cudaStream_t s) {
+  if (!p || !field || !hsched || nsched < 0 || p->htotal > 0) return UPPE_ERR_ARG;
+  Batch1D b = p->b;
+  b.field = field;
+  b.hsched = hsched;
+  b.nsched = nsched;
+  return run1(p, b, results, s);
+}
+
+extern "C" long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K) {
+  if (Nt <= 0 || nsteps < 0 || K <= 0) return -1;
+  const long long nseg = (nsteps + K - 1) / K;
+  return (18LL + (nseg > 0 ? nseg : 1) + K) * Nt;
+}
+
+extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int nsteps, int K,
+                              const void* A0, const void* Abar, void* A0bar, void* gD, double* gG,
+                              void* rhs, void* work, cudaStream_t s) {
+  g_uppe_err[0] = 0;
+  if (!p || inst < 0 || inst >= p->ninst || !hlog || nsteps < 0 || K <= 0 || !A0 || !Abar ||
+      !A0bar || !gD || !gG || !rhs || !work)
+    return UPPE_ERR_ARG;
+  if (!p->dbl) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err), "uppe1d_adjoint: the adjoint needs a complex128 plan");
+    return UPPE_ERR_ARG;
+  }
+  const Inst1D& q = p->h_inst[inst];
+  if (q.raman || q.plasma) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err),
+             "uppe1d_adjoint: Raman and plasma terms have no adjoint here (Kerr + steepening only)");
+    return UPPE_ERR_ARG;
+  }
+  Adj1D a;
+  a.b = p->b;
+  a.inst = inst;
+  a.hlog = hlog;
+  a.nsteps = nsteps;
+  a.K = K;
+  a.A0 = (const double2*)A0;
+  a.Abar = (const double2*)Abar;
+  a.A0bar = (double2*)A0bar;
+  a.gD = (double2*)gD;
+  a.gG = gG;
+  a.rhs = (double2*)rhs;
+  a.work = (double2*)work;
+  UPPE1_CK(launch_uppe1d_adjoint(a, p->smem, s));
+  return 0;
+}

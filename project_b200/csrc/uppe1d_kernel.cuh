@@ -65,6 +65,10 @@ struct Batch1D {
   long long scratch_per_block;   // complex elements
   const void* tw;                // packed twiddles: size N at offset N-1
   Lut lut;
+  double* hlog;                  // accepted step sizes, hlog_cap per instance (or null)
+  int hlog_cap;
+  const double* hsched;          // replay: nsched step sizes per instance, all accepted (or null)
+  int nsched;
 };
 
 template <int N> struct Cfg1 {
@@ -243,7 +247,8 @@ __device__ bool plasma_line(Ctx1<Rl>& c) {
 // Returns sum |u|^2 for IN_5 (else 0).
 template <typename Rl, int N>
 __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename CT<Rl>::T* out,
-                          typename CT<Rl>::T* hist_t) {
+                          typename CT<Rl>::T* hist_t, typename CT<Rl>::T* save_u = nullptr,
+                          bool input_only = false) {
   using C = typename CT<Rl>::T;
   constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
@@ -276,8 +281,10 @@ __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename
       }
     }
     c.s[pad1(w)] = u;
+    if (save_u) save_u[w] = u;
   }
   __syncthreads();
+  if (input_only) return 0.0;     // stage input formed (and saved) only
   stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
   const Rl invN = (Rl)(1.0 / N);
   const bool raman = c.in->raman, plasma = c.in->plasma;
@@ -406,6 +413,10 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
     z += hh;
     C* t0 = c.A; c.A = c.A4; c.A4 = t0;     // state <- A4
     C* t1 = c.K1; c.K1 = c.O; c.O = t1;     // k1 <- alpha5' (FSAL)
+    if (b.hlog) {                           // step log for the adjoint
+      if (accepted < b.hlog_cap) { if (tid == 0) b.hlog[(long long)i * b.hlog_cap + accepted] = hh; }
+      else status |= 16;
+    }
     accepted += 1;
     if (hcount < 1000 || (z - zlast) > L / 500) {   // :327
       if (hist && hcount < in.hist_cap) {
@@ -417,7 +428,18 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
       }
     }
   };
-  while (z < L) {
+  if (b.hsched) {
+    // replay of a fixed step sequence, every step accepted (no control)
+    const double* hs = b.hsched + (long long)i * b.nsched;
+    for (int k = 0; k < b.nsched; ++k) {
+      const double hh = hs[k];
+      err = attempt1<Rl, N>(c, hh, cand());
+      attempts += 1;
+      if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
+      accept(hh);
+    }
+  }
+  while (!b.hsched && z < L) {
     if (z + h > L) h = L - z;
     err = attempt1<Rl, N>(c, h, cand());
     attempts += 1;
@@ -485,6 +507,211 @@ __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
     }
   }
 }
+
+// ---------------------------------------------------------------------------
+// Adjoint (reverse mode) of the ERK4(3)-IP step for Kerr + steepening with
+// dispersion and loss (no Raman, no plasma), complex128.  Convention: for a real
+// loss L and complex x, the cotangent xb satisfies dL = Re sum conj(xb) dx (the
+// same as torch's complex gradients).  Frozen accepted step sizes.
+// ---------------------------------------------------------------------------
+// VJP of N(u) = i G F(|a|^2 a), a = F^* u / N, with cotangent nb:
+//   p^b = F^*(-i G nb), ab = 2|a|^2 p^b + a^2 conj(p^b), ub = F ab / N;
+// accumulates gG[w] += Re(conj(nb) i F(|a|^2 a)).
+template <int N>
+__device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const double2* nb,
+                                      double2* out, double* gG) {
+  using C = double2;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const double invN = 1.0 / N;
+  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = u[w];
+  __syncthreads();
+  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int t = tid; t < N; t += T1) {
+    const C a = cscale(c.s[pad1(t)], invN);
+    c.GA[t] = a;
+    c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
+  }
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) {
+    const C ph = c.s[pad1(w)];
+    const C n = nb[w];
+    gG[w] += -n.x * ph.y + n.y * ph.x;
+    const double g = c.G[w];
+    c.s[pad1(w)] = C{g * n.y, -g * n.x};          // -i G nb
+  }
+  __syncthreads();
+  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int t = tid; t < N; t += T1) {
+    const C a = c.GA[t];
+    const C pb = c.s[pad1(t)];
+    const double I2 = 2.0 * (a.x * a.x + a.y * a.y);
+    const C a2 = cmul(a, a);
+    c.s[pad1(t)] = cadd(cscale(pb, I2), cmul(a2, cconj(pb)));
+  }
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) out[w] = cscale(c.s[pad1(w)], invN);
+  __syncthreads();
+}
+
+struct Adj1D {
+  Batch1D b;            // tables, twiddles, instance records of the plan
+  int inst;
+  const double* hlog;   // accepted step sizes of the forward run
+  int nsteps, K;        // steps, checkpoint interval
+  const double2* A0;    // time-domain input field
+  const double2* Abar;  // cotangent of the final state (omega domain)
+  double2* A0bar;       // out: cotangent of fft(A0) (omega domain)
+  double2* gD;          // out: dL/dD
+  double* gG;           // out: dL/dG
+  double2* rhs;         // out: D A_L + N(A_L) (for d/dL)
+  double2* work;        // 18 N + (ceil(nsteps/K) + K) N complex
+};
+
+template <int N>
+__device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
+  using C = double2;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const Inst1D& in = a.b.inst[a.inst];
+  Ctx1<double> c;
+  c.s = reinterpret_cast<C*>(smem);
+  c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
+  c.starts = c.red + 64;
+  c.tw = reinterpret_cast<const C*>(a.b.tw) + (N - 1);
+  C* w = a.work;
+  c.A = w; c.K1 = w + N; c.T = w + 2 * N; c.O = w + 3 * N;
+  c.A4 = w + 4 * N; c.A4P = w + 5 * N; c.GA = w + 6 * N;
+  C *A2 = w + 7 * N, *A3 = w + 8 * N, *U2 = w + 9 * N, *U3 = w + 10 * N, *U4 = w + 11 * N;
+  C *AB = w + 12 * N, *VB = w + 13 * N, *A1B = w + 14 * N, *A2B = w + 15 * N, *A3B = w + 16 * N;
+  C *TMP = w + 17 * N;
+  const int nseg = (a.nsteps + a.K - 1) / a.K;
+  C* CK = w + 18 * N;
+  C* SEG = CK + (long long)(nseg > 0 ? nseg : 1) * N;
+  c.D = a.b.D + in.off;
+  c.G = a.b.G + in.off;
+  c.H = nullptr;
+  c.in = &in;
+  c.lut = a.b.lut;
+  auto copy = [&](C* dst, const C* src) {
+    for (int x = tid; x < N; x += T1) dst[x] = src[x];
+    __syncthreads();
+  };
+  auto advance = [&](double hh) {      // one accepted forward step (state A, FSAL K1)
+    attempt1<double, N>(c, hh, nullptr);
+    C* t0 = c.A; c.A = c.A4; c.A4 = t0;
+    C* t1 = c.K1; c.K1 = c.O; c.O = t1;
+  };
+  // forward replay with checkpoints every K steps
+  for (int t = tid; t < N; t += T1) c.s[pad1(t)] = a.A0[t];
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int x = tid; x < N; x += T1) { c.A[x] = c.s[pad1(x)]; a.gD[x] = C{0, 0}; a.gG[x] = 0.0; }
+  __syncthreads();
+  copy(CK, c.A);
+  nl_eval<double, N>(c, IN_A, 0.0, c.K1, nullptr);
+  for (int j = 0; j < a.nsteps; ++j) {
+    advance(a.hlog[j]);
+    if ((j + 1) % a.K == 0 && j + 1 < a.nsteps) copy(CK + (long long)((j + 1) / a.K) * N, c.A);
+  }
+  // d/dL of the final state: D A_L + N(A_L) (K1 holds N(A_L) by FSAL)
+  for (int x = tid; x < N; x += T1) a.rhs[x] = cadd(cmul(c.D[x], c.A[x]), c.K1[x]);
+  copy(AB, a.Abar);
+  C* O0 = c.O;
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int j0 = sg * a.K, j1 = min(a.nsteps, j0 + a.K);
+    copy(c.A, CK + (long long)sg * N);
+    copy(SEG, c.A);
+    nl_eval<double, N>(c, IN_A, 0.0, c.K1, nullptr);
+    for (int j = j0; j < j1 - 1; ++j) {
+      advance(a.hlog[j]);
+      copy(SEG + (long long)(j - j0 + 1) * N, c.A);
+    }
+    for (int j = j1 - 1; j >= j0; --j) {
+      const double h = a.hlog[j];
+      // recompute the step's stage inputs from its start state
+      copy(c.A, SEG + (long long)(j - j0) * N);
+      nl_eval<double, N>(c, IN_A, 0.0, c.K1, nullptr);            // k1
+      nl_eval<double, N>(c, IN_2, h, A2, nullptr, U2);            // T = a1, a2
+      C* Osave = c.O;
+      c.O = A2;
+      nl_eval<double, N>(c, IN_3, h, A3, nullptr, U3);            // T += 2 a2, a3
+      c.O = A3;
+      nl_eval<double, N>(c, IN_4, h, nullptr, nullptr, U4, true); // T = beta, u4
+      c.O = Osave;
+      // reverse of A' = beta + h/6 a4, beta = E (v + h/6 T)
+      for (int x = tid; x < N; x += T1) {
+        const C E = EFac<double>::get(c.D[x], 0.5 * h);
+        const C ab = AB[x];
+        a.gD[x] = cadd(a.gD[x], cscale(cmul(ab, cconj(c.T[x])), 0.5 * h));
+        const C wb = cmul(cconj(E), ab);
+        const C tb = cscale(wb, h / 6);
+        VB[x] = wb;
+        A1B[x] = tb;
+        A2B[x] = cscale(tb, 2.0);
+        A3B[x] = cscale(tb, 2.0);
+        TMP[x] = cscale(ab, h / 6);                  // a4 bar
+      }
+      __syncthreads();
+      vjp_eval<N>(c, U4, TMP, AB, a.gG);             // u4 bar -> AB
+      for (int x = tid; x < N; x += T1) {            // u4 = E z, z = v + h a3
+        const C E = EFac<double>::get(c.D[x], 0.5 * h);
+        const C u4b = AB[x];
+        a.gD[x] = cadd(a.gD[x], cscale(cmul(u4b, cconj(U4[x])), 0.5 * h));
+        const C zb = cmul(cconj(E), u4b);
+        VB[x] = cadd(VB[x], zb);
+        A3B[x] = cadd(A3B[x], cscale(zb, h));
+      }
+      __syncthreads();
+      vjp_eval<N>(c, U3, A3B, TMP, a.gG);            // u3 bar
+      for (int x = tid; x < N; x += T1) {            // u3 = v + h/2 a2
+        VB[x] = cadd(VB[x], TMP[x]);
+        A2B[x] = cadd(A2B[x], cscale(TMP[x], h / 2));
+      }
+      __syncthreads();
+      vjp_eval<N>(c, U2, A2B, TMP, a.gG);            // u2 bar
+      for (int x = tid; x < N; x += T1) {            // u2 = v + h/2 a1, a1 = E k1
+        const C E = EFac<double>::get(c.D[x], 0.5 * h);
+        VB[x] = cadd(VB[x], TMP[x]);
+        const C a1b = cadd(A1B[x], cscale(TMP[x], h / 2));
+        const C a1 = cmul(E, c.K1[x]);
+        a.gD[x] = cadd(a.gD[x], cscale(cmul(a1b, cconj(a1)), 0.5 * h));
+        TMP[x] = cmul(cconj(E), a1b);                // k1 bar
+      }
+      __syncthreads();
+      vjp_eval<N>(c, c.A, TMP, AB, a.gG);            // through k1 = N(A)
+      for (int x = tid; x < N; x += T1) {            // v = E A
+        const C E = EFac<double>::get(c.D[x], 0.5 * h);
+        const C vb = VB[x];
+        const C v = cmul(E, c.A[x]);
+        a.gD[x] = cadd(a.gD[x], cscale(cmul(vb, cconj(v)), 0.5 * h));
+        AB[x] = cadd(AB[x], cmul(cconj(E), vb));
+      }
+      __syncthreads();
+    }
+  }
+  c.O = O0;
+  copy(a.A0bar, AB);
+}
+
+static __global__ void __launch_bounds__(T1, 1) k_uppe1d_adjoint(Adj1D a) {
+  extern __shared__ __align__(16) unsigned char smem[];
+  switch (a.b.inst[a.inst].log2n) {
+    case 6: adjoint_instance<64>(a, smem); break;
+    case 7: adjoint_instance<128>(a, smem); break;
+    case 8: adjoint_instance<256>(a, smem); break;
+    case 9: adjoint_instance<512>(a, smem); break;
+    case 10: adjoint_instance<1024>(a, smem); break;
+    case 11: adjoint_instance<2048>(a, smem); break;
+    case 12: adjoint_instance<4096>(a, smem); break;
+    case 13: adjoint_instance<8192>(a, smem); break;
+    default: break;
+  }
+}
+
+cudaError_t launch_uppe1d_adjoint(const Adj1D& a, size_t smem, cudaStream_t s);
 
 // launcher implemented once per precision (uppe1d_f32.cu / uppe1d_f64.cu)
 template <typename Rl> cudaError_t launch_uppe1d(const Batch1D& b, int nblocks, size_t smem, cudaStream_t s);
