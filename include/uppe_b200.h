@@ -69,6 +69,7 @@ typedef struct {
   double rho_nt;           /* neutral density (rounded to float32 as in :187)      */
   double ava_coef;         /* W_ava = ava_coef * I (0 for the gases)               */
   int plasma_on;           /* 0 disables the plasma terms                          */
+  const double* omega_abs; /* [Nt] omega + omega0 (photon number; NULL: not computed) */
 } uppe3d_desc;
 
 typedef struct {
@@ -135,6 +136,7 @@ typedef struct {
   double A_eff;            /* [m^2] for the plasma intensity                          */
   double Ui, sigma_drude, omega0_tau_c, rate_rec, rho_nt, ava_coef;   /* plasma constants */
   int hist_cap;            /* history slots (the reference saves <= 1501); 0 = none   */
+  double omega0;           /* carrier angular frequency (photon number; 0: not computed) */
 } uppe1d_inst_desc;
 
 typedef struct {
@@ -154,6 +156,9 @@ typedef struct {
   long long attempts, accepted;
   int status;              /* UPPE_STATUS_* bits; 8 = history capacity reached          */
   int hist_count;          /* saved history slots (slot 0 = A0)                        */
+  double energy;           /* sum |A|^2 dt of the final field [J]                      */
+  double photons;          /* photon number of the final field (NaN if omega0 = 0)     */
+  double peak_ion;         /* max rho/rho_nt over the initial and accepted states      */
 } uppe1d_result;
 
 typedef struct uppe1d_plan uppe1d_plan;
@@ -218,6 +223,13 @@ int uppe1d_propagate_noalloc(const uppe1d_inst_desc* inst, int precision, const 
                              const double* G, const double* H, int lut_n,
                              const void* lut_log10I, const void* lut_W, void* field,
                              uppe1d_result* result, uppe_stream_t stream);
+
+/* Diagnostics of the current 3D state: out3 = {pulse energy sum |A|^2 dx dy dt [J],
+ * photon number sum_omega E_omega / (hbar omega_abs) (omega_abs > 0), peak ionisation
+ * fraction max rho/rho_nt over the states at which steps started and the current
+ * state}.  The reference prints no diagnostics; these are the quantities its
+ * drivers compute from the returned field (src/3+1D-ERK4(3)IP UPPE/sim.py:140-249). */
+int uppe3d_diagnostics(uppe3d_plan* plan, double dx, double dy, double* out3, uppe_stream_t stream);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);

@@ -191,6 +191,20 @@ class Solver1D:
             out = out + self.plasma.term(A, self._dt)[0]
         return out
 
+    def diagnostics(self, A, t):
+        """energy sum |A|^2 dt and photon number sum_w E_w / (hbar w_abs), w_abs > 0."""
+        N = len(t)
+        dt = t[1] - t[0]
+        Ew = np.abs(fft(A)) ** 2 * dt / N
+        wa = 2 * np.pi * fftfreq(N, dt) + self.omega0
+        return float(np.sum(np.abs(A) ** 2) * dt), float(np.sum(Ew[wa > 0] / (1.054571817e-34 * wa[wa > 0])))
+
+    def ionization_fraction(self, A):
+        if self.plasma is None:
+            return 0.0
+        rho = self.plasma.term(A, self._dt)[1]
+        return float(rho.max()) / float(np.float32(self.plasma.rho_nt))
+
     def erk43_step(self, A, h):
         """erk43ip_method.py:256-286 (alpha1 always from N(A): the FSAL shortcut is
         bit-identical to it)."""

@@ -330,8 +330,29 @@ class Solver3D:
                 break
         return self._finish(A, z, log)
 
+    def ionization_fraction(self, A_t):
+        """max rho/rho_nt of a normalised time-domain state (media_physics.py:165-189)."""
+        m = self.medium
+        A_phys = A_t * self.A_scale
+        I = np.abs(A_phys) ** 2
+        W_ion = m.get_ionization_rate(I).astype(np.float32)
+        Nt = I.shape[-1]
+        rho, _ = plasma_scan(W_ion.reshape(-1, Nt), np.zeros((W_ion.size // Nt, Nt), np.float32),
+                             np.float32(1.0 / m.tau_rec), np.float32(self.dt), np.float32(m.rho_nt))
+        return float(rho.max()) / float(np.float32(m.rho_nt))
+
+    def diagnostics(self, A_t):
+        """energy sum |A|^2 dx dy dt, photon number sum E_w/(hbar w_abs), w_abs > 0."""
+        A = A_t * self.A_scale
+        E = float(np.sum(np.abs(A) ** 2)) * self.dx * self.dy * self.dt
+        Ew = np.sum(np.abs(sfft.fft(A, axis=-1)) ** 2, axis=(0, 1)) * self.dx * self.dy * self.dt / self.Nt
+        wa = np.fft.fftfreq(self.Nt, self.dt) * 2 * np.pi + self.omega0
+        ph = float(np.sum(Ew[wa > 0] / (1.054571817e-34 * wa[wa > 0])))
+        return E, ph
+
     def _finish(self, A, z, log):
         """solver_3d.py:215-233"""
+        self.last_state = A.copy()
         A = A * self.A_scale
         A_w_raw = sfft.fft(A, axis=-1)
         A_w_final = np.fft.fftshift(A_w_raw, axes=-1)

@@ -27,7 +27,7 @@ class Desc3D(ctypes.Structure):
                 ('filt', _P), ('kperp2', _P), ('damp', _P), ('lut_n', _I),
                 ('lut_log10I', _P), ('lut_W', _P), ('gamma_kerr', _D), ('gamma_hoke', _D),
                 ('Ui', _D), ('sigma_drude', _D), ('omega0_tau_c', _D), ('rate_rec', _D),
-                ('rho_nt', _D), ('ava_coef', _D), ('plasma_on', _I)]
+                ('rho_nt', _D), ('ava_coef', _D), ('plasma_on', _I), ('omega_abs', _P)]
 
 
 class Result3D(ctypes.Structure):
@@ -40,7 +40,7 @@ class InstDesc1D(ctypes.Structure):
                 ('min_step', _D), ('max_attempts', _LL), ('raman', _I), ('plasma', _I),
                 ('f_R', _D), ('A_eff', _D), ('Ui', _D), ('sigma_drude', _D),
                 ('omega0_tau_c', _D), ('rate_rec', _D), ('rho_nt', _D), ('ava_coef', _D),
-                ('hist_cap', _I)]
+                ('hist_cap', _I), ('omega0', _D)]
 
 
 class Desc1D(ctypes.Structure):
@@ -50,7 +50,7 @@ class Desc1D(ctypes.Structure):
 
 class Result1D(ctypes.Structure):
     _fields_ = [('z', _D), ('h', _D), ('err', _D), ('attempts', _LL), ('accepted', _LL),
-                ('status', _I), ('hist_count', _I)]
+                ('status', _I), ('hist_count', _I), ('energy', _D), ('photons', _D), ('peak_ion', _D)]
 
 
 STATUS_HIST_FULL = 8
@@ -71,6 +71,7 @@ SIGNATURES = {
     'uppe3d_get_spectrum': (_I, [_P, _P, _P]),
     'uppe3d_get_field': (_I, [_P, _P, _P]),
     'uppe3d_launches_per_step': (_I, [_P]),
+    'uppe3d_diagnostics': (_I, [_P, _D, _D, ctypes.POINTER(_D), _P]),
     'uppe1d_plan_create': (_I, [ctypes.POINTER(Desc1D), ctypes.POINTER(_P)]),
     'uppe1d_plan_destroy': (_I, [_P]),
     'uppe1d_field_elems': (_LL, [_P]),

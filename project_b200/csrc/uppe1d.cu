@@ -98,6 +98,7 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     q.pc.Ui = s.Ui; q.pc.sigma_half = s.sigma_drude / 2.0; q.pc.w0tc = s.omega0_tau_c;
     q.pc.rr = (double)(float)s.rate_rec; q.pc.dt = (double)(float)s.dt;
     q.pc.rho_nt = (double)(float)s.rho_nt; q.pc.ava = s.ava_coef;
+    q.omega0 = s.omega0;
     any_raman |= s.raman != 0;
     off += n;
     hoff += (long long)s.hist_cap * n;
@@ -212,6 +213,7 @@ extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double*
       results[i].z = r.z; results[i].h = r.h; results[i].err = r.err;
       results[i].attempts = r.attempts; results[i].accepted = r.accepted;
       results[i].status = r.status; results[i].hist_count = r.hist_count;
+      results[i].energy = r.energy; results[i].photons = r.photons; results[i].peak_ion = r.peak_ion;
     }
   }
   return 0;
@@ -230,6 +232,7 @@ static int run1(uppe1d_plan* p, Batch1D& b, uppe1d_result* results, cudaStream_t
       results[i].z = r.z; results[i].h = r.h; results[i].err = r.err;
       results[i].attempts = r.attempts; results[i].accepted = r.accepted;
       results[i].status = r.status; results[i].hist_count = r.hist_count;
+      results[i].energy = r.energy; results[i].photons = r.photons; results[i].peak_ion = r.peak_ion;
     }
   }
   return 0;

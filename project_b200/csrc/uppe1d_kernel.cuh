@@ -41,12 +41,14 @@ struct Inst1D {
   int raman, plasma;
   double f_R, A_eff;
   PlasmaConst pc;
+  double omega0;         // carrier angular frequency (photon number)
 };
 
 struct Res1D {
   double z, h, err;
   long long attempts, accepted;
   int status, hist_count;
+  double energy, photons, peak_ion;
 };
 
 struct Batch1D {
@@ -152,7 +154,7 @@ template <typename Rl> struct Ctx1 {
 // Returns false (nothing written) when the whole line has W_ion = 0 and no
 // avalanche, i.e. the term is identically zero.
 template <typename Rl, int N>
-__device__ bool plasma_line(Ctx1<Rl>& c) {
+__device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
   using C = typename CT<Rl>::T;
   constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
   const int tid = threadIdx.x;
@@ -222,6 +224,7 @@ __device__ bool plasma_line(Ctx1<Rl>& c) {
     rho0 = tid < NA ? c.starts[tid] : 0.0;
     __syncthreads();
   }
+  double ion = 0.0;
   if (tid < NA) {
     double rho = rho0;
     for (int t = tid * CH; t < tid * CH + CH; ++t) {
@@ -231,12 +234,21 @@ __device__ bool plasma_line(Ctx1<Rl>& c) {
       const double w = (double)(float)lut_eval<Rl>(c.lut, I);
       const double wa = (double)(float)(m.ava * (double)I);
       const double rho_t = rho;
+      ion = fmax(ion, rho_t);
       const double gen = rho_step(rho, w, wa, m);
       const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
       c.s[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
     }
+  }
+  if (ion_out) {   // block max of rho/rho_nt (every thread gets it)
+    ion = warp_max(ion / m.rho_nt);
+    if ((tid & 31) == 0) c.red[tid >> 5] = ion;
+    __syncthreads();
+    double mx = 0.0;
+    for (int wv = 0; wv < T1 / 32; ++wv) mx = fmax(mx, c.red[wv]);
+    *ion_out = fmax(*ion_out, mx);
   }
   __syncthreads();
   return true;
@@ -248,7 +260,7 @@ __device__ bool plasma_line(Ctx1<Rl>& c) {
 template <typename Rl, int N>
 __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename CT<Rl>::T* out,
                           typename CT<Rl>::T* hist_t, typename CT<Rl>::T* save_u = nullptr,
-                          bool input_only = false) {
+                          bool input_only = false, double* ion_out = nullptr) {
   using C = typename CT<Rl>::T;
   constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
@@ -327,7 +339,7 @@ __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename
   }
   __syncthreads();
   if (plasma) {
-    if (plasma_line<Rl, N>(c)) {
+    if (plasma_line<Rl, N>(c, ion_out)) {
       stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
       for (int w = tid; w < N; w += T1) out[w] = cadd(out[w], c.s[pad1(w)]);
       __syncthreads();
@@ -339,13 +351,14 @@ __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename
 // one erk43_step from the state (A, K1); leaves A4, a4' (A4P), a5 (O), beta (T);
 // returns the error of erk43ip_method.py:279-284
 template <typename Rl, int N>
-__device__ __noinline__ double attempt1(Ctx1<Rl>& c, double h, typename CT<Rl>::T* hist_t) {
+__device__ __noinline__ double attempt1(Ctx1<Rl>& c, double h, typename CT<Rl>::T* hist_t,
+                                        double* ion_cand = nullptr) {
   using C = typename CT<Rl>::T;
   const int tid = threadIdx.x;
   nl_eval<Rl, N>(c, IN_2, h, c.O, nullptr);     // alpha2
   nl_eval<Rl, N>(c, IN_3, h, c.O, nullptr);     // alpha3
   nl_eval<Rl, N>(c, IN_4, h, c.A4P, nullptr);   // alpha4'
-  const double nrm = nl_eval<Rl, N>(c, IN_5, h, c.O, hist_t);   // alpha5' = N(A4)
+  const double nrm = nl_eval<Rl, N>(c, IN_5, h, c.O, hist_t, nullptr, false, ion_cand);   // alpha5' = N(A4)
   double acc = 0.0;
   const Rl h30 = (Rl)(h / 30);
   for (int w = tid; w < N; w += T1) {
@@ -401,7 +414,8 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
   for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
   __syncthreads();
-  nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr);   // k1 = N(A)
+  double ion_peak = 0.0, ion_cand = 0.0;
+  nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr, nullptr, false, &ion_peak);   // k1 = N(A)
 
   // adaptive loop (erk43ip_method.py:294-367), evaluated identically by all threads
   const double L = in.L, tol = in.tol, max_step = in.max_step, min_step = in.min_step;
@@ -411,6 +425,7 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   auto cand = [&]() -> C* { return (hist && hcount < in.hist_cap) ? hist + (long long)hcount * N : nullptr; };
   auto accept = [&](double hh) {
     z += hh;
+    ion_peak = fmax(ion_peak, ion_cand);    // the accepted state's density (FSAL evaluation)
     C* t0 = c.A; c.A = c.A4; c.A4 = t0;     // state <- A4
     C* t1 = c.K1; c.K1 = c.O; c.O = t1;     // k1 <- alpha5' (FSAL)
     if (b.hlog) {                           // step log for the adjoint
@@ -433,7 +448,8 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
     const double* hs = b.hsched + (long long)i * b.nsched;
     for (int k = 0; k < b.nsched; ++k) {
       const double hh = hs[k];
-      err = attempt1<Rl, N>(c, hh, cand());
+      ion_cand = 0.0;
+      err = attempt1<Rl, N>(c, hh, cand(), &ion_cand);
       attempts += 1;
       if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
       accept(hh);
@@ -441,7 +457,8 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   }
   while (!b.hsched && z < L) {
     if (z + h > L) h = L - z;
-    err = attempt1<Rl, N>(c, h, cand());
+    ion_cand = 0.0;
+    err = attempt1<Rl, N>(c, h, cand(), &ion_cand);
     attempts += 1;
     if (!isfinite(err) || !isfinite(h)) { status |= UPPE_STATUS_NONFINITE; break; }
     if (err < tol) {
@@ -454,7 +471,8 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
       const double factor = 0.95 * pow(tol / (err + 1e-30), 0.25);
       h = fmax(h * fmax(factor, 0.1), min_step);
       if (h <= min_step) {   // forced step (:345-367)
-        err = attempt1<Rl, N>(c, h, cand());
+        ion_cand = 0.0;
+        err = attempt1<Rl, N>(c, h, cand(), &ion_cand);
         attempts += 1;
         status |= UPPE_STATUS_MIN_STEP;
         if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
@@ -467,6 +485,20 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
       break;
     }
   }
+  // energy sum |A|^2 dt and photon number (Parseval in omega), FP64, fixed order
+  double en = 0.0, ph = 0.0;
+  {
+    const double dw = 6.283185307179586476925286766559 / (N * in.dt);
+    for (int w = tid; w < N; w += T1) {
+      const C v = c.A[w];
+      const double a2 = (double)v.x * v.x + (double)v.y * v.y;
+      en += a2;
+      const double wa = in.omega0 + dw * (w < (N + 1) / 2 ? w : w - N);
+      if (wa > 0.0) ph += a2 / (1.054571817e-34 * wa);
+    }
+    en = block_sum(en, c.red) * in.dt / N;
+    ph = block_sum(ph, c.red) * in.dt / N;
+  }
   // final state back to the time domain
   for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
   __syncthreads();
@@ -477,6 +509,7 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
     Res1D r;
     r.z = z; r.h = h; r.err = err; r.attempts = attempts; r.accepted = accepted;
     r.status = status; r.hist_count = hist ? hcount : 0;
+    r.energy = en; r.photons = in.omega0 > 0.0 ? ph : NAN; r.peak_ion = ion_peak;
     b.res[i] = r;
   }
   __syncthreads();

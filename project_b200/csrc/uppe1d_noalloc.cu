@@ -138,6 +138,7 @@ extern "C" int uppe1d_propagate_noalloc(const uppe1d_inst_desc* s, int precision
   q.pc.Ui = s->Ui; q.pc.sigma_half = s->sigma_drude / 2.0; q.pc.w0tc = s->omega0_tau_c;
   q.pc.rr = (double)(float)s->rate_rec; q.pc.dt = (double)(float)s->dt;
   q.pc.rho_nt = (double)(float)s->rho_nt; q.pc.ava = s->ava_coef;
+  q.omega0 = s->omega0;
   const int order_counter[2] = {0, 0};   // the work-queue counter must start at zero
 
   Batch1D b;
@@ -199,6 +200,7 @@ extern "C" int uppe1d_propagate_noalloc(const uppe1d_inst_desc* s, int precision
     result->z = r.z; result->h = r.h; result->err = r.err;
     result->attempts = r.attempts; result->accepted = r.accepted;
     result->status = r.status; result->hist_count = 0;
+    result->energy = r.energy; result->photons = r.photons; result->peak_ion = r.peak_ion;
   }
   return 0;
 }

@@ -45,6 +45,7 @@ struct State3D {
   double err, err_num, err_den;
   double A_scale, inv_A_scale;
   unsigned long long red_norm, red_diff;
+  unsigned long long ion_bits;   // running max of rho/rho_nt over step-start and final states
   long long attempts, accepted, max_attempts;
   int fail_count, zidx, fresh, done, status, last_accept;
 };
@@ -513,6 +514,7 @@ k_xpass_sq(SpaceArgs a) {
 enum TMode { T_GENERAL = 0, T_FROM_Z = 1 };
 
 struct TArgs {
+  int diag;           // 1: evaluate even when the run is done (final-state diagnostics)
   State3D* st;
   Tables3D tb;
   Medium3D md;
@@ -576,7 +578,7 @@ k_tpass(TArgs a) {
   }
   __syncthreads();
   State3D* st = a.st;
-  if (st->done) return;
+  if (st->done && !a.diag) return;
   if (a.mode == T_FROM_Z && !st->fresh) return;
   const long long line = (long long)blockIdx.x * WPB + warp;
   const long long nlines = (long long)a.g.Nx * a.g.Ny;
@@ -663,6 +665,7 @@ k_tpass(TArgs a) {
     }
   }
   // Kerr (+ plasma) terms; exact per-sample density update from the chunk start
+  double ion = 0.0;
   {
     double rho = rho0;
 #pragma unroll
@@ -680,6 +683,7 @@ k_tpass(TArgs a) {
         else w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
         const double wa = (double)(float)(m.ava * (double)I);
         const double rho_t = rho;
+        ion = fmax(ion, rho_t);
         const double gen = rho_step(rho, w, wa, m);
         const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
         const double cr = loss - m.sigma_half * rho_t;
@@ -687,6 +691,10 @@ k_tpass(TArgs a) {
         sP[tpad(t)] = C{(Rl)cr * av.x - (Rl)ci * av.y, (Rl)cr * av.y + (Rl)ci * av.x};
       }
     }
+  }
+  if (plasma_line && a.mode == T_FROM_Z) {
+    ion = warp_max(ion / m.rho_nt);
+    if (lane == 0) atomic_max_nonneg(&st->ion_bits, ion);
   }
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sK, tw, lane, idx, wsync);
@@ -816,7 +824,7 @@ k_tpass_w(TArgs a) {
   }
   __syncthreads();
   State3D* st = a.st;
-  if (st->done) return;
+  if (st->done && !a.diag) return;
   if (a.mode == T_FROM_Z && !st->fresh) return;
   const long long line = (long long)blockIdx.x * WPB + warp;
   const long long nlines = (long long)a.g.Nx * a.g.Ny;
@@ -890,7 +898,7 @@ k_tpass_w(TArgs a) {
       rho0 = starts[lane];
     }
     __syncwarp();
-    double rho = rho0;
+    double rho = rho0, ion = 0.0;
     for (int i = 0; i < E; ++i) {
       const int t = t0 + i;
       const C av = S[tpad(t)];
@@ -899,11 +907,16 @@ k_tpass_w(TArgs a) {
       const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
       const double wa = (double)(float)(m.ava * (double)I);
       const double rho_t = rho;
+      ion = fmax(ion, rho_t);
       const double gen = rho_step(rho, w, wa, m);
       const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
       S[tpad(t)] = C{(Rl)cr * av.x - (Rl)ci * av.y, (Rl)cr * av.y + (Rl)ci * av.x};
+    }
+    if (a.mode == T_FROM_Z) {
+      ion = warp_max(ion / m.rho_nt);
+      if (lane == 0) atomic_max_nonneg(&st->ion_bits, ion);
     }
     __syncwarp();
 #pragma unroll
@@ -979,6 +992,7 @@ __global__ void k_set_scale(State3D* st) {
   if (!(s >= 1e-30)) s = 1.0;   // solver_3d.py:166-168
   st->A_scale = s;
   st->inv_A_scale = 1.0 / s;
+  st->ion_bits = 0ull;
   st->zidx = 0;
   st->fresh = 1;
   st->done = 0;
@@ -1154,6 +1168,8 @@ struct uppe3d_plan {
   Bufs3D b;
   std::vector<void*> allocs;
   cudaGraphExec_t g_attempt = nullptr, g_step = nullptr;
+  const double* wabs = nullptr;   // omega + omega0 per omega bin (photon number)
+  double* diag_buf = nullptr;     // per-block partial sums + 3 results
   cudaStream_t cap_stream = nullptr;
 };
 
@@ -1261,8 +1277,9 @@ static void launch_t_n(const TArgs& a, long long nlines, cudaStream_t s) {
 }
 
 template <typename Rl, int KIND>
-static int launch_t(uppe3d_plan* p, int mode, const void* in, void* out, cudaStream_t s) {
+static int launch_t(uppe3d_plan* p, int mode, const void* in, void* out, cudaStream_t s, int diag = 0) {
   TArgs a;
+  a.diag = diag;
   a.st = p->st; a.tb = p->tb; a.md = p->md; a.b = p->b; a.g = p->g;
   a.in = in; a.out = out; a.mode = mode;
   const long long nl = (long long)p->g.Nx * p->g.Ny;
@@ -1455,6 +1472,13 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
   UPPE_TRY(dev_upload(p, &ptr, d->filt, 8 * Nt)); p->tb.filt = (const double*)ptr;
   UPPE_TRY(dev_upload(p, &ptr, d->kperp2, 8 * (size_t)Nxy)); p->tb.q = (const double*)ptr;
   UPPE_TRY(dev_upload(p, &ptr, d->damp, 8 * (size_t)Nxy)); p->tb.damp = (const double*)ptr;
+  if (d->omega_abs) { UPPE_TRY(dev_upload(p, &ptr, d->omega_abs, 8 * Nt)); p->wabs = (const double*)ptr; }
+  {
+    cudaError_t e = cudaMalloc(&ptr, sizeof(double) * (2 * 592 + 3));
+    if (e != cudaSuccess) { snprintf(g_uppe_err, sizeof(g_uppe_err), "cudaMalloc diag: %s", cudaGetErrorString(e)); uppe3d_plan_destroy(p); return UPPE_ERR_CUDA; }
+    p->allocs.push_back(ptr);
+    p->diag_buf = (double*)ptr;
+  }
   {
     auto tx = p->dbl ? twiddles<double>(d->Nx) : twiddles<float>(d->Nx);
     auto ty = p->dbl ? twiddles<double>(d->Ny) : twiddles<float>(d->Ny);
@@ -1664,4 +1688,68 @@ extern "C" int uppe3d_profile_attempt(uppe3d_plan* p, int cap, float* ms, int* k
   for (auto e : rec.ev) cudaEventDestroy(e);
   *n = m < cap ? m : cap;
   return rc;
+}
+
+// ---- diagnostics: energy, photon number, peak ionisation fraction ------------
+namespace uppe {
+constexpr int kDiagBlocks = 592;
+constexpr double kHbar = 1.054571817e-34;
+
+template <typename Rl>
+__global__ void __launch_bounds__(256) k_diag_partial(const typename CT<Rl>::T* __restrict__ z,
+                                                      long long n, int Nt, const double* wabs,
+                                                      double* partial) {
+  double e = 0.0, ph = 0.0;
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const auto v = z[i];
+    const double a2 = (double)v.x * v.x + (double)v.y * v.y;
+    e += a2;
+    if (wabs) {
+      const double w = wabs[i % Nt];
+      if (w > 0.0) ph += a2 / (kHbar * w);
+    }
+  }
+  __shared__ double se[256], sp[256];
+  se[threadIdx.x] = e;
+  sp[threadIdx.x] = ph;
+  __syncthreads();
+  for (int o = 128; o > 0; o >>= 1) {
+    if (threadIdx.x < o) { se[threadIdx.x] += se[threadIdx.x + o]; sp[threadIdx.x] += sp[threadIdx.x + o]; }
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) { partial[2 * blockIdx.x] = se[0]; partial[2 * blockIdx.x + 1] = sp[0]; }
+}
+
+__global__ void k_diag_final(const double* partial, int nb, const State3D* st, double scale,
+                             double* out) {
+  if (threadIdx.x != 0) return;
+  double e = 0.0, ph = 0.0;
+  for (int b = 0; b < nb; ++b) { e += partial[2 * b]; ph += partial[2 * b + 1]; }
+  const double s2 = st->A_scale * st->A_scale * scale;
+  out[0] = e * s2;
+  out[1] = ph * s2;
+  out[2] = __longlong_as_double((long long)st->ion_bits);
+}
+}  // namespace uppe
+
+extern "C" int uppe3d_diagnostics(uppe3d_plan* p, double dx, double dy, double* out3, cudaStream_t s) {
+  if (!p || !out3) return UPPE_ERR_ARG;
+  // the final state's own density (the loop evaluated only step-start states)
+  int rc = p->dbl ? launch_t<double, 0>(p, T_FROM_Z, nullptr, p->b.tmp[0], s, 1)
+                  : launch_t<float, 0>(p, T_FROM_Z, nullptr, p->b.tmp[0], s, 1);
+  if (rc) return rc;
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  const void* z = p->b.z[p->st_host->zidx];
+  const long long n = p->g.npts;
+  if (p->dbl) k_diag_partial<double><<<kDiagBlocks, 256, 0, s>>>((const double2*)z, n, p->g.Nt, p->wabs, p->diag_buf);
+  else k_diag_partial<float><<<kDiagBlocks, 256, 0, s>>>((const float2*)z, n, p->g.Nt, p->wabs, p->diag_buf);
+  // sum_t |A|^2 dt = (dt / Nt) sum_omega |fft_t A|^2
+  const double scale = dx * dy * p->d.dt / (double)p->g.Nt;
+  k_diag_final<<<1, 32, 0, s>>>(p->diag_buf, kDiagBlocks, p->st, scale, p->diag_buf + 2 * kDiagBlocks);
+  UPPE_CK(cudaGetLastError());
+  UPPE_CK(cudaMemcpyAsync(out3, p->diag_buf + 2 * kDiagBlocks, 3 * sizeof(double), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  if (!p->wabs) out3[1] = NAN;
+  return 0;
 }

@@ -167,6 +167,7 @@ class ERK43IP_UPPE:
         d.raman = 1 if self.use_raman else 0
         d.f_R = self.f_R
         d.hist_cap = int(hist_cap)
+        d.omega0 = self.omega0
         p = self.plasma
         if p is not None:
             d.plasma = 1

@@ -53,7 +53,8 @@ class ERK43IP_UPPE_3D_Optimized:
             raise ValueError('the medium has no ionisation LUT')
         self._keep = [np.ascontiguousarray(a) for a in (
             self.a_w, self.k_sq, self.k_ref, self.valid, self.shock, self.filter,
-            self.K2_perp.ravel(), self.damp.ravel(), m.lut_log10I, m.lut_W)]
+            self.K2_perp.ravel(), self.damp.ravel(), m.lut_log10I, m.lut_W,
+            self.omega + m.omega0)]
         ptr = [a.ctypes.data for a in self._keep]
         d = _lib.Desc3D()
         d.Nx, d.Ny, d.Nt, d.precision, d.dt = self.Nx, self.Ny, self.Nt, self._prec, self.dt
@@ -69,6 +70,7 @@ class ERK43IP_UPPE_3D_Optimized:
         d.rho_nt = m.rho_nt
         d.ava_coef = m.avalanche_coef
         d.plasma_on = 1 if m.plasma else 0
+        d.omega_abs = ptr[10]
         plan = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             _lib.check(self._lib.uppe3d_plan_create(ctypes.byref(d), ctypes.byref(plan)),
@@ -131,6 +133,13 @@ class ERK43IP_UPPE_3D_Optimized:
         _lib.check(self._lib.uppe3d_get_field(self._plan, ctypes.c_void_p(out.data_ptr()),
                                               _lib.stream_ptr(stream)), 'uppe3d_get_field')
         return out
+
+    def diagnostics(self, stream=None):
+        """{'energy' [J], 'photons', 'peak_ionization'} of the current state (device)."""
+        out = (ctypes.c_double * 3)()
+        _lib.check(self._lib.uppe3d_diagnostics(self._plan, self.dx, self.dy, out, _lib.stream_ptr(stream)),
+                   'uppe3d_diagnostics')
+        return {'energy': out[0], 'photons': out[1], 'peak_ionization': out[2]}
 
     # ---- the reference surface ---------------------------------------------------
     def propagate(self, A0, L, tol=1e-4, max_step=1e-2, min_step=1e-9, return_gpu=False,

@@ -120,3 +120,21 @@ def test_batched_instances_match_individual_oracle_runs():
     for f, r0, r in zip(finals, refs, res):
         assert r.status == 0
         assert rel_l2(f, r0) < 1e-10
+
+
+def test_diagnostics_vs_oracle():
+    """Energy, photon number and peak ionisation fraction (initial and accepted states)."""
+    from oracle.inputs import gaussian_pulse
+    osol, psol = _plasma_pair()
+    t = np.linspace(-0.5e-12, 0.5e-12, 1024)
+    fwhm = 30e-15
+    A0 = gaussian_pulse(t, 2e9 * fwhm * np.sqrt(np.pi / (4 * np.log(2))), fwhm)
+    zo, Ao, _, log = osol.propagate(A0, t, L=0.05, tol=1e-6)
+    peak = max(osol.ionization_fraction(a) for a in Ao)     # every accepted state is in the history
+    Eo, pho = osol.diagnostics(Ao[-1], t)
+    psol.propagate(A0, t, L=0.05, tol=1e-6)
+    r = psol.last_result
+    assert peak > 1e-8
+    assert abs(r.energy - Eo) <= 1e-10 * Eo
+    assert abs(r.photons - pho) <= 1e-10 * pho
+    assert abs(r.peak_ion - peak) <= 1e-8 * peak

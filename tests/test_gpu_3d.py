@@ -142,3 +142,27 @@ def test_long_lines_vs_oracle(Nt, precision, W0):
         sol.commit(acc)
     tol = 1e-10 if precision == 'double' else 1e-4
     assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < tol
+
+
+def test_diagnostics_vs_oracle():
+    """Energy, photon number and peak ionisation fraction of a propagation with
+    significant ionisation (MPI-like table), complex128, against the oracle."""
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(N=16, Nt=64, W0=3e9, I_peak=5e16)
+    z, freq, Ao, log = osol.propagate(A0, 0.01, tol=1e-5)
+    # peak over the states at which steps started and the final state
+    An = (A0 / osol.A_scale).astype(np.complex128)
+    peak = osol.ionization_fraction(An)
+    for z0, h, err, acc in log:
+        if acc:
+            An = osol.erk43_step(An, h)[0]
+            peak = max(peak, osol.ionization_fraction(An))
+    Eo, pho = osol.diagnostics(osol.last_state)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(lam, 1.0, 'double', True, lut=lut), precision='double')
+    sol.propagate(A0, 0.01, tol=1e-5)
+    d = sol.diagnostics()
+    assert peak > 1e-6
+    assert abs(d['energy'] - Eo) <= 1e-10 * Eo
+    assert abs(d['photons'] - pho) <= 1e-10 * pho
+    assert abs(d['peak_ionization'] - peak) <= 1e-8 * peak
