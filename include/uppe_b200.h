@@ -231,6 +231,21 @@ int uppe1d_propagate_noalloc(const uppe1d_inst_desc* inst, int precision, const 
  * drivers compute from the returned field (src/3+1D-ERK4(3)IP UPPE/sim.py:140-249). */
 int uppe3d_diagnostics(uppe3d_plan* plan, double dx, double dy, double* out3, uppe_stream_t stream);
 
+/* Record the accepted step sizes of later uppe3d_propagate runs in hlog (device,
+ * cap entries; NULL stops recording).  No reference counterpart (the adjoint's input). */
+int uppe3d_set_step_log(uppe3d_plan* plan, double* hlog, long long cap, uppe_stream_t stream);
+/* Workspace of uppe3d_adjoint in bytes. */
+long long uppe3d_adjoint_work_bytes(const uppe3d_plan* plan, int nsteps, int K);
+/* Reverse-mode derivative of the frozen-schedule 3D propagation (Kerr + self-steepening,
+ * dispersion, diffraction, filter, absorber; plasma terms held fixed).  hlog_host: the
+ * nsteps accepted step sizes (host); A0: device input field (time domain, physical);
+ * Zbar: device cotangent of the final state in the (x, y, omega) domain with the
+ * state normalised by A_scale (dL = Re sum conj(Zbar) dZ); A0bar: device output,
+ * cotangent of A0 (time domain).  Checkpoints every K steps, recomputes within
+ * segments.  Overwrites the plan's state.  No reference counterpart. */
+int uppe3d_adjoint(uppe3d_plan* plan, const double* hlog_host, int nsteps, int K, const void* A0,
+                   const void* Zbar, void* A0bar, void* work, uppe_stream_t stream);
+
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,

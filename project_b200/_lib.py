@@ -72,6 +72,9 @@ SIGNATURES = {
     'uppe3d_get_field': (_I, [_P, _P, _P]),
     'uppe3d_launches_per_step': (_I, [_P]),
     'uppe3d_diagnostics': (_I, [_P, _D, _D, ctypes.POINTER(_D), _P]),
+    'uppe3d_set_step_log': (_I, [_P, _P, _LL, _P]),
+    'uppe3d_adjoint_work_bytes': (_LL, [_P, _I, _I]),
+    'uppe3d_adjoint': (_I, [_P, _P, _I, _I, _P, _P, _P, _P, _P]),
     'uppe1d_plan_create': (_I, [ctypes.POINTER(Desc1D), ctypes.POINTER(_P)]),
     'uppe1d_plan_destroy': (_I, [_P]),
     'uppe1d_field_elems': (_LL, [_P]),

@@ -167,3 +167,70 @@ class CapillaryCompression:
         A_L = propagate_1d(self.input_field(knots), D, G, L, self.template, self.t, tol=tol, K=K)
         tl = torch.fft.ifft(torch.fft.fft(A_L).abs())          # ideal phase removal
         return -(tl.real ** 2 + tl.imag ** 2).max()
+
+
+# ---------------------------------------------------------------------------
+# 3+1D: gradients of the final field with respect to the input field
+# ---------------------------------------------------------------------------
+class Propagate3D(torch.autograd.Function):
+    """Final time-domain field A(x, y, t) of ERK43IP_UPPE_3D_Optimized.propagate as a
+    differentiable function of the input field A0 (frozen accepted steps, device
+    adjoint ``uppe3d_adjoint``; the plasma terms are held fixed in the derivative)."""
+
+    @staticmethod
+    def forward(ctx, A0, solver, L, tol, max_step, min_step, K):
+        solver.propagate(A0, L, tol=tol, max_step=max_step, min_step=min_step, return_gpu=True,
+                         log_steps=True)
+        out = solver.field().clone()
+        ctx.solver, ctx.steps, ctx.K = solver, np.ascontiguousarray(solver.last_steps), int(K)
+        ctx.save_for_backward(solver._as_device_field(A0))
+        Propagate3D.last_steps = ctx.steps
+        return out
+
+    @staticmethod
+    def backward(ctx, gA):
+        (A0,) = ctx.saved_tensors
+        sol = ctx.solver
+        lib = _lib.load()
+        Nt = sol.Nt
+        A_scale = float(A0.abs().max())
+        Zbar = (torch.fft.fft(gA.to(sol.complex_dtype), dim=-1) * (A_scale / Nt)).contiguous()
+        nb = lib.uppe3d_adjoint_work_bytes(sol._plan, len(ctx.steps), ctx.K)
+        work = torch.empty(nb, dtype=torch.uint8, device=A0.device)
+        A0bar = torch.empty_like(A0)
+        _lib.check(lib.uppe3d_adjoint(sol._plan, ctx.steps.ctypes.data, len(ctx.steps), ctx.K,
+                                      ctypes.c_void_p(A0.data_ptr()), ctypes.c_void_p(Zbar.data_ptr()),
+                                      ctypes.c_void_p(A0bar.data_ptr()), ctypes.c_void_p(work.data_ptr()),
+                                      _lib.stream_ptr()), 'uppe3d_adjoint')
+        Propagate3D.workspace_bytes = nb
+        return A0bar, None, None, None, None, None, None
+
+
+def propagate_3d(A0, solver, L, tol=1e-4, max_step=1e-2, min_step=1e-9, K=32):
+    return Propagate3D.apply(A0, solver, L, tol, max_step, min_step, K)
+
+
+class FilamentZernike:
+    """3+1D filament objective: a Gaussian beam (w0, energy, FWHM) with a wavefront
+    sum_j c_j Z_j (Noll j = 1..jmax over an aperture) and an input GDD applied along
+    t; loss = - on-axis fluence of the output, sum_t |A(0, 0, t)|^2 dt."""
+
+    def __init__(self, solver, w0, energy, fwhm, aperture_radius, jmax=15):
+        from .pulses import gaussian_beam, zernike_basis
+        self.sol = solver
+        dev = solver.device
+        self.env = torch.from_numpy(gaussian_beam(solver.x, solver.y, solver.t, w0, energy, fwhm)).to(dev)
+        self.Z = torch.from_numpy(zernike_basis(solver.x, solver.y, aperture_radius, jmax)).to(dev)
+        om = 2 * np.pi * np.fft.fftfreq(solver.Nt, solver.dt)
+        self.w2 = torch.from_numpy(0.5 * om ** 2).to(dev)
+        self.ix, self.iy = solver.Nx // 2, solver.Ny // 2
+
+    def input_field(self, coeffs, gdd):
+        phase = torch.einsum('j,jxy->xy', coeffs, self.Z)
+        A = self.env * torch.exp(1j * phase)[:, :, None]
+        return torch.fft.ifft(torch.fft.fft(A, dim=-1) * torch.exp(1j * gdd * self.w2), dim=-1)
+
+    def loss(self, coeffs, gdd, L, tol=1e-4, K=32):
+        A = propagate_3d(self.input_field(coeffs, gdd).to(self.sol.complex_dtype), self.sol, L, tol=tol, K=K)
+        a = A[self.ix, self.iy, :].to(torch.complex128)
+        return -(a.real ** 2 + a.imag ** 2).sum() * self.sol.dt

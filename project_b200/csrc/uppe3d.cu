@@ -46,6 +46,8 @@ struct State3D {
   double A_scale, inv_A_scale;
   unsigned long long red_norm, red_diff;
   unsigned long long ion_bits;   // running max of rho/rho_nt over step-start and final states
+  double* hlog;                  // accepted step sizes (for the adjoint), or null
+  long long hlog_cap;
   long long attempts, accepted, max_attempts;
   int fail_count, zidx, fresh, done, status, last_accept;
 };
@@ -71,7 +73,8 @@ struct Tables3D {
   Lut lut;               // ionisation table (field precision)
 };
 
-enum SpaceMode { XINV = 0, XINV_Z, XFWD, XFWD_Z, YMID1, YMID1R, YMID2, YMID3, YMID4, YFWD5 };
+enum SpaceMode { XINV = 0, XINV_Z, XFWD, XFWD_Z, YMID1, YMID1R, YMID2, YMID3, YMID4, YFWD5,
+                 YPLAIN_INV, YPLAIN_FWD };
 
 struct Bufs3D {
   void* z[2];     // accepted state / candidate (x, y, omega)
@@ -190,6 +193,8 @@ struct SpaceArgs {
   const void* in;     // primary input (pass temporaries)
   void* out;          // primary output
   int mode;
+  void* save_u;       // y passes: also store the stage input u (kx, ky, omega) here
+  double scale;       // plain y passes: output scale
 };
 
 template <typename C> struct TileIdx {
@@ -301,6 +306,19 @@ k_space(SpaceArgs a) {
     return;
   }
 
+  if (mode == YPLAIN_INV || mode == YPLAIN_FWD) {   // plain y FFT (adjoint passes)
+    load_tile<C, N, NTHR>(s, in, base, stride, tid);
+    __syncthreads();
+    if (mode == YPLAIN_INV) stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+    else stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    if (a.scale != 1.0) {
+      const Rl sc = (Rl)a.scale;
+      for (int e = tid; e < N * kW; e += NTHR) s[e] = cscale(s[e], sc);
+      __syncthreads();
+    }
+    store_tile<C, N, NTHR>(s, out, base, stride, tid);
+    return;
+  }
   // ---------------- y passes (stage algebra in the (kx, ky, omega) domain) ----
   C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
   C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
@@ -396,12 +414,14 @@ k_space(SpaceArgs a) {
       const C a1 = cmul(k1, Ef);
       tsum[gi] = a1;
       s[idx(w, n)] = cadd(v, cscale(a1, h2R));
+      if (a.save_u) reinterpret_cast<C*>(a.save_u)[gi] = s[idx(w, n)];   // u2
     } else if (mode == YMID2) {
       const C a2 = s[idx(w, n)];
       const C v = cmul(opA[i], Ef);
       const C ts = opB[i];
       tsum[gi] = cadd(ts, cscale(a2, (Rl)2));
       s[idx(w, n)] = cadd(v, cscale(a2, h2R));
+      if (a.save_u) reinterpret_cast<C*>(a.save_u)[gi] = s[idx(w, n)];   // u3
     } else {   // YMID3
       const C a3 = s[idx(w, n)];
       const C v = cmul(opA[i], Ef);
@@ -409,6 +429,7 @@ k_space(SpaceArgs a) {
       const C beta = cmul(cadd(v, cscale(ts, h6R)), Ef);
       tsum[gi] = beta;
       s[idx(w, n)] = cmul(cadd(v, cscale(a3, hR)), Ef);
+      if (a.save_u) reinterpret_cast<C*>(a.save_u)[gi] = s[idx(w, n)];   // u4
     }
   }
   if (mode == YMID4 || mode == YFWD5) {
@@ -1026,6 +1047,7 @@ __global__ void k_controller(State3D* st) {
   }
   const double tol = st->tol, min_step = st->min_step, max_step = st->max_step;
   if (err < tol || h <= min_step * 1.01) {
+    if (st->hlog && st->accepted < st->hlog_cap) st->hlog[st->accepted] = h;
     st->fail_count = (h <= min_step * 1.01 && err > tol) ? st->fail_count + 1 : 0;
     if (st->fail_count > 0) st->status |= UPPE_STATUS_MIN_STEP;
     st->z += h;
@@ -1169,6 +1191,8 @@ struct uppe3d_plan {
   std::vector<void*> allocs;
   cudaGraphExec_t g_attempt = nullptr, g_step = nullptr;
   const double* wabs = nullptr;   // omega + omega0 per omega bin (photon number)
+  void* save_u[3] = {nullptr, nullptr, nullptr};   // adjoint recompute: u2, u3, u4
+  double pass_scale = 1.0;                          // plain y passes
   double* diag_buf = nullptr;     // per-block partial sums + 3 results
   cudaStream_t cap_stream = nullptr;
 };
@@ -1233,6 +1257,9 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   using C = typename CT<Rl>::T;
   SpaceArgs a;
   a.st = p->st; a.tb = p->tb; a.b = p->b; a.g = p->g; a.in = in; a.out = out; a.mode = mode;
+  a.save_u = (mode == YMID1 || mode == YMID1R) ? p->save_u[0]
+           : mode == YMID2 ? p->save_u[1] : mode == YMID3 ? p->save_u[2] : nullptr;
+  a.scale = p->pass_scale;
   const bool xpass = mode <= XFWD_Z;
   const int N = xpass ? p->g.Nx : p->g.Ny;
   const long long nouter = xpass ? p->g.Ny : p->g.Nx;
@@ -1752,4 +1779,332 @@ extern "C" int uppe3d_diagnostics(uppe3d_plan* p, double dx, double dy, double* 
   UPPE_CK(cudaStreamSynchronize(s));
   if (!p->wabs) out3[1] = NAN;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint (reverse mode) of the 3D ERK4(3)-IP propagation for the Kerr +
+// self-steepening response with dispersion, diffraction, filter and absorber.
+// The plasma terms are held fixed (their derivative is not propagated; exact
+// while the ionisation rate is zero over the field).  Convention:
+// dL = Re sum conj(xb) dx.
+// ---------------------------------------------------------------------------
+namespace uppe {
+
+enum AdjPoint { AP_BOUND = 0, AP_R1, AP_R2, AP_R3, AP_R4, AP_R5 };
+
+struct AdjPointArgs {
+  Tables3D tb;
+  Geom g;
+  int mode;
+  double h;
+  void *ab, *vb, *a1b, *a2b, *a3b, *tmp;
+  const void *acur, *beta, *u4, *zb;
+};
+
+// pointwise transposed stage algebra over all (kx, ky, omega) (AP_R*) and the step
+// boundary multiply c(x, y, omega) = filter(omega) exp(-damp(x, y) h) / (Nx Ny) (AP_BOUND)
+template <typename Rl>
+__global__ void __launch_bounds__(256) k_adj_point(AdjPointArgs a) {
+  using C = typename CT<Rl>::T;
+  const long long n = (long long)a.g.Nx * a.g.Ny * a.g.Nt;
+  const int Nt = a.g.Nt;
+  const double h = a.h, h2 = 0.5 * h;
+  C* ab = reinterpret_cast<C*>(a.ab);
+  C* vb = reinterpret_cast<C*>(a.vb);
+  C* a1b = reinterpret_cast<C*>(a.a1b);
+  C* a2b = reinterpret_cast<C*>(a.a2b);
+  C* a3b = reinterpret_cast<C*>(a.a3b);
+  C* tmp = reinterpret_cast<C*>(a.tmp);
+  const C* acur = reinterpret_cast<const C*>(a.acur);
+  const C* beta = reinterpret_cast<const C*>(a.beta);
+  const C* u4 = reinterpret_cast<const C*>(a.u4);
+  const C* zb = reinterpret_cast<const C*>(a.zb);
+  for (long long i = blockIdx.x * 256LL + threadIdx.x; i < n; i += (long long)gridDim.x * 256) {
+    const int iw = (int)(i % Nt);
+    const long long xy = i / Nt;
+    if (a.mode == AP_BOUND) {
+      const double c = a.tb.filt[iw] * exp(-a.tb.damp[xy] * h) / ((double)a.g.Nx * a.g.Ny);
+      tmp[i] = cscale(zb[i], (Rl)c);
+      continue;
+    }
+    const OmegaCol oc(a.tb, iw);
+    const C E = IPFactor<Rl>::get(a.tb, oc, iw, a.tb.q[xy], h2);
+    const C Ec = cconj(E);
+    if (a.mode == AP_R1) {            // A' = beta + h/6 a4, beta = E (v + h/6 T)
+      const C ab_ = ab[i];
+      const C wb = cmul(Ec, ab_);
+      const C tb = cscale(wb, (Rl)(h / 6));
+      vb[i] = wb;
+      a1b[i] = tb;
+      a2b[i] = cscale(tb, (Rl)2);
+      a3b[i] = cscale(tb, (Rl)2);
+      tmp[i] = cscale(ab_, (Rl)(h / 6));
+    } else if (a.mode == AP_R2) {     // u4 = E (v + h a3)
+      const C zb_ = cmul(Ec, ab[i]);
+      vb[i] = cadd(vb[i], zb_);
+      a3b[i] = cadd(a3b[i], cscale(zb_, (Rl)h));
+    } else if (a.mode == AP_R3) {     // u3 = v + h/2 a2
+      vb[i] = cadd(vb[i], tmp[i]);
+      a2b[i] = cadd(a2b[i], cscale(tmp[i], (Rl)(h / 2)));
+    } else if (a.mode == AP_R4) {     // u2 = v + h/2 a1, a1 = E k1
+      vb[i] = cadd(vb[i], tmp[i]);
+      const C a1b_ = cadd(a1b[i], cscale(tmp[i], (Rl)(h / 2)));
+      tmp[i] = cmul(Ec, a1b_);
+    } else {                          // v = E A
+      ab[i] = cadd(ab[i], cmul(Ec, vb[i]));
+    }
+  }
+  (void)acur; (void)beta; (void)u4;
+}
+
+// VJP of the t-line part: in U' = F*_xy u and X' = F*_xy nb (both (x, y, omega)),
+// out = F_t(ab) / Ntot with a = F*_t U' / Ntot, kb = F*_t(mask shock X'),
+// ab = 2|a|^2 conj(c) kb + c a^2 conj(kb), c = i gk A_scale^2.
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_tvjp(TArgs a, const void* xin) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* sU = tw + NT + warp * 2 * PAD;
+  C* sX = sU + PAD;
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(a.tb.twt)[i];
+  __syncthreads();
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  if (line >= (long long)a.g.Nx * a.g.Ny) return;
+  const C* uin = reinterpret_cast<const C*>(a.in) + line * NT;
+  const C* xn = reinterpret_cast<const C*>(xin) + line * NT;
+  C* out = reinterpret_cast<C*>(a.out) + line * NT;
+  const double ntot = (double)NT * a.g.Nx * a.g.Ny;
+  const Rl inv = (Rl)(1.0 / ntot);
+  const Rl gp = (Rl)(a.md.gk * a.st->A_scale * a.st->A_scale);   // c = i gp
+  for (int i = 0; i < E; ++i) {
+    const int wi = lane + 32 * i;
+    sU[tpad(wi)] = uin[wi];
+    const Rl ms = a.tb.valid[wi] ? (Rl)a.tb.shock[wi] : (Rl)0;
+    sX[tpad(wi)] = cscale(xn[wi], ms);
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sU, tw, lane, LineIdx(), WarpSync());
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sX, tw, lane, LineIdx(), WarpSync());
+  for (int i = 0; i < E; ++i) {
+    const int t = lane + 32 * i;
+    const C av = cscale(sU[tpad(t)], inv);
+    const C kb = sX[tpad(t)];
+    const Rl I2 = (Rl)2 * (av.x * av.x + av.y * av.y);
+    // 2|a|^2 conj(c) kb with conj(c) = -i gp ;  c a^2 conj(kb) with c = i gp
+    const C t1 = cscale(C{kb.y, -kb.x}, gp * I2);
+    const C a2 = cmul(av, av);
+    const C t2p = cmul(a2, cconj(kb));
+    const C t2 = cscale(C{-t2p.y, t2p.x}, gp);
+    sU[tpad(t)] = cadd(t1, t2);
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sU, tw, lane, LineIdx(), WarpSync());
+  for (int i = 0; i < E; ++i) {
+    const int wi = lane + 32 * i;
+    out[wi] = cscale(sU[tpad(wi)], inv);
+  }
+}
+
+// out = scale * (unnormalised FFT along t of in), DIR = -1 forward, +1 inverse
+template <typename Rl, int NT, int WPB, int DIR>
+__global__ void __launch_bounds__(WPB * 32) k_tline(TArgs a, double scale) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* sK = tw + NT + warp * 2 * PAD;
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(a.tb.twt)[i];
+  __syncthreads();
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  if (line >= (long long)a.g.Nx * a.g.Ny) return;
+  const C* src = reinterpret_cast<const C*>(a.in) + line * NT;
+  C* dst = reinterpret_cast<C*>(a.out) + line * NT;
+  for (int i = 0; i < E; ++i) sK[tpad(lane + 32 * i)] = src[lane + 32 * i];
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, DIR, 1, C>(sK, tw, lane, LineIdx(), WarpSync());
+  const Rl sc = (Rl)scale;
+  for (int i = 0; i < E; ++i) dst[lane + 32 * i] = cscale(sK[tpad(lane + 32 * i)], sc);
+}
+
+__global__ void k_set_state(State3D* st, int zidx, int fresh, double h) {
+  st->zidx = zidx;
+  st->fresh = fresh;
+  st->h = h;
+  st->done = 0;
+}
+
+__global__ void k_set_log(State3D* st, double* hlog, long long cap) {
+  st->hlog = hlog;
+  st->hlog_cap = cap;
+}
+
+}  // namespace uppe
+
+template <typename Rl, int NT, int KIND>
+static int adj_tlaunch_n(uppe3d_plan* p, const void* in, const void* xin, void* out, double scale,
+                         cudaStream_t s) {
+  TArgs a;
+  memset(&a, 0, sizeof(a));
+  a.st = p->st; a.tb = p->tb; a.md = p->md; a.b = p->b; a.g = p->g; a.in = in; a.out = out;
+  constexpr int WPB = TLaunch<NT, Rl>::WPB;
+  const long long nl = (long long)p->g.Nx * p->g.Ny;
+  const unsigned nb = (unsigned)((nl + WPB - 1) / WPB);
+  const size_t smem = TLaunch<NT, Rl>::smem();
+  cudaError_t e;
+  if (KIND == 0) {
+    e = cudaFuncSetAttribute(k_tvjp<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) k_tvjp<Rl, NT, WPB><<<nb, WPB * 32, smem, s>>>(a, xin);
+  } else {
+    e = cudaFuncSetAttribute(k_tline<Rl, NT, WPB, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) k_tline<Rl, NT, WPB, +1><<<nb, WPB * 32, smem, s>>>(a, scale);
+  }
+  if (e != cudaSuccess) return UPPE_ERR_CUDA;
+  return cudaGetLastError() == cudaSuccess ? 0 : UPPE_ERR_CUDA;
+}
+
+template <typename Rl, int KIND>
+static int adj_tlaunch(uppe3d_plan* p, const void* in, const void* xin, void* out, double scale,
+                       cudaStream_t s) {
+  switch (p->g.Nt) {
+#define UPPE_AT(n) case n: return adj_tlaunch_n<Rl, n, KIND>(p, in, xin, out, scale, s);
+    UPPE_AT(32) UPPE_AT(64) UPPE_AT(128) UPPE_AT(256) UPPE_AT(512) UPPE_AT(1024) UPPE_AT(2048)
+#undef UPPE_AT
+    default: return UPPE_ERR_SIZE;
+  }
+}
+
+template <typename Rl>
+static int adj_point(uppe3d_plan* p, int mode, double h, void* const* w, const void* zb, cudaStream_t s) {
+  AdjPointArgs a;
+  a.tb = p->tb; a.g = p->g; a.mode = mode; a.h = h;
+  a.ab = w[0]; a.vb = w[1]; a.a1b = w[2]; a.a2b = w[3]; a.a3b = w[4]; a.tmp = w[5];
+  a.acur = p->b.acur; a.beta = p->b.tsum; a.u4 = nullptr; a.zb = zb;
+  k_adj_point<Rl><<<148 * 8, 256, 0, s>>>(a);
+  return cudaGetLastError() == cudaSuccess ? 0 : UPPE_ERR_CUDA;
+}
+
+template <typename Rl>
+static int adj_plain_y(uppe3d_plan* p, int mode, const void* in, void* out, double scale, cudaStream_t s) {
+  p->pass_scale = scale;
+  const int rc = launch_space<Rl>(p, mode, in, out, s);
+  p->pass_scale = 1.0;
+  return rc;
+}
+
+// VJP of N at u with cotangent nb -> out (all (kx, ky, omega)); uses tmp[0..2]
+template <typename Rl>
+static int adj_vjp(uppe3d_plan* p, const void* u, const void* nb, void* out, cudaStream_t s) {
+  void* const* t = p->b.tmp;
+  int rc = 0;
+  rc |= adj_plain_y<Rl>(p, YPLAIN_INV, u, t[0], 1.0, s);
+  rc |= launch_space<Rl>(p, XINV, t[0], t[1], s);              // U'
+  rc |= adj_plain_y<Rl>(p, YPLAIN_INV, nb, t[0], 1.0, s);
+  rc |= launch_space<Rl>(p, XINV, t[0], t[2], s);              // X'
+  rc |= adj_tlaunch<Rl, 0>(p, t[1], t[2], t[0], 1.0, s);       // F_t(ab)/Ntot
+  rc |= launch_space<Rl>(p, XFWD, t[0], t[1], s);
+  rc |= adj_plain_y<Rl>(p, YPLAIN_FWD, t[1], out, 1.0, s);
+  return rc;
+}
+
+template <typename Rl>
+static int adjoint_impl(uppe3d_plan* p, const double* hl, int nsteps, int K, const void* A0,
+                        const void* Zbar, void* A0bar, void* work, cudaStream_t s) {
+  const size_t F = p->csz * (size_t)p->g.npts;
+  unsigned char* wb = static_cast<unsigned char*>(work);
+  void* W[6];                       // ab, vb, a1b, a2b, a3b, tmp
+  for (int k = 0; k < 6; ++k) W[k] = wb + k * F;
+  void* U2 = wb + 6 * F; void* U3 = wb + 7 * F; void* U4 = wb + 8 * F; void* ZB = wb + 9 * F;
+  const int nseg = (nsteps + K - 1) / K;
+  unsigned char* CK = wb + 10 * F;
+  unsigned char* SEG = CK + (size_t)(nseg > 0 ? nseg : 1) * F;
+  int rc = uppe3d_set_field(p, A0, s);
+  if (rc) return rc;
+  int zidx = 0;
+  Recorder rec;
+  rec.s = s;
+  auto attempt = [&](double h) {
+    k_set_h<<<1, 1, 0, s>>>(p->st, h);
+    return enqueue_attempt<Rl>(p, rec);
+  };
+  // forward replay with checkpoints every K steps
+  UPPE_CK(cudaMemcpyAsync(CK, p->b.z[zidx], F, cudaMemcpyDeviceToDevice, s));
+  for (int j = 0; j < nsteps; ++j) {
+    rc |= attempt(hl[j]);
+    k_commit<<<1, 1, 0, s>>>(p->st, 1);
+    zidx ^= 1;
+    if ((j + 1) % K == 0 && j + 1 < nsteps)
+      UPPE_CK(cudaMemcpyAsync(CK + (size_t)((j + 1) / K) * F, p->b.z[zidx], F, cudaMemcpyDeviceToDevice, s));
+  }
+  UPPE_CK(cudaMemcpyAsync(ZB, Zbar, F, cudaMemcpyDeviceToDevice, s));
+  for (int sg = nseg - 1; sg >= 0; --sg) {
+    const int j0 = sg * K, j1 = nsteps < j0 + K ? nsteps : j0 + K;
+    UPPE_CK(cudaMemcpyAsync(p->b.z[0], CK + (size_t)sg * F, F, cudaMemcpyDeviceToDevice, s));
+    UPPE_CK(cudaMemcpyAsync(SEG, p->b.z[0], F, cudaMemcpyDeviceToDevice, s));
+    k_set_state<<<1, 1, 0, s>>>(p->st, 0, 1, hl[j0]);
+    int zi = 0;
+    for (int j = j0; j < j1 - 1; ++j) {
+      rc |= attempt(hl[j]);
+      k_commit<<<1, 1, 0, s>>>(p->st, 1);
+      zi ^= 1;
+      UPPE_CK(cudaMemcpyAsync(SEG + (size_t)(j - j0 + 1) * F, p->b.z[zi], F, cudaMemcpyDeviceToDevice, s));
+    }
+    for (int j = j1 - 1; j >= j0; --j) {
+      const double h = hl[j];
+      // recompute the step from its start state, saving u2, u3, u4
+      UPPE_CK(cudaMemcpyAsync(p->b.z[0], SEG + (size_t)(j - j0) * F, F, cudaMemcpyDeviceToDevice, s));
+      k_set_state<<<1, 1, 0, s>>>(p->st, 0, 1, h);
+      p->save_u[0] = U2; p->save_u[1] = U3; p->save_u[2] = U4;
+      rc |= enqueue_attempt<Rl>(p, rec);
+      p->save_u[0] = p->save_u[1] = p->save_u[2] = nullptr;
+      // boundary: A4 bar = F_xy(c Zbar) / (Nx Ny)
+      rc |= adj_point<Rl>(p, AP_BOUND, h, W, ZB, s);
+      rc |= launch_space<Rl>(p, XFWD, W[5], p->b.tmp[0], s);
+      rc |= adj_plain_y<Rl>(p, YPLAIN_FWD, p->b.tmp[0], W[0], 1.0, s);
+      // stages
+      rc |= adj_point<Rl>(p, AP_R1, h, W, nullptr, s);
+      rc |= adj_vjp<Rl>(p, U4, W[5], W[0], s);            // u4 bar -> ab
+      rc |= adj_point<Rl>(p, AP_R2, h, W, nullptr, s);
+      rc |= adj_vjp<Rl>(p, U3, W[4], W[5], s);            // u3 bar -> tmp
+      rc |= adj_point<Rl>(p, AP_R3, h, W, nullptr, s);
+      rc |= adj_vjp<Rl>(p, U2, W[3], W[5], s);            // u2 bar -> tmp
+      rc |= adj_point<Rl>(p, AP_R4, h, W, nullptr, s);
+      rc |= adj_vjp<Rl>(p, p->b.acur, W[5], W[0], s);     // through k1 = N(A) -> ab
+      rc |= adj_point<Rl>(p, AP_R5, h, W, nullptr, s);
+      // Zbar of the step start: A = F_xy Z -> Zbar = F*_xy(ab)
+      rc |= adj_plain_y<Rl>(p, YPLAIN_INV, W[0], p->b.tmp[0], 1.0, s);
+      rc |= launch_space<Rl>(p, XINV, p->b.tmp[0], ZB, s);
+    }
+  }
+  // Z0 = F_t(A0 / A_scale) -> A0 bar = F*_t(Zbar) / A_scale (A_scale is read on the host)
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  rc |= adj_tlaunch<Rl, 1>(p, ZB, nullptr, A0bar, 1.0 / p->st_host->A_scale, s);
+  UPPE_CK(cudaGetLastError());
+  return rc;
+}
+
+extern "C" long long uppe3d_adjoint_work_bytes(const uppe3d_plan* p, int nsteps, int K) {
+  if (!p || nsteps < 0 || K <= 0) return -1;
+  const long long nseg = (nsteps + K - 1) / K;
+  return (10LL + (nseg > 0 ? nseg : 1) + K) * (long long)p->csz * p->g.npts;
+}
+
+extern "C" int uppe3d_set_step_log(uppe3d_plan* p, double* hlog, long long cap, cudaStream_t s) {
+  if (!p || cap < 0) return UPPE_ERR_ARG;
+  k_set_log<<<1, 1, 0, s>>>(p->st, hlog, hlog ? cap : 0);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nsteps, int K, const void* A0,
+                              const void* Zbar, void* A0bar, void* work, cudaStream_t s) {
+  if (!p || !hlog_host || nsteps < 0 || K <= 0 || !A0 || !Zbar || !A0bar || !work) return UPPE_ERR_ARG;
+  return p->dbl ? adjoint_impl<double>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s)
+                : adjoint_impl<float>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s);
 }

@@ -79,3 +79,38 @@ def gaussian_beam(x, y, t, w0, pulse_energy, pulse_fwhm, dtype=np.complex128):
     E = np.sum(sp ** 2) * np.sum(tp ** 2) * (x[1] - x[0]) * (y[1] - y[0]) * (t[1] - t[0])
     s = np.sqrt(pulse_energy / E)
     return ((s * sp)[:, :, None] * tp[None, None, :]).astype(dtype)
+
+
+def noll_nm(j):
+    """(n, m) of Zernike polynomial number j in Noll's ordering (j >= 1)."""
+    n, j1 = 0, j - 1
+    while j1 > n:
+        n += 1
+        j1 -= n
+    m = (-1) ** j * ((n % 2) + 2 * int((j1 + ((n + 1) % 2)) / 2))
+    return n, m
+
+
+def zernike(j, rho, theta):
+    """Orthonormal Zernike polynomial Z_j (Noll) on the unit disk; rho is clipped to 1
+    outside the aperture so the phase screen stays bounded there."""
+    from math import factorial
+    n, m = noll_nm(j)
+    am = abs(m)
+    r = np.minimum(np.asarray(rho, dtype=np.float64), 1.0)
+    R = np.zeros_like(r)
+    for k in range((n - am) // 2 + 1):
+        R += ((-1) ** k * factorial(n - k)
+              / (factorial(k) * factorial((n + am) // 2 - k) * factorial((n - am) // 2 - k))) * r ** (n - 2 * k)
+    if m == 0:
+        return np.sqrt(n + 1.0) * R
+    ang = np.cos(m * theta) if m > 0 else np.sin(am * theta)
+    return np.sqrt(2.0 * (n + 1.0)) * R * ang
+
+
+def zernike_basis(x, y, aperture_radius, jmax=15):
+    """[jmax, Nx, Ny] array of Z_1..Z_jmax over the (x, y) grid."""
+    X, Y = np.meshgrid(np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64), indexing='ij')
+    rho = np.sqrt(X ** 2 + Y ** 2) / aperture_radius
+    th = np.arctan2(Y, X)
+    return np.stack([zernike(j, rho, th) for j in range(1, jmax + 1)])

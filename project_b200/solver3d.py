@@ -141,9 +141,17 @@ class ERK43IP_UPPE_3D_Optimized:
                    'uppe3d_diagnostics')
         return {'energy': out[0], 'photons': out[1], 'peak_ionization': out[2]}
 
+    def replay(self, A0, steps, stream=None):
+        """Frozen-schedule forward map: every step in ``steps`` accepted."""
+        self.set_field(A0, stream)
+        for h in steps:
+            self.attempt(float(h), stream)
+            self.commit(True, stream)
+        return self.field(stream=stream)
+
     # ---- the reference surface ---------------------------------------------------
     def propagate(self, A0, L, tol=1e-4, max_step=1e-2, min_step=1e-9, return_gpu=False,
-                  max_attempts=0, stream=None, out=None):
+                  max_attempts=0, stream=None, out=None, log_steps=False):
         """solver_3d.py:162-233 -> (z_reached, freq_axis_hz, A_w_final).
 
         ``out``: optional host tensor (e.g. pinned) that receives the spectrum.
@@ -153,12 +161,22 @@ class ERK43IP_UPPE_3D_Optimized:
         with ``last_result.status & STATUS_NONFINITE`` set.
         """
         self.set_field(A0, stream)
+        hlog = None
+        if log_steps:   # accepted step sizes, for the adjoint
+            cap = int(max_attempts) if max_attempts and max_attempts > 0 else 1 << 20
+            hlog = torch.zeros(cap, dtype=torch.float64, device=self.device)
+            _lib.check(self._lib.uppe3d_set_step_log(self._plan, ctypes.c_void_p(hlog.data_ptr()), cap,
+                                                     _lib.stream_ptr(stream)), 'uppe3d_set_step_log')
         r = _lib.Result3D()
         _lib.check(self._lib.uppe3d_propagate(self._plan, float(L), float(tol), float(max_step),
                                               float(min_step), int(max_attempts), ctypes.byref(r),
                                               _lib.stream_ptr(stream)), 'uppe3d_propagate')
         self.last_result = r
         self.A_scale = r.A_scale
+        if hlog is not None:
+            self.last_steps = hlog[:int(r.accepted)].cpu().numpy()
+            _lib.check(self._lib.uppe3d_set_step_log(self._plan, None, 0, _lib.stream_ptr(stream)),
+                       'uppe3d_set_step_log')
         A_w = self.spectrum(stream=stream)
         if return_gpu:
             return r.z, self.freq_axis_hz, A_w
