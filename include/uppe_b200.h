@@ -192,15 +192,17 @@ int uppe1d_propagate_schedule(uppe1d_plan* plan, void* field, const double* hsch
 /* Workspace of uppe1d_adjoint, in complex128 elements. */
 long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K);
 /* Reverse-mode derivative of one instance's frozen-schedule propagation (complex128
- * plan; Kerr + self-steepening + dispersion + loss; no Raman/plasma).  Replays the
- * forward with a checkpoint every K steps and recomputes within segments.  Inputs
- * (device): hlog[nsteps], A0 (time domain), Abar = dL/dA_L in the omega domain
- * (dL = Re sum conj(Abar) dA).  Outputs (device): A0bar = dL/dfft(A0), gD = dL/dD,
- * gG = dL/dG (the tables of uppe1d_desc), rhs = D A_L + N(A_L) (so dL/dL = Re
- * sum conj(Abar) rhs).  No reference counterpart (the reference is not differentiable). */
+ * plan; Kerr + self-steepening + dispersion + loss + the plasma term without
+ * avalanche; no Raman).  Replays the forward with a checkpoint every K steps and
+ * recomputes within segments.  Inputs (device): hlog[nsteps], A0 (time domain),
+ * Abar = dL/dA_L in the omega domain (dL = Re sum conj(Abar) dA).  Outputs (device):
+ * A0bar = dL/dfft(A0), gD = dL/dD, gG = dL/dG (the tables of uppe1d_desc), rhs =
+ * D A_L + N(A_L) (so dL/dL = Re sum conj(Abar) rhs), gPlasma[3] = dL/d(rho_nt,
+ * sigma_drude, omega0_tau_c) (required for plasma instances, else may be NULL).
+ * No reference counterpart (the reference is not differentiable). */
 int uppe1d_adjoint(uppe1d_plan* plan, int inst, const double* hlog, int nsteps, int K,
                    const void* A0, const void* Abar, void* A0bar, void* gD, double* gG, void* rhs,
-                   void* work, uppe_stream_t stream);
+                   double* gPlasma, void* work, uppe_stream_t stream);
 
 /* Allocation-free single propagation, for callers that cannot allocate device
  * memory (a host framework that owns the CUDA allocator and forbids cudaMalloc
@@ -237,7 +239,8 @@ int uppe3d_set_step_log(uppe3d_plan* plan, double* hlog, long long cap, uppe_str
 /* Workspace of uppe3d_adjoint in bytes. */
 long long uppe3d_adjoint_work_bytes(const uppe3d_plan* plan, int nsteps, int K);
 /* Reverse-mode derivative of the frozen-schedule 3D propagation (Kerr + self-steepening,
- * dispersion, diffraction, filter, absorber; plasma terms held fixed).  hlog_host: the
+ * dispersion, diffraction, filter, absorber, the plasma terms without avalanche; no
+ * n4 term).  hlog_host: the
  * nsteps accepted step sizes (host); A0: device input field (time domain, physical);
  * Zbar: device cotangent of the final state in the (x, y, omega) domain with the
  * state normalised by A_scale (dL = Re sum conj(Zbar) dZ); A0bar: device output,

@@ -84,7 +84,7 @@ SIGNATURES = {
     'uppe1d_propagate_logged': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe1d_propagate_schedule': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe1d_adjoint_work_elems': (_LL, [_I, _I, _I]),
-    'uppe1d_adjoint': (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P]),
+    'uppe1d_adjoint': (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     'uppe1d_propagate_noalloc': (_I, [ctypes.POINTER(InstDesc1D), _I, _P, _P, _P, _I, _P, _P, _P,
                                       ctypes.POINTER(Result1D), _P]),
     'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),

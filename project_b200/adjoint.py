@@ -7,10 +7,11 @@ steps, recomputation within segments, transposed ERK4(3)-IP stages with the
 conjugate interaction-picture factor, vector-Jacobian products of the Kerr +
 self-steepening term.  Differentiable inputs: the time-domain input field, the
 dispersion table D(omega) (so anything D depends on, e.g. pressure), the
-nonlinear table G(omega) = gamma (w_abs/w0)(n0/n(w)), and the length L (through
-dA_L/dL = D A_L + N(A_L)).  complex128 only; Raman and plasma terms have no
-adjoint here.  torch.fft only converts cotangents between the time and omega
-domains at the boundary.
+nonlinear table G(omega) = gamma (w_abs/w0)(n0/n(w)), the length L (through
+dA_L/dL = D A_L + N(A_L)) and, for plasma instances, the plasma parameters
+(rho_nt, sigma_drude, omega0 tau_c).  complex128 only; the Raman response and
+avalanche ionisation have no adjoint here.  torch.fft only converts cotangents
+between the time and omega domains at the boundary.
 """
 import ctypes
 
@@ -25,13 +26,14 @@ C0 = 299792458.0
 
 class Propagate1D(torch.autograd.Function):
     @staticmethod
-    def forward(ctx, A0, D, G, L, solver, t, tol, max_step, min_step, K):
+    def forward(ctx, A0, D, G, L, plasma_par, solver, t, tol, max_step, min_step, K):
         lib = _lib.load()
         inst = solver.instance(t, float(L), tol, max_step, min_step)
         inst['D'] = D.detach().cpu().numpy().astype(np.complex128)
         inst['G'] = G.detach().cpu().numpy().astype(np.float64)
-        if inst['desc'].raman or inst['desc'].plasma:
-            raise NotImplementedError('the adjoint covers Kerr + self-steepening (no Raman/plasma)')
+        if inst['desc'].raman:
+            raise NotImplementedError('the adjoint covers Kerr, self-steepening and plasma (no Raman)')
+        _set_plasma(inst, plasma_par)
         bp = BatchedPropagator([inst], precision='double', device=A0.device)
         field = A0.detach().to(torch.complex128).contiguous().clone()
         cap = 2_000_000 if inst['desc'].max_attempts <= 0 else int(inst['desc'].max_attempts)
@@ -47,6 +49,7 @@ class Propagate1D(torch.autograd.Function):
         ctx.bp, ctx.hlog, ctx.nsteps, ctx.K = bp, hlog, int(r.accepted), int(K)
         Propagate1D.last_steps = hlog[:int(r.accepted)].cpu().numpy()
         ctx.result = r
+        ctx.plasma = bool(inst['desc'].plasma)
         ctx.save_for_backward(A0.detach().to(torch.complex128).contiguous())
         return field
 
@@ -63,21 +66,33 @@ class Propagate1D(torch.autograd.Function):
         gD = torch.empty(N, dtype=torch.complex128, device=dev)
         gG = torch.empty(N, dtype=torch.float64, device=dev)
         rhs = torch.empty(N, dtype=torch.complex128, device=dev)
+        gPl = torch.zeros(3, dtype=torch.float64, device=dev)
         P = lambda x: ctypes.c_void_p(x.data_ptr())
         _lib.check(lib.uppe1d_adjoint(ctx.bp._plan, 0, P(ctx.hlog), ctx.nsteps, ctx.K, P(A0), P(Abar),
-                                      P(A0bar), P(gD), P(gG), P(rhs), P(work), _lib.stream_ptr()),
+                                      P(A0bar), P(gD), P(gG), P(rhs), P(gPl), P(work), _lib.stream_ptr()),
                    'uppe1d_adjoint')
         gA0 = torch.fft.ifft(A0bar) * N
         gL = (torch.conj(Abar) * rhs).real.sum()
-        return gA0, gD, gG, gL, None, None, None, None, None, None
+        return gA0, gD, gG, gL, (gPl if ctx.plasma else None), None, None, None, None, None, None
 
 
-def replay_1d(A0, D, G, solver, t, hs):
+def _set_plasma(inst, plasma_par):
+    """Plasma parameters (rho_nt, sigma_drude, omega0 tau_c) of a plasma instance."""
+    if plasma_par is None:
+        return
+    if not inst['desc'].plasma:
+        raise ValueError('plasma parameters given for an instance without the plasma term')
+    v = [float(x) for x in plasma_par.detach().cpu()]
+    inst['desc'].rho_nt, inst['desc'].sigma_drude, inst['desc'].omega0_tau_c = v
+
+
+def replay_1d(A0, D, G, solver, t, hs, plasma_par=None):
     """Forward map with a frozen step sequence hs (every step accepted), on the device."""
     lib = _lib.load()
     inst = solver.instance(np.asarray(t, dtype=np.float64), float(np.sum(hs)), 1.0, 1.0, 1e-30)
     inst['D'] = D.detach().cpu().numpy().astype(np.complex128)
     inst['G'] = G.detach().cpu().numpy().astype(np.float64)
+    _set_plasma(inst, plasma_par)
     bp = BatchedPropagator([inst], precision='double', device=A0.device)
     field = A0.detach().to(torch.complex128).contiguous().clone()
     hsd = torch.as_tensor(np.asarray(hs, dtype=np.float64), device=A0.device)
@@ -88,12 +103,14 @@ def replay_1d(A0, D, G, solver, t, hs):
     return field
 
 
-def propagate_1d(A0, D, G, L, solver, t, tol=1e-6, max_step=1e-2, min_step=1e-11, K=32):
-    """Differentiable final field A(L) (time domain) of a 1D propagation."""
+def propagate_1d(A0, D, G, L, solver, t, tol=1e-6, max_step=1e-2, min_step=1e-11, K=32,
+                 plasma_par=None):
+    """Differentiable final field A(L) (time domain) of a 1D propagation;
+    plasma_par = (rho_nt, sigma_drude, omega0 tau_c) for a solver with a plasma term."""
     if not torch.is_tensor(L):
         L = torch.tensor(float(L), dtype=torch.float64)
-    return Propagate1D.apply(A0, D, G, L, solver, np.asarray(t, dtype=np.float64), tol, max_step,
-                             min_step, K)
+    return Propagate1D.apply(A0, D, G, L, plasma_par, solver, np.asarray(t, dtype=np.float64), tol,
+                             max_step, min_step, K)
 
 
 # ---------------------------------------------------------------------------
@@ -113,14 +130,16 @@ def spline_basis(x_eval, x_knots):
 
 
 class CapillaryCompression:
-    """Argon capillary (Taylor dispersion, loss, Kerr with self-steepening) whose
+    """Argon capillary (Taylor dispersion, loss, Kerr with self-steepening and,
+    with ``plasma``, the ionisation/plasma term with I = |A|^2 / A_eff) whose
     input spectral phase is a cubic spline over n_knots knots spanning the band
     where the input spectrum exceeds 1 % of its peak.  Loss = -peak power of the
-    output after ideal phase removal (the transform-limited output pulse)."""
+    output after ideal phase removal (the transform-limited output pulse).
+    Pressure P scales beta2, beta3, n2, rho_nt (2.45e25 P) and 1/tau_c (190 fs / P)."""
 
     def __init__(self, t, A0_time, n_knots=64, lam=800e-9, radius=125e-6, beta2=15e-30, beta3=15e-45,
-                 n2_per_bar=1e-23, loss_db_per_m=0.5, device='cuda'):
-        from .solver1d import ERK43IP_UPPE
+                 n2_per_bar=1e-23, loss_db_per_m=0.5, device='cuda', plasma=False, lut=None):
+        from .solver1d import ERK43IP_UPPE, GasPlasma1D
         self.t = np.asarray(t, dtype=np.float64)
         self.N = len(self.t)
         self.dev = torch.device(device)
@@ -139,9 +158,10 @@ class CapillaryCompression:
         self.B = torch.from_numpy(spline_basis(self.omega, self.knots_x)).to(self.dev)
         self.spec0 = torch.from_numpy(spec).to(self.dev)
         # solver template: the tables are replaced by the differentiable ones below
+        self.plasma = GasPlasma1D(self.A_eff, 1.0, lam, lut=lut) if plasma else None
         self.template = ERK43IP_UPPE(material='argon_gas', n2=n2_per_bar, beam_radius=0.65 * radius,
                                      center_wavelength=lam, alpha=self.alpha, use_raman=False,
-                                     taylor=(beta2, beta3), precision='double')
+                                     taylor=(beta2, beta3), precision='double', plasma=self.plasma)
         om = torch.from_numpy(self.omega).to(self.dev)
         self.poly = 0.5 * beta2 * om ** 2 + (1.0 / 6.0) * beta3 * om ** 3
         wa = self.omega0 + om
@@ -158,13 +178,24 @@ class CapillaryCompression:
         G = gamma * (self.wa / self.omega0) * (1.0 / n_safe)
         return D.to(torch.complex128), G.to(torch.float64)
 
+    def plasma_params(self, P):
+        """(rho_nt, sigma_drude, omega0 tau_c) at pressure P (media_physics.py:412-419)."""
+        if self.plasma is None:
+            return None
+        from .solver1d import E_CHARGE, EPS0, M_E
+        tau_c = 190e-15 / P
+        w = self.omega0
+        sigma = (E_CHARGE ** 2 * tau_c) / (C0 * EPS0 * 1.0 * M_E * (1.0 + w ** 2 * tau_c ** 2))
+        return torch.stack([2.45e25 * P, sigma, w * tau_c]).to(torch.float64)
+
     def input_field(self, knots):
         phase = self.B @ knots
         return torch.fft.ifft(self.spec0 * torch.exp(1j * phase))
 
     def loss(self, knots, P, L, tol=1e-6, K=32):
         D, G = self.tables(P)
-        A_L = propagate_1d(self.input_field(knots), D, G, L, self.template, self.t, tol=tol, K=K)
+        A_L = propagate_1d(self.input_field(knots), D, G, L, self.template, self.t, tol=tol, K=K,
+                           plasma_par=self.plasma_params(P))
         tl = torch.fft.ifft(torch.fft.fft(A_L).abs())          # ideal phase removal
         return -(tl.real ** 2 + tl.imag ** 2).max()
 
@@ -175,7 +206,7 @@ class CapillaryCompression:
 class Propagate3D(torch.autograd.Function):
     """Final time-domain field A(x, y, t) of ERK43IP_UPPE_3D_Optimized.propagate as a
     differentiable function of the input field A0 (frozen accepted steps, device
-    adjoint ``uppe3d_adjoint``; the plasma terms are held fixed in the derivative)."""
+    adjoint ``uppe3d_adjoint``: Kerr, self-steepening and the plasma terms)."""
 
     @staticmethod
     def forward(ctx, A0, solver, L, tol, max_step, min_step, K):

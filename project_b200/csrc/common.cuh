@@ -265,4 +265,73 @@ struct AffineStep {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Reverse mode of the plasma term P(a) = c a (media_physics.py:165-203),
+//   c = -Ui gen / (2 I + 1e-30) - (sigma/2)(1 + i omega0 tau_c) rho,
+// with I = alpha |a|^2, W = lut(I), and the density update of rho_step for
+// w_av = 0.  Cotangent convention: dL = Re sum conj(xb) dx.
+// ---------------------------------------------------------------------------
+
+// dW/dI of lut_eval: the slope of the bracketing interval over (I + 1e-30) ln 10;
+// 0 where log10(I) is clipped to the table ends or below the table's zero run.
+template <typename Rl>
+__device__ __forceinline__ double lut_slope(const Lut& L, Rl I) {
+  const Rl* xp = reinterpret_cast<const Rl*>(L.x);
+  const Rl* fp = reinterpret_cast<const Rl*>(L.w);
+  const int n = L.n;
+  const Rl x = (sizeof(Rl) == 8) ? (Rl)log10((double)I + 1e-30) : (Rl)log10f((float)I + 1e-30f);
+  const Rl x0 = __ldg(xp), x1 = __ldg(xp + n - 1);
+  if (!(x > x0) || !(x < x1)) return 0.0;
+  if ((double)x <= L.zero_x) return 0.0;
+  int j = (int)floor(((double)x - L.x0) * L.inv_dx);
+  j = j < 0 ? 0 : (j > n - 1 ? n - 1 : j);
+  while (j < n - 1 && __ldg(xp + j + 1) <= x) ++j;
+  while (j > 0 && __ldg(xp + j) > x) --j;
+  if (j >= n - 1) return 0.0;
+  const double slope = ((double)__ldg(fp + j + 1) - (double)__ldg(fp + j)) /
+                       ((double)__ldg(xp + j + 1) - (double)__ldg(xp + j));
+  return slope / (((double)I + 1e-30) * 2.302585092994046);
+}
+
+// One sample.  cur = density before the update, W / dW = rate and slope at I,
+// (ar, ai) = field sample, (qr, qi) = cotangent of the term's sample.  Gives the
+// reverse recurrence lam_t = A lam_{t+1} + B for lam = cotangent of the density.
+// With OUT, lam_next = lam_{t+1} gives the field cotangent (oar, oai) and adds
+// d/d(rho_nt, sigma_drude, omega0 tau_c) into g (when g is not null).
+template <bool OUT>
+__device__ __forceinline__ void plasma_rev(const PlasmaConst& m, const AffineStep& aff, double alpha,
+                                           double cur, double W, double dW, double I, double ar,
+                                           double ai, double qr, double qi, double& A, double& B,
+                                           double lam_next = 0.0, double* oar = nullptr,
+                                           double* oai = nullptr, double* g = nullptr) {
+  const double den = 2.0 * I + 1e-30;
+  const double kr = m.sigma_half, ki = m.sigma_half * m.w0tc;
+  double depl = (m.rho_nt - cur) / m.rho_nt;
+  const bool dpos = depl >= 0.0;
+  if (!dpos) depl = 0.0;
+  const double gen = W * m.rho_nt * depl;
+  const double r = cur * aff.e + gen * aff.sf;
+  const bool hi = r > m.rho_nt, lo = r < 0.0;
+  const double sr = qr * ar + qi * ai, si = qr * ai - qi * ar;   // s = conj(q) a
+  const double genb = -m.Ui / den * sr;
+  const double rhob = -(kr * sr - ki * si);
+  const double gw = dpos ? W : 0.0;                               // d gen / d rho_nt
+  A = (hi || lo) ? 0.0 : (aff.e - gw * aff.sf);
+  B = rhob - genb * gw;
+  if constexpr (OUT) {
+    const double lam_eff = (hi || lo) ? 0.0 : lam_next;
+    const double Wb = dpos ? (genb + lam_eff * aff.sf) * (m.rho_nt * depl) : 0.0;
+    const double Ib = 2.0 * m.Ui * gen / (den * den) * sr + Wb * dW;
+    const double cr = -m.Ui * gen / den - kr * cur, ci = -ki * cur;
+    *oar = cr * qr + ci * qi + 2.0 * alpha * Ib * ar;             // conj(c) q + 2 alpha Ib a
+    *oai = cr * qi - ci * qr + 2.0 * alpha * Ib * ai;
+    if (g) {
+      g[0] += genb * gw + (hi ? lam_next : (lo ? 0.0 : lam_next * gw * aff.sf));
+      const double gkr = -cur * sr, gki = cur * si;                // d/d kr, d/d ki
+      g[1] += 0.5 * gkr + 0.5 * m.w0tc * gki;                      // kr = sigma/2, ki = sigma w0tc/2
+      g[2] += m.sigma_half * gki;
+    }
+  }
+}
+
 }  // namespace uppe

@@ -266,7 +266,7 @@ extern "C" long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K) {
 
 extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int nsteps, int K,
                               const void* A0, const void* Abar, void* A0bar, void* gD, double* gG,
-                              void* rhs, void* work, cudaStream_t s) {
+                              void* rhs, double* gPlasma, void* work, cudaStream_t s) {
   g_uppe_err[0] = 0;
   if (!p || inst < 0 || inst >= p->ninst || !hlog || nsteps < 0 || K <= 0 || !A0 || !Abar ||
       !A0bar || !gD || !gG || !rhs || !work)
@@ -276,9 +276,13 @@ extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int 
     return UPPE_ERR_ARG;
   }
   const Inst1D& q = p->h_inst[inst];
-  if (q.raman || q.plasma) {
+  if (q.raman || (q.plasma && q.pc.ava != 0.0)) {
     snprintf(g_uppe_err, sizeof(g_uppe_err),
-             "uppe1d_adjoint: Raman and plasma terms have no adjoint here (Kerr + steepening only)");
+             "uppe1d_adjoint: the Raman response and avalanche ionisation have no adjoint here");
+    return UPPE_ERR_ARG;
+  }
+  if (q.plasma && !gPlasma) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err), "uppe1d_adjoint: a plasma instance needs gPlasma[3]");
     return UPPE_ERR_ARG;
   }
   Adj1D a;
@@ -293,6 +297,7 @@ extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int 
   a.gD = (double2*)gD;
   a.gG = gG;
   a.rhs = (double2*)rhs;
+  a.gPl = gPlasma;
   a.work = (double2*)work;
   UPPE1_CK(launch_uppe1d_adjoint(a, p->smem, s));
   return 0;

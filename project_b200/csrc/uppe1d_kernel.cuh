@@ -149,12 +149,12 @@ template <typename Rl> struct Ctx1 {
   Lut lut;
 };
 
-// plasma term P(t) = (loss + defocus)(t) * a(t) into the shared line, from the
-// time-domain field in GA (media_physics.py:156-203 with I = |A|^2 / A_eff).
-// Returns false (nothing written) when the whole line has W_ion = 0 and no
-// avalanche, i.e. the term is identically zero.
+// Density at the start of each thread's chunk of the line (time-domain field in
+// GA): a block scan of the chunks' affine maps, or lane 0's exact serial update
+// when a clamp binds.  Returns false when the whole line has W_ion = 0 and no
+// avalanche (the density stays 0).
 template <typename Rl, int N>
-__device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
+__device__ bool density_starts(Ctx1<Rl>& c, double& rho0) {
   using C = typename CT<Rl>::T;
   constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
   const int tid = threadIdx.x;
@@ -178,7 +178,6 @@ __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
   const bool any_block = __syncthreads_or(any_w) || m.ava != 0.0;
   if (!any_block) return false;
   const bool all_ok = __syncthreads_and(ok);
-  double rho0;
   if (all_ok) {
     // block exclusive scan of affine maps (c1,d1) then (c2,d2) = (c1 c2, c2 d1 + d2)
     const int lane = tid & 31, warp = tid >> 5;
@@ -224,6 +223,22 @@ __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
     rho0 = tid < NA ? c.starts[tid] : 0.0;
     __syncthreads();
   }
+  return true;
+}
+
+// plasma term P(t) = (loss + defocus)(t) * a(t) into the shared line, from the
+// time-domain field in GA (media_physics.py:156-203 with I = |A|^2 / A_eff).
+// Returns false (nothing written) when the whole line has W_ion = 0 and no
+// avalanche, i.e. the term is identically zero.
+template <typename Rl, int N>
+__device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
+  using C = typename CT<Rl>::T;
+  constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
+  const int tid = threadIdx.x;
+  double rho0 = 0.0;
+  if (!density_starts<Rl, N>(c, rho0)) return false;
+  const PlasmaConst& m = c.in->pc;
+  const double Aeff = c.in->A_eff;
   double ion = 0.0;
   if (tid < NA) {
     double rho = rho0;
@@ -550,22 +565,119 @@ __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
 // VJP of N(u) = i G F(|a|^2 a), a = F^* u / N, with cotangent nb:
 //   p^b = F^*(-i G nb), ab = 2|a|^2 p^b + a^2 conj(p^b), ub = F ab / N;
 // accumulates gG[w] += Re(conj(nb) i F(|a|^2 a)).
+// Reverse mode of the plasma term over the line (complex128): field a_t in GA,
+// cotangent q_t of the term's time samples in the shared line.  Writes the field
+// cotangent into acc and adds d/d(rho_nt, sigma_drude, omega0 tau_c) into gpl
+// (thread 0).  The density cotangent obeys lam_t = A_t lam_{t+1} + B_t: each
+// thread composes its chunk's maps, a block suffix scan gives every chunk its
+// end value, and the chunk is walked back once more.  Returns false (nothing
+// written) when the line does not ionise.
+template <int N>
+__device__ bool plasma_vjp1(Ctx1<double>& c, double2* acc, double* gpl) {
+  using C = double2;
+  constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  double rho0 = 0.0;
+  if (!density_starts<double, N>(c, rho0)) return false;
+  const PlasmaConst& m = c.in->pc;
+  const double Aeff = c.in->A_eff, alpha = 1.0 / Aeff;
+  const AffineStep aff(m);
+  double cur[CH];
+  double Ac = 1.0, Bc = 0.0;
+  if (tid < NA) {
+    double rho = rho0;
+    for (int i = 0; i < CH; ++i) {
+      const C a = c.GA[tid * CH + i];
+      const double I = (a.x * a.x + a.y * a.y) / Aeff;
+      cur[i] = rho;
+      rho_step(rho, (double)(float)lut_eval<double>(c.lut, I), 0.0, m);
+    }
+    for (int i = CH - 1; i >= 0; --i) {
+      const int t = tid * CH + i;
+      const C a = c.GA[t], q = c.s[pad1(t)];
+      const double I = (a.x * a.x + a.y * a.y) / Aeff;
+      double A, B;
+      plasma_rev<false>(m, aff, alpha, cur[i], (double)(float)lut_eval<double>(c.lut, I),
+                        lut_slope<double>(c.lut, I), I, a.x, a.y, q.x, q.y, A, B);
+      Bc = A * Bc + B;
+      Ac = A * Ac;
+    }
+  }
+  // inclusive suffix scan over the warp: (A, B) o (A', B') = (A A', A B' + B)
+  double sa = Ac, sb = Bc;
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double an = __shfl_down_sync(0xffffffffu, sa, off);
+    const double bn = __shfl_down_sync(0xffffffffu, sb, off);
+    if (lane + off < 32) { sb = sa * bn + sb; sa = sa * an; }
+  }
+  double* wa = c.starts;              // warp composites, then the value at each warp's end
+  double* wb = c.starts + T1 / 32;
+  if (lane == 0) { wa[warp] = sa; wb[warp] = sb; }
+  __syncthreads();
+  if (tid == 0) {
+    double lam = 0.0;                 // cotangent of the density after the last sample
+    for (int w = T1 / 32 - 1; w >= 0; --w) {
+      const double a2 = wa[w], b2 = wb[w];
+      wb[w] = lam;
+      lam = a2 * lam + b2;
+    }
+  }
+  __syncthreads();
+  double xa = __shfl_down_sync(0xffffffffu, sa, 1);
+  double xb = __shfl_down_sync(0xffffffffu, sb, 1);
+  if (lane == 31) { xa = 1.0; xb = 0.0; }
+  double lam = xa * wb[warp] + xb;    // cotangent of the density at this chunk's end
+  double g[3] = {0.0, 0.0, 0.0};
+  if (tid < NA) {
+    for (int i = CH - 1; i >= 0; --i) {
+      const int t = tid * CH + i;
+      const C a = c.GA[t], q = c.s[pad1(t)];
+      const double I = (a.x * a.x + a.y * a.y) / Aeff;
+      double A, B, oar, oai;
+      plasma_rev<true>(m, aff, alpha, cur[i], (double)(float)lut_eval<double>(c.lut, I),
+                       lut_slope<double>(c.lut, I), I, a.x, a.y, q.x, q.y, A, B, lam, &oar, &oai, g);
+      acc[t] = C{oar, oai};
+      lam = A * lam + B;
+    }
+  }
+  for (int k = 0; k < 3; ++k) {
+    const double tot = block_sum(g[k], c.red);
+    if (tid == 0 && gpl) gpl[k] += tot;
+  }
+  return true;
+}
+
 template <int N>
 __device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const double2* nb,
-                                      double2* out, double* gG) {
+                                      double2* out, double* gG, double* gpl) {
   using C = double2;
   constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const double invN = 1.0 / N;
+  const bool pl = c.in->plasma;
   for (int w = tid; w < N; w += T1) c.s[pad1(w)] = u[w];
   __syncthreads();
   stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
   for (int t = tid; t < N; t += T1) {
     const C a = cscale(c.s[pad1(t)], invN);
     c.GA[t] = a;
-    c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
+    if (!pl) c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
   }
   __syncthreads();
+  bool pl_any = false;
+  if (pl) {   // plasma term: q = F*(nb) (time domain), field cotangent into A4P
+    for (int w = tid; w < N; w += T1) c.s[pad1(w)] = nb[w];
+    __syncthreads();
+    stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    pl_any = plasma_vjp1<N>(c, c.A4P, gpl);
+    __syncthreads();
+    for (int t = tid; t < N; t += T1) {
+      const C a = c.GA[t];
+      c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
+    }
+    __syncthreads();
+  }
   stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
   for (int w = tid; w < N; w += T1) {
     const C ph = c.s[pad1(w)];
@@ -581,7 +693,9 @@ __device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const d
     const C pb = c.s[pad1(t)];
     const double I2 = 2.0 * (a.x * a.x + a.y * a.y);
     const C a2 = cmul(a, a);
-    c.s[pad1(t)] = cadd(cscale(pb, I2), cmul(a2, cconj(pb)));
+    C ab = cadd(cscale(pb, I2), cmul(a2, cconj(pb)));
+    if (pl_any) ab = cadd(ab, c.A4P[t]);
+    c.s[pad1(t)] = ab;
   }
   __syncthreads();
   stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
@@ -600,6 +714,7 @@ struct Adj1D {
   double2* gD;          // out: dL/dD
   double* gG;           // out: dL/dG
   double2* rhs;         // out: D A_L + N(A_L) (for d/dL)
+  double* gPl;          // out: d/d(rho_nt, sigma_drude, omega0 tau_c) (plasma instances)
   double2* work;        // 18 N + (ceil(nsteps/K) + K) N complex
 };
 
@@ -642,6 +757,7 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
   __syncthreads();
   stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
   for (int x = tid; x < N; x += T1) { c.A[x] = c.s[pad1(x)]; a.gD[x] = C{0, 0}; a.gG[x] = 0.0; }
+  if (tid < 3 && a.gPl) a.gPl[tid] = 0.0;
   __syncthreads();
   copy(CK, c.A);
   nl_eval<double, N>(c, IN_A, 0.0, c.K1, nullptr);
@@ -688,7 +804,7 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
         TMP[x] = cscale(ab, h / 6);                  // a4 bar
       }
       __syncthreads();
-      vjp_eval<N>(c, U4, TMP, AB, a.gG);             // u4 bar -> AB
+      vjp_eval<N>(c, U4, TMP, AB, a.gG, a.gPl);             // u4 bar -> AB
       for (int x = tid; x < N; x += T1) {            // u4 = E z, z = v + h a3
         const C E = EFac<double>::get(c.D[x], 0.5 * h);
         const C u4b = AB[x];
@@ -698,13 +814,13 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
         A3B[x] = cadd(A3B[x], cscale(zb, h));
       }
       __syncthreads();
-      vjp_eval<N>(c, U3, A3B, TMP, a.gG);            // u3 bar
+      vjp_eval<N>(c, U3, A3B, TMP, a.gG, a.gPl);            // u3 bar
       for (int x = tid; x < N; x += T1) {            // u3 = v + h/2 a2
         VB[x] = cadd(VB[x], TMP[x]);
         A2B[x] = cadd(A2B[x], cscale(TMP[x], h / 2));
       }
       __syncthreads();
-      vjp_eval<N>(c, U2, A2B, TMP, a.gG);            // u2 bar
+      vjp_eval<N>(c, U2, A2B, TMP, a.gG, a.gPl);            // u2 bar
       for (int x = tid; x < N; x += T1) {            // u2 = v + h/2 a1, a1 = E k1
         const C E = EFac<double>::get(c.D[x], 0.5 * h);
         VB[x] = cadd(VB[x], TMP[x]);
@@ -714,7 +830,7 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
         TMP[x] = cmul(cconj(E), a1b);                // k1 bar
       }
       __syncthreads();
-      vjp_eval<N>(c, c.A, TMP, AB, a.gG);            // through k1 = N(A)
+      vjp_eval<N>(c, c.A, TMP, AB, a.gG, a.gPl);            // through k1 = N(A)
       for (int x = tid; x < N; x += T1) {            // v = E A
         const C E = EFac<double>::get(c.D[x], 0.5 * h);
         const C vb = VB[x];

@@ -1784,9 +1784,8 @@ extern "C" int uppe3d_diagnostics(uppe3d_plan* p, double dx, double dy, double* 
 // ---------------------------------------------------------------------------
 // Adjoint (reverse mode) of the 3D ERK4(3)-IP propagation for the Kerr +
 // self-steepening response with dispersion, diffraction, filter and absorber.
-// The plasma terms are held fixed (their derivative is not propagated; exact
-// while the ionisation rate is zero over the field).  Convention:
-// dL = Re sum conj(xb) dx.
+// The plasma terms (without avalanche) are differentiated along each t-line in
+// k_tvjp.  Convention: dL = Re sum conj(xb) dx.
 // ---------------------------------------------------------------------------
 namespace uppe {
 
@@ -1857,9 +1856,116 @@ __global__ void __launch_bounds__(256) k_adj_point(AdjPointArgs a) {
   (void)acur; (void)beta; (void)u4;
 }
 
+template <int NT, typename Rl> struct VLaunch {   // k_tvjp: three lines + 32 doubles per warp
+  using C = typename CT<Rl>::T;
+  static constexpr size_t per_warp = 3 * (size_t)TCfg<NT>::PAD * sizeof(C) + 32 * sizeof(double);
+  static constexpr int WPB = (NT * sizeof(C) + 4 * per_warp <= 200 * 1024) ? 4
+                           : (NT * sizeof(C) + 2 * per_warp <= 200 * 1024) ? 2 : 1;
+  static size_t smem() { return NT * sizeof(C) + WPB * per_warp; }
+};
+
+// Reverse mode of the plasma term on one t-line held by a warp: the scaled field
+// is sU * inv (time domain), the cotangent of the term's samples is in sQ; sQ is
+// overwritten with the field cotangent.  Density chunk starts as in the forward
+// t-pass (warp scan of affine maps, lane 0's serial update when a clamp binds);
+// the density cotangent lam_t = A_t lam_{t+1} + B_t by a warp suffix scan.
+template <typename Rl, int NT>
+__device__ void tline_plasma_vjp(const TArgs& a, typename CT<Rl>::T* sU, typename CT<Rl>::T* sQ,
+                                 double* starts, int lane, Rl inv) {
+  using C = typename CT<Rl>::T;
+  constexpr int E = NT / 32;
+  const Medium3D& m = a.md;
+  const AffineStep aff(m);
+  const Rl AsR = (Rl)a.st->A_scale;
+  const double alpha = a.st->A_scale * a.st->A_scale;
+  const int t0 = lane * E;
+  auto inten = [&](int t, C& av) {
+    av = cscale(sU[tpad(t)], inv);
+    const C Ap = cscale(av, AsR);
+    return (Rl)(Ap.x * Ap.x + Ap.y * Ap.y);
+  };
+  bool ok = true;
+  double cm = 1.0, dm = 0.0;
+  for (int i = 0; i < E; ++i) {
+    C av;
+    const double w = (double)(float)lut_eval<Rl>(a.tb.lut, inten(t0 + i, av));
+    const double cc = aff.e - w * aff.sf;
+    ok &= (cc >= 0.0);
+    dm = cc * dm + w * m.rho_nt * aff.sf;
+    cm = cc * cm;
+  }
+  double rho0;
+  if (__all_sync(0xffffffffu, ok)) {
+    double cc = cm, dd = dm;
+#pragma unroll
+    for (int off = 1; off < 32; off <<= 1) {
+      const double cp = __shfl_up_sync(0xffffffffu, cc, off);
+      const double dp = __shfl_up_sync(0xffffffffu, dd, off);
+      if (lane >= off) { dd = cc * dp + dd; cc = cc * cp; }
+    }
+    const double excl = __shfl_up_sync(0xffffffffu, dd, 1);
+    rho0 = lane == 0 ? 0.0 : excl;
+  } else {
+    if (lane == 0) {
+      double rho = 0.0;
+      for (int t = 0; t < NT; ++t) {
+        if (t % E == 0) starts[t / E] = rho;
+        C av;
+        rho_step(rho, (double)(float)lut_eval<Rl>(a.tb.lut, inten(t, av)), 0.0, m);
+      }
+    }
+    __syncwarp();
+    rho0 = starts[lane];
+    __syncwarp();
+  }
+  double cur[E];
+  {
+    double rho = rho0;
+    for (int i = 0; i < E; ++i) {
+      C av;
+      cur[i] = rho;
+      rho_step(rho, (double)(float)lut_eval<Rl>(a.tb.lut, inten(t0 + i, av)), 0.0, m);
+    }
+  }
+  double Ac = 1.0, Bc = 0.0;
+  for (int i = E - 1; i >= 0; --i) {
+    C av;
+    const Rl I = inten(t0 + i, av);
+    const C q = sQ[tpad(t0 + i)];
+    double A, B;
+    plasma_rev<false>(m, aff, alpha, cur[i], (double)(float)lut_eval<Rl>(a.tb.lut, I),
+                      lut_slope<Rl>(a.tb.lut, I), (double)I, (double)av.x, (double)av.y, (double)q.x,
+                      (double)q.y, A, B);
+    Bc = A * Bc + B;
+    Ac = A * Ac;
+  }
+  double sa = Ac, sb = Bc;   // inclusive suffix scan: (A, B) o (A', B') = (A A', A B' + B)
+#pragma unroll
+  for (int off = 1; off < 32; off <<= 1) {
+    const double an = __shfl_down_sync(0xffffffffu, sa, off);
+    const double bn = __shfl_down_sync(0xffffffffu, sb, off);
+    if (lane + off < 32) { sb = sa * bn + sb; sa = sa * an; }
+  }
+  double lam = __shfl_down_sync(0xffffffffu, sb, 1);
+  if (lane == 31) lam = 0.0;
+  for (int i = E - 1; i >= 0; --i) {
+    C av;
+    const Rl I = inten(t0 + i, av);
+    const C q = sQ[tpad(t0 + i)];
+    double A, B, oar, oai;
+    plasma_rev<true>(m, aff, alpha, cur[i], (double)(float)lut_eval<Rl>(a.tb.lut, I),
+                     lut_slope<Rl>(a.tb.lut, I), (double)I, (double)av.x, (double)av.y, (double)q.x,
+                     (double)q.y, A, B, lam, &oar, &oai, nullptr);
+    sQ[tpad(t0 + i)] = C{(Rl)oar, (Rl)oai};
+    lam = A * lam + B;
+  }
+  __syncwarp();
+}
+
 // VJP of the t-line part: in U' = F*_xy u and X' = F*_xy nb (both (x, y, omega)),
 // out = F_t(ab) / Ntot with a = F*_t U' / Ntot, kb = F*_t(mask shock X'),
 // ab = 2|a|^2 conj(c) kb + c a^2 conj(kb), c = i gk A_scale^2.
+// plus the plasma term's VJP on lines where it is non-zero.
 template <typename Rl, int NT, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_tvjp(TArgs a, const void* xin) {
   using C = typename CT<Rl>::T;
@@ -1868,8 +1974,11 @@ __global__ void __launch_bounds__(WPB * 32) k_tvjp(TArgs a, const void* xin) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* sU = tw + NT + warp * 2 * PAD;
+  unsigned char* wbase = smem_raw + NT * sizeof(C) + warp * VLaunch<NT, Rl>::per_warp;
+  C* sU = reinterpret_cast<C*>(wbase);
   C* sX = sU + PAD;
+  C* sQ = sX + PAD;
+  double* starts = reinterpret_cast<double*>(sQ + PAD);
   for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(a.tb.twt)[i];
   __syncthreads();
   const long long line = (long long)blockIdx.x * WPB + warp;
@@ -1889,6 +1998,25 @@ __global__ void __launch_bounds__(WPB * 32) k_tvjp(TArgs a, const void* xin) {
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sU, tw, lane, LineIdx(), WarpSync());
   stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sX, tw, lane, LineIdx(), WarpSync());
+  bool pl = false;
+  if (a.md.plasma) {   // the plasma term is non-zero only on lines where some W > 0
+    const Rl AsR = (Rl)a.st->A_scale;
+    bool any = false;
+    for (int i = 0; i < E; ++i) {
+      const C Ap = cscale(cscale(sU[tpad(lane * E + i)], inv), AsR);
+      any |= (float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y) != 0.f;
+    }
+    pl = __any_sync(0xffffffffu, any);
+  }
+  if (pl) {
+    for (int i = 0; i < E; ++i) {
+      const int wi = lane + 32 * i;
+      sQ[tpad(wi)] = a.tb.valid[wi] ? xn[wi] : C{0, 0};
+    }
+    __syncwarp();
+    stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sQ, tw, lane, LineIdx(), WarpSync());
+    tline_plasma_vjp<Rl, NT>(a, sU, sQ, starts, lane, inv);
+  }
   for (int i = 0; i < E; ++i) {
     const int t = lane + 32 * i;
     const C av = cscale(sU[tpad(t)], inv);
@@ -1899,7 +2027,9 @@ __global__ void __launch_bounds__(WPB * 32) k_tvjp(TArgs a, const void* xin) {
     const C a2 = cmul(av, av);
     const C t2p = cmul(a2, cconj(kb));
     const C t2 = cscale(C{-t2p.y, t2p.x}, gp);
-    sU[tpad(t)] = cadd(t1, t2);
+    C r = cadd(t1, t2);
+    if (pl) r = cadd(r, sQ[tpad(t)]);
+    sU[tpad(t)] = r;
   }
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(sU, tw, lane, LineIdx(), WarpSync());
@@ -1958,8 +2088,11 @@ static int adj_tlaunch_n(uppe3d_plan* p, const void* in, const void* xin, void* 
   const size_t smem = TLaunch<NT, Rl>::smem();
   cudaError_t e;
   if (KIND == 0) {
-    e = cudaFuncSetAttribute(k_tvjp<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e == cudaSuccess) k_tvjp<Rl, NT, WPB><<<nb, WPB * 32, smem, s>>>(a, xin);
+    constexpr int VW = VLaunch<NT, Rl>::WPB;
+    const size_t vsm = VLaunch<NT, Rl>::smem();
+    const unsigned vnb = (unsigned)((nl + VW - 1) / VW);
+    e = cudaFuncSetAttribute(k_tvjp<Rl, NT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm);
+    if (e == cudaSuccess) k_tvjp<Rl, NT, VW><<<vnb, VW * 32, vsm, s>>>(a, xin);
   } else {
     e = cudaFuncSetAttribute(k_tline<Rl, NT, WPB, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) k_tline<Rl, NT, WPB, +1><<<nb, WPB * 32, smem, s>>>(a, scale);
@@ -2105,6 +2238,11 @@ extern "C" int uppe3d_set_step_log(uppe3d_plan* p, double* hlog, long long cap, 
 extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nsteps, int K, const void* A0,
                               const void* Zbar, void* A0bar, void* work, cudaStream_t s) {
   if (!p || !hlog_host || nsteps < 0 || K <= 0 || !A0 || !Zbar || !A0bar || !work) return UPPE_ERR_ARG;
+  if (p->md.g4 != 0.0 || (p->md.plasma && p->md.ava != 0.0)) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err),
+             "uppe3d_adjoint: the n4 term and avalanche ionisation have no adjoint here");
+    return UPPE_ERR_ARG;
+  }
   return p->dbl ? adjoint_impl<double>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s)
                 : adjoint_impl<float>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s);
 }

@@ -6,27 +6,37 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 
-def _setup(N=16, Nt=64, precision='double', energy=2.0e-4):
+def _setup(N=16, Nt=64, precision='double', energy=2.0e-4, plasma=False, W0=1e9):
+    """Argon at 1.5 bar; with ``plasma`` an MPI-like test table W = W0 (I / 4e15 W/m^2)^8
+    (shared by the device medium and the oracle medium) makes the plasma terms
+    matter at these energies."""
     from oracle import uppe3d
     from project_b200.adjoint import FilamentZernike
     from project_b200.media import Argon
     from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
     x = np.linspace(-2e-3, 2e-3, N)
     t = np.linspace(-150e-15, 150e-15, Nt)
-    med = Argon(800e-9, 1.5, precision, True)
-    med.plasma = False
+    om = uppe3d.argon(800e-9, 1.5, 'double', True)
+    lut = None
+    if plasma:
+        W = np.minimum(W0 * (10.0 ** om.log10_I_cpu / 4e15) ** 8, 1e20)
+        om.W_gpu = W
+        lut = (om.log10_I_cpu, W)
+    med = Argon(800e-9, 1.5, precision, True, lut=lut)
+    if not plasma:
+        med.plasma = False
     sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision=precision)
     obj = FilamentZernike(sol, w0=0.8e-3, energy=energy, fwhm=50e-15, aperture_radius=2e-3)
-    om = uppe3d.argon(800e-9, 1.5, 'double', True)
     osol = uppe3d.Solver3D(x, x, t, om, 'double')
     return sol, obj, osol
 
 
-def test_adjoint3d_matches_torch_autograd_reference():
+@pytest.mark.parametrize('plasma', [False, True])
+def test_adjoint3d_matches_torch_autograd_reference(plasma):
     import torch
     import torch_ref3d
     from project_b200.adjoint import Propagate3D, propagate_3d
-    sol, obj, osol = _setup()
+    sol, obj, osol = _setup(plasma=plasma)
     rng = np.random.Generator(np.random.PCG64(4))
     c = torch.tensor(rng.normal(0, 0.1, 15), dtype=torch.float64, device='cuda', requires_grad=True)
     gdd = torch.tensor(200e-30, dtype=torch.float64, device='cuda', requires_grad=True)
@@ -39,18 +49,23 @@ def test_adjoint3d_matches_torch_autograd_reference():
     assert len(hs) > 2
     c2 = c.detach().clone().requires_grad_(True)
     g2 = gdd.detach().clone().requires_grad_(True)
-    A2 = torch_ref3d.propagate(obj.input_field(c2, g2), hs, torch_ref3d.make(osol))
+    A2 = torch_ref3d.propagate(obj.input_field(c2, g2), hs, torch_ref3d.make(osol, plasma))
     assert float((A2.detach() - A.detach()).abs().max() / A.detach().abs().max()) < 1e-10
     loss2 = (w * (A2.real ** 2 + A2.imag ** 2) ** 2).sum()
     gc2, gg2 = torch.autograd.grad(loss2, [c2, g2])
     assert float((gc - gc2).norm() / gc2.norm()) < 1e-8
     assert abs(float(gg - gg2)) <= 1e-8 * abs(float(gg2))
+    if plasma:   # the plasma terms matter for these gradients
+        c3 = c.detach().clone().requires_grad_(True)
+        A3 = torch_ref3d.propagate(obj.input_field(c3, gdd.detach()), hs, torch_ref3d.make(osol, False))
+        gc3, = torch.autograd.grad((w * (A3.real ** 2 + A3.imag ** 2) ** 2).sum(), [c3])
+        assert float((gc3 - gc2).norm() / gc2.norm()) > 1e-2
 
 
-def _filament_grad(precision, N=32, Nt=64, L=0.1):
+def _filament_grad(precision, N=32, Nt=64, L=0.1, plasma=False):
     import torch
     from project_b200.adjoint import Propagate3D
-    sol, obj, _ = _setup(N=N, Nt=Nt, precision=precision, energy=4e-4)
+    sol, obj, _ = _setup(N=N, Nt=Nt, precision=precision, energy=4e-4, plasma=plasma)
     rng = np.random.Generator(np.random.PCG64(4))
     c0 = rng.normal(0, 0.1, 15)
     c = torch.tensor(c0, dtype=torch.float64, device='cuda', requires_grad=True)
@@ -60,9 +75,10 @@ def _filament_grad(precision, N=32, Nt=64, L=0.1):
     return sol, obj, c0, gc.cpu().numpy(), float(gg), np.array(Propagate3D.last_steps)
 
 
-def test_filament_gradients_vs_central_differences():
+@pytest.mark.parametrize('plasma', [False, True])
+def test_filament_gradients_vs_central_differences(plasma):
     import torch
-    sol, obj, c0, gc, gg, hs = _filament_grad('double')
+    sol, obj, c0, gc, gg, hs = _filament_grad('double', plasma=plasma)
 
     def f(cv, gv):
         A0 = obj.input_field(torch.tensor(cv, dtype=torch.float64, device='cuda'),
@@ -83,11 +99,12 @@ def test_filament_gradients_vs_central_differences():
     assert abs(fdg - gg) <= 1e-4 * abs(fdg)
 
 
-def test_filament_gradients_mixed_vs_fp64():
+@pytest.mark.parametrize('plasma', [False, True])
+def test_filament_gradients_mixed_vs_fp64(plasma):
     """Mixed precision (complex64 bulk): the adjoint of the complex64 forward map
     against the FP64 gradient (each with its own free-running schedule)."""
-    _, _, _, gd, ggd, _ = _filament_grad('double')
-    _, _, _, gs, ggs, _ = _filament_grad('single')
+    _, _, _, gd, ggd, _ = _filament_grad('double', plasma=plasma)
+    _, _, _, gs, ggs, _ = _filament_grad('single', plasma=plasma)
     rc = np.linalg.norm(gs - gd) / np.linalg.norm(gd)
     rg = abs(ggs - ggd) / abs(ggd)
     print('mixed vs fp64 gradient: coeffs %.3e  gdd %.3e' % (rc, rg))

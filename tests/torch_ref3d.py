@@ -1,24 +1,38 @@
 """complex128 torch restatement of the 3+1D ERK4(3)-IP step in the (kx, ky, omega)
-domain (solver_3d.py:100-160, Kerr + self-steepening, no plasma), frozen step
-sequence; autograd reference for the device adjoint.  Test infrastructure."""
+domain (solver_3d.py:100-160: Kerr + self-steepening, and the plasma term of
+media_physics.py:156-203 when the medium has one), frozen step sequence;
+autograd reference for the device adjoint.  Test infrastructure."""
+import numpy as np
 import torch
 
+import torch_plasma
 
-def make(osol):
+
+def make(osol, plasma=False):
     dev = 'cuda'
     D = torch.from_numpy(osol.D_operator).to(dev)
     mask = torch.from_numpy(osol.valid_freq_mask.astype('float64')).to(dev)
     shock = torch.from_numpy(osol.shock_operator.real.astype('float64')).to(dev)
     filt = torch.from_numpy(osol.anti_alias_filter.real.astype('float64')).to(dev)
     damp = torch.from_numpy(osol.damp_space.astype('float64')).to(dev)
-    gk = (osol.medium.omega0 / osol.medium.c) * osol.medium.n2
-    return dict(D=D, mask=mask, shock=shock, filt=filt, damp=damp, gk=gk)
+    md = osol.medium
+    gk = (md.omega0 / md.c) * md.n2
+    pl = None
+    if plasma:
+        pl = dict(lx=torch.from_numpy(md.log10_I_gpu.astype(np.float64)).to(dev),
+                  lw=torch.from_numpy(md.W_gpu.astype(np.float64)).to(dev), Ui=md.Ui,
+                  rr=1.0 / md.tau_rec, dt=osol.dt, rho_nt=torch.tensor(md.rho_nt, dtype=torch.float64),
+                  sigma=md.sigma_drude, w0tc=md.omega0 * md.tau_c)
+    return dict(D=D, mask=mask, shock=shock, filt=filt, damp=damp, gk=gk, pl=pl)
 
 
 def nonlinear(u, p, A_s):
     a = torch.fft.ifftn(u, dim=(0, 1, 2))
-    K = 1j * p['gk'] * A_s ** 2 * (a.real ** 2 + a.imag ** 2) * a
-    return torch.fft.fft2(p['mask'] * p['shock'] * torch.fft.fft(K, dim=-1), dim=(0, 1))
+    I = A_s ** 2 * (a.real ** 2 + a.imag ** 2)
+    Nw = p['shock'] * torch.fft.fft(1j * p['gk'] * I * a, dim=-1)
+    if p['pl'] is not None:
+        Nw = Nw + torch.fft.fft(torch_plasma.term(a, I, p['pl'])[0], dim=-1)
+    return torch.fft.fft2(p['mask'] * Nw, dim=(0, 1))
 
 
 def step(Z, h, p, A_s):
