@@ -189,6 +189,32 @@ int uppe1d_propagate_logged(uppe1d_plan* plan, void* field, double* hlog, int hl
  * differentiates (used for finite-difference checks).  No reference counterpart. */
 int uppe1d_propagate_schedule(uppe1d_plan* plan, void* field, const double* hsched, int nsched,
                               uppe1d_result* results, uppe_stream_t stream);
+/* One operation of a propagation program.  inst >= 0: propagate through plan
+ * instance inst (its D/G/H tables, medium, L, tol, max_step, min_step, max_attempts),
+ * starting like a fresh propagate() call.  inst < 0: mirror, A_w *= amp exp(i (gdd w^2/2
+ * + tod w^3/6)) with w = 2 pi fftfreq(Nt, dt) (test_gaussian_pulse GDD TOD 1mj copy.py:
+ * 282-290; amp = sqrt(1 - loss)).  record != 0 stores the time-domain field after it. */
+typedef struct {
+  int inst;
+  int record;
+  double amp;
+  double gdd;
+  double tod;
+} uppe1d_op;
+
+/* Run nprog propagation programs (multipass cells, sliced capillaries with per-slice
+ * gamma: gas.py:104-147, test_gaussian_pulse GDD TOD 1mj copy.py:196-290) in one
+ * persistent launch, one CTA per program, the field kept on chip between operations.
+ * Program p is ops[op_begin[p] .. op_begin[p+1]) (host arrays); all its propagation
+ * instances share one Nt and dt, and it has at least one.  fields (device): the
+ * programs' time-domain input fields packed back to back (Nt_p elements each),
+ * overwritten with the outputs.  records (device, may be NULL): the recorded fields,
+ * packed per program in operation order.  op_results (host, may be NULL): one per
+ * operation (z, steps, status, energy after it; hist_count = 1 when recorded).
+ * Replaces the reference's Python slice/pass loops around propagate(). */
+int uppe1d_run_programs(uppe1d_plan* plan, int nprog, const long long* op_begin, const uppe1d_op* ops,
+                        void* fields, void* records, uppe1d_result* op_results, uppe_stream_t stream);
+
 /* Workspace of uppe1d_adjoint, in complex128 elements. */
 long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K);
 /* Reverse-mode derivative of one instance's frozen-schedule propagation (complex128

@@ -55,6 +55,10 @@ class Result1D(ctypes.Structure):
 
 STATUS_HIST_FULL = 8
 
+
+class Op1D(ctypes.Structure):
+    _fields_ = [('inst', _I), ('record', _I), ('amp', _D), ('gdd', _D), ('tod', _D)]
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     'uppe_last_error': (ctypes.c_char_p, []),
@@ -83,6 +87,8 @@ SIGNATURES = {
     'uppe1d_propagate': (_I, [_P, _P, _P, _P, ctypes.POINTER(Result1D), _P]),
     'uppe1d_propagate_logged': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe1d_propagate_schedule': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
+    'uppe1d_run_programs': (_I, [_P, _I, ctypes.POINTER(_LL), ctypes.POINTER(Op1D), _P, _P,
+                                 ctypes.POINTER(Result1D), _P]),
     'uppe1d_adjoint_work_elems': (_LL, [_I, _I, _I]),
     'uppe1d_adjoint': (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     'uppe1d_propagate_noalloc': (_I, [ctypes.POINTER(InstDesc1D), _I, _P, _P, _P, _I, _P, _P, _P,

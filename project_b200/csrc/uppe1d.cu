@@ -23,12 +23,19 @@ struct uppe1d_plan {
   long long htotal;       // sum hist_cap * Nt
   long long zhtotal;      // sum hist_cap
   int nblocks;
+  int nsm;
   size_t smem;
   Batch1D b;
   Inst1D* d_inst;
   std::vector<Inst1D> h_inst;
   std::vector<void*> allocs;
   Res1D* h_res;
+  // program buffers (grown on demand by uppe1d_run_programs)
+  void* d_prog = nullptr;
+  size_t prog_bytes = 0;
+  void* d_prog_scratch = nullptr;   // stage arrays when programs outnumber the plan's CTAs
+  int prog_blocks = 0;
+  std::vector<unsigned char> h_prog;
 };
 
 #define UPPE1_CK(x)                                                                \
@@ -51,6 +58,8 @@ static int up1(uppe1d_plan* p, void** dst, const void* src, size_t bytes) {
 extern "C" int uppe1d_plan_destroy(uppe1d_plan* p) {
   if (!p) return 0;
   for (void* a : p->allocs) cudaFree(a);
+  if (p->d_prog) cudaFree(p->d_prog);
+  if (p->d_prog_scratch) cudaFree(p->d_prog_scratch);
   if (p->h_res) cudaFreeHost(p->h_res);
   delete p;
   return 0;
@@ -176,6 +185,7 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+  p->nsm = nsm;
   p->nblocks = std::min(p->ninst, nsm);
   p->b.scratch_per_block = 7LL * nmax;
   TRY1(up1(p, &ptr, nullptr, p->csz * (size_t)p->b.scratch_per_block * p->nblocks)); p->b.scratch = ptr;
@@ -256,6 +266,126 @@ extern "C" int uppe1d_propagate_schedule(uppe1d_plan* p, void* field, const doub
   b.hsched = hsched;
   b.nsched = nsched;
   return run1(p, b, results, s);
+}
+
+static int prog_fail(const char* msg) {
+  snprintf(g_uppe_err, sizeof(g_uppe_err), "uppe1d_run_programs: %s", msg);
+  return UPPE_ERR_ARG;
+}
+
+extern "C" int uppe1d_run_programs(uppe1d_plan* p, int nprog, const long long* op_begin,
+                                   const uppe1d_op* ops, void* fields, void* records,
+                                   uppe1d_result* op_results, cudaStream_t s) {
+  g_uppe_err[0] = 0;
+  if (!p || nprog <= 0 || !op_begin || !ops || !fields) return prog_fail("null argument or nprog <= 0");
+  if (op_begin[0] != 0) return prog_fail("op_begin[0] must be 0");
+  const long long nops = op_begin[nprog];
+  if (nops <= 0) return prog_fail("no operations");
+  std::vector<Prog1D> progs(nprog);
+  std::vector<Op1D> hops(nops);
+  long long foff = 0, roff = 0;
+  for (int q = 0; q < nprog; ++q) {
+    Prog1D& g = progs[q];
+    g.op_begin = op_begin[q];
+    g.op_end = op_begin[q + 1];
+    if (g.op_end < g.op_begin || g.op_end > nops) return prog_fail("op_begin must be non-decreasing");
+    g.Nt = 0;
+    int nrec = 0;
+    for (long long o = g.op_begin; o < g.op_end; ++o) {
+      const uppe1d_op& u = ops[o];
+      if (u.inst >= p->ninst) return prog_fail("operation names an instance outside the plan");
+      if (u.inst >= 0) {
+        const Inst1D& in = p->h_inst[u.inst];
+        if (in.hist_cap > 0) return prog_fail("program instances must have hist_cap = 0");
+        if (g.Nt == 0) { g.Nt = in.Nt; g.log2n = in.log2n; g.dt = in.dt; }
+        else if (in.Nt != g.Nt || in.dt != g.dt)
+          return prog_fail("the propagations of one program must share Nt and dt");
+      } else if (!(u.amp >= 0.0) || !isfinite(u.gdd) || !isfinite(u.tod)) {
+        return prog_fail("mirror needs amp >= 0 and finite gdd, tod");
+      }
+      hops[o].inst = u.inst < 0 ? -1 : u.inst;
+      hops[o].record = u.record ? 1 : 0;
+      hops[o].amp = u.amp; hops[o].gdd = u.gdd; hops[o].tod = u.tod;
+      nrec += u.record ? 1 : 0;
+    }
+    if (g.Nt == 0) return prog_fail("a program needs at least one propagation");
+    g.field_off = foff;
+    g.rec_off = roff;
+    foff += g.Nt;
+    roff += (long long)nrec * g.Nt;
+  }
+  if (roff > 0 && !records) return prog_fail("operations record fields but records is NULL");
+  // one device buffer: programs, operations, per-operation results, queue order
+  const size_t bp = sizeof(Prog1D) * nprog, bo = sizeof(Op1D) * nops, br = sizeof(Res1D) * nops,
+               bq = sizeof(int) * nprog;
+  auto al = [](size_t x) { return (x + 255) & ~(size_t)255; };
+  const size_t need = al(bp) + al(bo) + al(br) + al(bq);
+  if (need > p->prog_bytes) {
+    if (p->d_prog) UPPE1_CK(cudaFree(p->d_prog));
+    p->d_prog = nullptr;
+    p->prog_bytes = 0;
+    UPPE1_CK(cudaMalloc(&p->d_prog, need));
+    p->prog_bytes = need;
+  }
+  unsigned char* base = static_cast<unsigned char*>(p->d_prog);
+  Prog1D* d_progs = reinterpret_cast<Prog1D*>(base);
+  Op1D* d_ops = reinterpret_cast<Op1D*>(base + al(bp));
+  Res1D* d_res = reinterpret_cast<Res1D*>(base + al(bp) + al(bo));
+  int* d_order = reinterpret_cast<int*>(base + al(bp) + al(bo) + al(br));
+  // longest programs first (cost ~ Nt log Nt x sum of L / max_step)
+  std::vector<double> cost(nprog, 0.0);
+  for (int q = 0; q < nprog; ++q)
+    for (long long o = progs[q].op_begin; o < progs[q].op_end; ++o)
+      if (hops[o].inst >= 0) {
+        const Inst1D& in = p->h_inst[hops[o].inst];
+        cost[q] += (double)in.Nt * in.log2n * fmax(1.0, in.L / in.max_step);
+      }
+  std::vector<int> order(nprog);
+  std::iota(order.begin(), order.end(), 0);
+  std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+  p->h_prog.resize(need);
+  memcpy(p->h_prog.data(), progs.data(), bp);
+  memcpy(p->h_prog.data() + al(bp), hops.data(), bo);
+  memcpy(p->h_prog.data() + al(bp) + al(bo) + al(br), order.data(), bq);
+  UPPE1_CK(cudaMemcpyAsync(base, p->h_prog.data(), need, cudaMemcpyHostToDevice, s));
+  Batch1D b = p->b;
+  int nb = std::min(p->nblocks, nprog);
+  const int want = std::min(nprog, p->nsm);
+  if (want > nb) {   // more programs than the plan's CTAs: scratch for one CTA per SM
+    if (want > p->prog_blocks) {
+      if (p->d_prog_scratch) UPPE1_CK(cudaFree(p->d_prog_scratch));
+      p->d_prog_scratch = nullptr;
+      p->prog_blocks = 0;
+      UPPE1_CK(cudaMalloc(&p->d_prog_scratch, p->csz * (size_t)p->b.scratch_per_block * want));
+      p->prog_blocks = want;
+    }
+    b.scratch = p->d_prog_scratch;
+    nb = want;
+  }
+  b.field = fields;
+  b.prog = d_progs;
+  b.ops = d_ops;
+  b.op_res = d_res;
+  b.records = records;
+  b.order = d_order;
+  b.ninst = nprog;
+  b.hlog = nullptr;
+  b.hsched = nullptr;
+  UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
+  UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, nb, p->smem, s) : launch_uppe1d<float>(b, nb, p->smem, s));
+  if (op_results) {
+    std::vector<Res1D> hr(nops);
+    UPPE1_CK(cudaMemcpyAsync(hr.data(), d_res, br, cudaMemcpyDeviceToHost, s));
+    UPPE1_CK(cudaStreamSynchronize(s));
+    for (long long o = 0; o < nops; ++o) {
+      const Res1D& r = hr[o];
+      uppe1d_result& x = op_results[o];
+      x.z = r.z; x.h = r.h; x.err = r.err; x.attempts = r.attempts; x.accepted = r.accepted;
+      x.status = r.status; x.hist_count = r.hist_count;
+      x.energy = r.energy; x.photons = r.photons; x.peak_ion = r.peak_ion;
+    }
+  }
+  return 0;
 }
 
 extern "C" long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K) {

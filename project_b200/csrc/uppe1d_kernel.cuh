@@ -51,6 +51,21 @@ struct Res1D {
   double energy, photons, peak_ion;
 };
 
+// One operation of a propagation program: a propagation through plan instance
+// `inst` (its tables, medium, L, tol, step limits), or, with inst < 0, a mirror
+// A_w *= amp exp(i (gdd w^2 / 2 + tod w^3 / 6)); `record` stores the
+// time-domain field after the operation.
+struct Op1D {
+  int inst, record;
+  double amp, gdd, tod;
+};
+struct Prog1D {
+  long long op_begin, op_end;   // operations [op_begin, op_end)
+  long long field_off;          // element offset of the program's field
+  long long rec_off;            // element offset of its recorded fields
+  int Nt, log2n;
+  double dt;
+};
 struct Batch1D {
   const Inst1D* inst;
   Res1D* res;
@@ -71,6 +86,10 @@ struct Batch1D {
   int hlog_cap;
   const double* hsched;          // replay: nsched step sizes per instance, all accepted (or null)
   int nsched;
+  const Prog1D* prog;            // programs (work items are programs when set)
+  const Op1D* ops;
+  Res1D* op_res;                 // one result per operation
+  void* records;                 // recorded fields (or null)
 };
 
 template <int N> struct Cfg1 {
@@ -395,44 +414,22 @@ __device__ __noinline__ double attempt1(Ctx1<Rl>& c, double h, typename CT<Rl>::
   return sqrt(num / N) / normA;
 }
 
+// State of one adaptive run.
+struct Run1 {
+  double z, h, err;
+  long long attempts, accepted;
+  int status, hcount;
+  double ion_peak;
+};
+
+// The adaptive loop (erk43ip_method.py:294-367) from the state (A, K1 = N(A)),
+// evaluated identically by all threads; i indexes the step log (b.hlog).
 template <typename Rl, int N>
-__device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
+__device__ __forceinline__ void adaptive_run(Ctx1<Rl>& c, const Batch1D& b, int i, const Inst1D& in,
+                                             typename CT<Rl>::T* hist, double* zh, Run1& r) {
   using C = typename CT<Rl>::T;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
-  const Inst1D& in = b.inst[i];
-  Ctx1<Rl> c;
-  c.s = reinterpret_cast<C*>(smem);
-  c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
-  c.starts = c.red + 64;
-  c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
-  C* sc = reinterpret_cast<C*>(b.scratch) + (long long)blockIdx.x * b.scratch_per_block;
-  c.A = sc; c.K1 = sc + N; c.T = sc + 2 * N; c.O = sc + 3 * N;
-  c.A4 = sc + 4 * N; c.A4P = sc + 5 * N; c.GA = sc + 6 * N;
-  c.D = b.D + in.off;
-  c.G = b.G + in.off;
-  c.H = b.H ? b.H + in.off : nullptr;
-  c.in = &in;
-  c.lut = b.lut;
-  C* field = reinterpret_cast<C*>(b.field) + in.off;
-  C* hist = in.hist_cap > 0 ? reinterpret_cast<C*>(b.hist) + in.hist_off : nullptr;
-  double* zh = in.hist_cap > 0 ? b.zhist + in.zh_off : nullptr;
-
-  // A0 -> history slot 0, state = fft(A0)
-  for (int t = tid; t < N; t += T1) {
-    const C a = field[t];
-    c.s[pad1(t)] = a;
-    if (hist) hist[t] = a;
-  }
-  if (zh && tid == 0) zh[0] = 0.0;
-  __syncthreads();
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
-  __syncthreads();
-  double ion_peak = 0.0, ion_cand = 0.0;
-  nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr, nullptr, false, &ion_peak);   // k1 = N(A)
-
-  // adaptive loop (erk43ip_method.py:294-367), evaluated identically by all threads
+  double ion_peak = r.ion_peak, ion_cand = 0.0;
   const double L = in.L, tol = in.tol, max_step = in.max_step, min_step = in.min_step;
   double z = 0.0, h = max_step / 100, err = 0.0, err_prev = -1.0, zlast = 0.0;
   long long attempts = 0, accepted = 0;
@@ -500,8 +497,19 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
       break;
     }
   }
-  // energy sum |A|^2 dt and photon number (Parseval in omega), FP64, fixed order
-  double en = 0.0, ph = 0.0;
+  r.z = z; r.h = h; r.err = err;
+  r.attempts = attempts; r.accepted = accepted;
+  r.status = status; r.hcount = hcount;
+  r.ion_peak = ion_peak;
+}
+
+// energy sum |A|^2 dt and photon number (Parseval in omega), FP64, fixed order
+template <typename Rl, int N>
+__device__ __forceinline__ void energy_photons(Ctx1<Rl>& c, const Inst1D& in, double& en, double& ph) {
+  using C = typename CT<Rl>::T;
+  const int tid = threadIdx.x;
+  en = 0.0;
+  ph = 0.0;
   {
     const double dw = 6.283185307179586476925286766559 / (N * in.dt);
     for (int w = tid; w < N; w += T1) {
@@ -514,6 +522,54 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
     en = block_sum(en, c.red) * in.dt / N;
     ph = block_sum(ph, c.red) * in.dt / N;
   }
+}
+
+template <typename Rl, int N>
+__device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
+  using C = typename CT<Rl>::T;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const Inst1D& in = b.inst[i];
+  Ctx1<Rl> c;
+  c.s = reinterpret_cast<C*>(smem);
+  c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
+  c.starts = c.red + 64;
+  c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
+  C* sc = reinterpret_cast<C*>(b.scratch) + (long long)blockIdx.x * b.scratch_per_block;
+  c.A = sc; c.K1 = sc + N; c.T = sc + 2 * N; c.O = sc + 3 * N;
+  c.A4 = sc + 4 * N; c.A4P = sc + 5 * N; c.GA = sc + 6 * N;
+  c.D = b.D + in.off;
+  c.G = b.G + in.off;
+  c.H = b.H ? b.H + in.off : nullptr;
+  c.in = &in;
+  c.lut = b.lut;
+  C* field = reinterpret_cast<C*>(b.field) + in.off;
+  C* hist = in.hist_cap > 0 ? reinterpret_cast<C*>(b.hist) + in.hist_off : nullptr;
+  double* zh = in.hist_cap > 0 ? b.zhist + in.zh_off : nullptr;
+
+  // A0 -> history slot 0, state = fft(A0)
+  for (int t = tid; t < N; t += T1) {
+    const C a = field[t];
+    c.s[pad1(t)] = a;
+    if (hist) hist[t] = a;
+  }
+  if (zh && tid == 0) zh[0] = 0.0;
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
+  __syncthreads();
+  double ion_peak = 0.0;
+  nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr, nullptr, false, &ion_peak);   // k1 = N(A)
+
+  Run1 run;
+  run.ion_peak = ion_peak;
+  adaptive_run<Rl, N>(c, b, i, in, hist, zh, run);
+  const double z = run.z, h = run.h, err = run.err;
+  const long long attempts = run.attempts, accepted = run.accepted;
+  const int status = run.status, hcount = run.hcount;
+  ion_peak = run.ion_peak;
+  double en, ph;
+  energy_photons<Rl, N>(c, in, en, ph);
   // final state back to the time domain
   for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
   __syncthreads();
@@ -530,6 +586,91 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   __syncthreads();
 }
 
+
+// One propagation program (a multipass cell: slices with their own tables,
+// mirrors with loss and GDD/TOD) run by this CTA with the state kept on chip
+// between operations (gas.py:104-147; test_gaussian_pulse GDD TOD 1mj copy.py:
+// 196-290).  Each propagation starts like a fresh propagate() call: h0 =
+// max_step/100, no controller memory, z from 0.
+template <typename Rl, int N>
+__device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
+  using C = typename CT<Rl>::T;
+  constexpr int FT = Cfg1<N>::FT;
+  const int tid = threadIdx.x;
+  const Prog1D& pg = b.prog[p];
+  Ctx1<Rl> c;
+  c.s = reinterpret_cast<C*>(smem);
+  c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
+  c.starts = c.red + 64;
+  c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
+  C* sc = reinterpret_cast<C*>(b.scratch) + (long long)blockIdx.x * b.scratch_per_block;
+  c.A = sc; c.K1 = sc + N; c.T = sc + 2 * N; c.O = sc + 3 * N;
+  c.A4 = sc + 4 * N; c.A4P = sc + 5 * N; c.GA = sc + 6 * N;
+  c.lut = b.lut;
+  C* field = reinterpret_cast<C*>(b.field) + pg.field_off;
+  C* rec = b.records ? reinterpret_cast<C*>(b.records) + pg.rec_off : nullptr;
+  const Rl invN = (Rl)(1.0 / N);
+  for (int t = tid; t < N; t += T1) c.s[pad1(t)] = field[t];
+  __syncthreads();
+  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
+  __syncthreads();
+  for (long long o = pg.op_begin; o < pg.op_end; ++o) {
+    const Op1D op = b.ops[o];
+    Res1D r;
+    memset(&r, 0, sizeof(r));
+    if (op.inst >= 0) {
+      const Inst1D& in = b.inst[op.inst];
+      c.D = b.D + in.off;
+      c.G = b.G + in.off;
+      c.H = b.H ? b.H + in.off : nullptr;
+      c.in = &in;
+      double ion = 0.0;
+      nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr, nullptr, false, &ion);   // k1 with these tables
+      Run1 run;
+      run.ion_peak = ion;
+      adaptive_run<Rl, N>(c, b, -1, in, nullptr, nullptr, run);
+      double en, ph;
+      energy_photons<Rl, N>(c, in, en, ph);
+      r.z = run.z; r.h = run.h; r.err = run.err; r.attempts = run.attempts;
+      r.accepted = run.accepted; r.status = run.status; r.energy = en;
+      r.photons = in.omega0 > 0.0 ? ph : NAN; r.peak_ion = run.ion_peak;
+    } else {
+      // mirror: loss and spectral phase on the omega-domain state
+      const double dw = 6.283185307179586476925286766559 / (N * pg.dt);
+      double en = 0.0;
+      for (int w = tid; w < N; w += T1) {
+        const double om = dw * (w < (N + 1) / 2 ? w : w - N);
+        double sn, cs;
+        sincos(0.5 * op.gdd * om * om + (1.0 / 6.0) * op.tod * om * om * om, &sn, &cs);
+        const C a = c.A[w];
+        const double ar = op.amp * ((double)a.x * cs - (double)a.y * sn);
+        const double ai = op.amp * ((double)a.x * sn + (double)a.y * cs);
+        c.A[w] = C{(Rl)ar, (Rl)ai};
+        en += ar * ar + ai * ai;
+      }
+      r.energy = block_sum(en, c.red) * pg.dt / N;
+      r.photons = NAN;
+    }
+    if (op.record && rec) {
+      for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+      __syncthreads();
+      stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+      for (int t = tid; t < N; t += T1) rec[t] = cscale(c.s[pad1(t)], invN);
+      rec += N;
+      r.hist_count = 1;
+      __syncthreads();
+    }
+    if (tid == 0) b.op_res[o] = r;
+    __syncthreads();
+  }
+  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+  __syncthreads();
+  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  for (int t = tid; t < N; t += T1) field[t] = cscale(c.s[pad1(t)], invN);
+  __syncthreads();
+}
+
 template <typename Rl>
 __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -541,6 +682,21 @@ __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
     __syncthreads();
     if (k >= b.ninst) return;
     const int i = b.order[k];
+    if (b.prog) {
+      switch (b.prog[i].log2n) {
+        case 6: run_program<Rl, 64>(b, i, smem); break;
+        case 7: run_program<Rl, 128>(b, i, smem); break;
+        case 8: run_program<Rl, 256>(b, i, smem); break;
+        case 9: run_program<Rl, 512>(b, i, smem); break;
+        case 10: run_program<Rl, 1024>(b, i, smem); break;
+        case 11: run_program<Rl, 2048>(b, i, smem); break;
+        case 12: run_program<Rl, 4096>(b, i, smem); break;
+        case 13: run_program<Rl, 8192>(b, i, smem); break;
+        case 14: if (sizeof(Rl) == 4) run_program<Rl, 16384>(b, i, smem); break;
+        default: break;
+      }
+      continue;
+    }
     switch (b.inst[i].log2n) {
       case 6: run_instance<Rl, 64>(b, i, smem); break;
       case 7: run_instance<Rl, 128>(b, i, smem); break;
@@ -558,13 +714,11 @@ __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
 
 // ---------------------------------------------------------------------------
 // Adjoint (reverse mode) of the ERK4(3)-IP step for Kerr + steepening with
-// dispersion and loss (no Raman, no plasma), complex128.  Convention: for a real
-// loss L and complex x, the cotangent xb satisfies dL = Re sum conj(xb) dx (the
-// same as torch's complex gradients).  Frozen accepted step sizes.
+// dispersion, loss and the plasma term (no Raman, no avalanche), complex128.
+// Convention: for a real loss L and complex x, the cotangent xb satisfies
+// dL = Re sum conj(xb) dx (the same as torch's complex gradients).  Frozen
+// accepted step sizes.
 // ---------------------------------------------------------------------------
-// VJP of N(u) = i G F(|a|^2 a), a = F^* u / N, with cotangent nb:
-//   p^b = F^*(-i G nb), ab = 2|a|^2 p^b + a^2 conj(p^b), ub = F ab / N;
-// accumulates gG[w] += Re(conj(nb) i F(|a|^2 a)).
 // Reverse mode of the plasma term over the line (complex128): field a_t in GA,
 // cotangent q_t of the term's time samples in the shared line.  Writes the field
 // cotangent into acc and adds d/d(rho_nt, sigma_drude, omega0 tau_c) into gpl
@@ -648,6 +802,9 @@ __device__ bool plasma_vjp1(Ctx1<double>& c, double2* acc, double* gpl) {
   return true;
 }
 
+// VJP of N(u) = i G F(|a|^2 a) + F(P(a)), a = F^* u / N, with cotangent nb:
+//   p^b = F^*(-i G nb), ab = 2|a|^2 p^b + a^2 conj(p^b) + VJP_P(F^* nb), ub = F ab / N;
+// accumulates gG[w] += Re(conj(nb) i F(|a|^2 a)).
 template <int N>
 __device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const double2* nb,
                                       double2* out, double* gG, double* gpl) {

@@ -131,3 +131,24 @@ def test_sharded_batch_gather_gloo_world2():
     assert keys == list(range(10))
     for r, part in enumerate(parts):
         assert all(owners[i] == r for i in part)
+
+
+def test_gas_cell_program_slices_follow_the_beam():
+    """gas.py:104-126: slice widths, w(z_mid) and gamma = (2 pi / lambda) n2 / (pi w^2)."""
+    from project_b200.programs import Slice, gas_cell_program
+
+    class Dummy:
+        pass
+    lam, w0, n2 = 800e-9, 150e-6, 1e-23
+    prog = gas_cell_program(Dummy(), L_cell=1.0, n_slices=50, w0=w0, n2=n2, center_wavelength=lam)
+    assert len(prog) == 50 and all(isinstance(s, Slice) for s in prog)
+    zR = np.pi * w0 ** 2 / lam
+    edges = np.linspace(-0.5, 0.5, 51)
+    for i, s in enumerate(prog):
+        zm = 0.5 * (edges[i] + edges[i + 1])
+        w = w0 * np.sqrt(1 + (zm / zR) ** 2)
+        assert abs(s.L - 0.02) < 1e-15 and abs(s.max_step - 0.002) < 1e-15
+        assert abs(s.gamma - (2 * np.pi / lam) * n2 / (np.pi * w ** 2)) <= 1e-12 * s.gamma
+    # symmetric about the focus, largest at the centre
+    g = np.array([s.gamma for s in prog])
+    assert np.allclose(g, g[::-1], rtol=1e-12) and g.argmax() in (24, 25)
