@@ -229,6 +229,77 @@ def run_batched1d(dev):
                         'one persistent launch'}
 
 
+def run_gradients(dev):
+    """Gradient evaluations through the device adjoints (forward with step log +
+    reverse pass, checkpoint every 32 steps), wall time with the device synchronised:
+    (1) 1D capillary compression, Nt 8192 over 2 ps, 2 GW 30 fs + one-photon noise,
+    argon 1 bar with ADK plasma, 1 m, tol 1e-6, gradients w.r.t. 64 spline knots,
+    pressure and length; (2) 3+1D filament, 128 x 128 x 1024 over 4 mm x 500 fs, 1.5 mJ
+    50 fs, w0 1 mm, 15 Zernike coefficients (sigma 0.1 rad, seed 4, aperture 2 mm) +
+    input GDD, argon 1.5 bar with ADK plasma, 1.5 m, tol 1e-4, mixed precision.
+    Peak memory = plan allocations + torch's peak (workspace, checkpoints, tensors)."""
+    import torch
+    from project_b200.adjoint import CapillaryCompression, FilamentZernike, Propagate1D, Propagate3D
+    from project_b200.media import Argon
+    from project_b200.pulses import gaussian_pulse, photon_noise
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    out = {}
+    Nt = 8192
+    t = np.linspace(-1e-12, 1e-12, Nt)
+    fw = 30e-15
+    A0 = gaussian_pulse(t, 2e9 * fw * np.sqrt(np.pi / (4 * np.log(2))), fw) + photon_noise(t, LAM_1D, 0)
+    cc = CapillaryCompression(t, A0, n_knots=64, plasma=True, device=dev)
+    knots = torch.zeros(64, dtype=torch.float64, device=dev, requires_grad=True)
+    P = torch.tensor(1.0, dtype=torch.float64, device=dev, requires_grad=True)
+    L = torch.tensor(1.0, dtype=torch.float64, requires_grad=True)
+    cc.loss(knots, P, L)          # warm-up
+    torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    t0 = time.perf_counter()
+    loss = cc.loss(knots, P, L, tol=1e-6, K=32)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    gk, gP, gL = torch.autograd.grad(loss, [knots, P, L])
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    out['capillary_1d'] = {'forward_s': t1 - t0, 'adjoint_s': t2 - t1, 'steps': len(Propagate1D.last_steps),
+                           'checkpoint_every': 32, 'params': 66, 'dtype': 'c128',
+                           'torch_peak_gb': torch.cuda.max_memory_allocated(dev) / 1e9,
+                           'grad_norm_knots': float(gk.norm()), 'dL_dP': float(gP), 'dL_dL': float(gL)}
+    N, Nt3 = 128, 1024
+    x = np.linspace(-2e-3, 2e-3, N)
+    t3 = np.linspace(-250e-15, 250e-15, Nt3)
+    free0 = torch.cuda.mem_get_info(dev)[0]
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t3, Argon(LAM_1D, 1.5, 'single', True), precision='single',
+                                    device=dev)
+    torch.cuda.synchronize(dev)
+    plan_bytes = free0 - torch.cuda.mem_get_info(dev)[0]
+    obj = FilamentZernike(sol, w0=1e-3, energy=1.5e-3, fwhm=50e-15, aperture_radius=2e-3)
+    rng = np.random.Generator(np.random.PCG64(4))
+    c = torch.tensor(rng.normal(0, 0.1, 15), dtype=torch.float64, device=dev, requires_grad=True)
+    gdd = torch.tensor(0.0, dtype=torch.float64, device=dev, requires_grad=True)
+    torch.cuda.synchronize(dev)
+    torch.cuda.reset_peak_memory_stats(dev)
+    base = torch.cuda.memory_allocated(dev)
+    t0 = time.perf_counter()
+    loss = obj.loss(c, gdd, 1.5, tol=1e-4, K=32)
+    torch.cuda.synchronize(dev)
+    t1 = time.perf_counter()
+    gc, gg = torch.autograd.grad(loss, [c, gdd])
+    torch.cuda.synchronize(dev)
+    t2 = time.perf_counter()
+    r = sol.last_result
+    out['filament_3d'] = {'forward_s': t1 - t0, 'adjoint_s': t2 - t1, 'steps': int(r.accepted),
+                          'attempts': int(r.attempts), 'checkpoint_every': 32, 'params': 16,
+                          'dtype': 'c64 bulk, FP64 phase/error/controller',
+                          'workspace_gb': Propagate3D.workspace_bytes / 1e9,
+                          'peak_memory_gb': (plan_bytes + torch.cuda.max_memory_allocated(dev) - base) / 1e9,
+                          'plan_gb': plan_bytes / 1e9,
+                          'peak_ionization': sol.diagnostics()['peak_ionization'],
+                          'grad_norm_zernike': float(gc.norm()), 'dL_dGDD': float(gg)}
+    return out
+
+
 def cpu_baseline_1d():
     """Oracle port of the reference 1D solver on one config-0 instance (Nt 4096, 2 GW 30 fs,
     argon 1 bar, 1 m, tol 1e-6, with the plasma term) on the host."""
@@ -371,6 +442,13 @@ def run_b200(args, rank, world, local_rank):
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             b1d['cpu_baseline'] = cpu_baseline_1d()
 
+    grads = None
+    if rank == 0 and not args.no_gradients:
+        try:
+            grads = run_gradients(dev)
+        except Exception as e:   # reported, never fatal
+            grads = {'error': str(e)[:300]}
+
     if rank == 0:
         line = {
             'metric': METRIC, 'value': value, 'unit': 'pt-steps/s', 'n_gpus': world,
@@ -401,6 +479,7 @@ def run_b200(args, rank, world, local_rank):
                            'spectrum copied back to pinned host memory'},
             'plain_gpu': plain,
             'batched_1d': b1d,
+            'gradients': grads,
             'gpu_launches': args.steps * lib.uppe3d_launches_per_step(sol._plan),
             'clocks': clk,
         }
@@ -442,6 +521,7 @@ def main():
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--no-plain-gpu', action='store_true')
     ap.add_argument('--no-batched-1d', action='store_true')
+    ap.add_argument('--no-gradients', action='store_true')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
     args = ap.parse_args()

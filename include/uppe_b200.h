@@ -259,6 +259,14 @@ int uppe1d_propagate_noalloc(const uppe1d_inst_desc* inst, int precision, const 
  * drivers compute from the returned field (src/3+1D-ERK4(3)IP UPPE/sim.py:140-249). */
 int uppe3d_diagnostics(uppe3d_plan* plan, double dx, double dy, double* out3, uppe_stream_t stream);
 
+/* Mirror on the current state (x, y, omega): Z *= amp exp(i (gdd w^2/2 + tod w^3/6
+ * - omega_abs r^2 / (c R))) with w = 2 pi fftfreq(Nt, dt), omega_abs = desc.omega_abs and
+ * r2[ix*Ny+iy] = x^2 + y^2 (device; NULL for a flat mirror, R then ignored).  The curved
+ * mirror of src/3+1D-ERK4(3)IP UPPE/sim.py:83-96 and the flat-mirror transmission
+ * :331 (amp = sqrt(T)); uppe3d_get_field then returns the reflected field. */
+int uppe3d_mirror(uppe3d_plan* plan, const double* r2, double R, double amp, double gdd, double tod,
+                  uppe_stream_t stream);
+
 /* Record the accepted step sizes of later uppe3d_propagate runs in hlog (device,
  * cap entries; NULL stops recording).  No reference counterpart (the adjoint's input). */
 int uppe3d_set_step_log(uppe3d_plan* plan, double* hlog, long long cap, uppe_stream_t stream);

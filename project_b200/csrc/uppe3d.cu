@@ -1782,6 +1782,53 @@ extern "C" int uppe3d_diagnostics(uppe3d_plan* p, double dx, double dy, double* 
 }
 
 // ---------------------------------------------------------------------------
+// Mirrors on the current state (x, y, omega): amplitude, spectral phase and the
+// curved-mirror phase -omega_abs r^2 / (c R) (src/3+1D-ERK4(3)IP UPPE/sim.py:83-96).
+// ---------------------------------------------------------------------------
+namespace uppe {
+template <typename Rl>
+__global__ void k_mirror3d(const State3D* st, Bufs3D b, long long n, int Nt, int Ny, double dt,
+                           const double* r2, const double* wabs, double invcR, double amp, double gdd,
+                           double tod) {
+  using C = typename CT<Rl>::T;
+  C* z = reinterpret_cast<C*>(b.z[st->zidx]);
+  const double dw = 6.283185307179586476925286766559 / (Nt * dt);
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const int w = (int)(i % Nt);
+    const double om = dw * (w < (Nt + 1) / 2 ? w : w - Nt);
+    double ph = 0.5 * gdd * om * om + (1.0 / 6.0) * tod * om * om * om;
+    if (r2) ph -= wabs[w] * invcR * r2[i / Nt];
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    const C a = z[i];
+    z[i] = C{(Rl)(amp * ((double)a.x * cs - (double)a.y * sn)), (Rl)(amp * ((double)a.x * sn + (double)a.y * cs))};
+  }
+  (void)Ny;
+}
+}  // namespace uppe
+
+extern "C" int uppe3d_mirror(uppe3d_plan* p, const double* r2, double R, double amp, double gdd, double tod,
+                             cudaStream_t s) {
+  if (!p || !(amp >= 0.0) || !isfinite(gdd) || !isfinite(tod)) return UPPE_ERR_ARG;
+  if (r2 && (!p->wabs || !(R != 0.0) || !isfinite(R))) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err),
+             "uppe3d_mirror: a curved mirror needs desc.omega_abs and a finite non-zero R");
+    return UPPE_ERR_ARG;
+  }
+  const double invcR = r2 ? 1.0 / (299792458.0 * R) : 0.0;
+  const long long n = p->g.npts;
+  if (p->dbl)
+    k_mirror3d<double><<<148 * 8, 256, 0, s>>>(p->st, p->b, n, p->g.Nt, p->g.Ny, p->d.dt, r2, p->wabs, invcR,
+                                                amp, gdd, tod);
+  else
+    k_mirror3d<float><<<148 * 8, 256, 0, s>>>(p->st, p->b, n, p->g.Nt, p->g.Ny, p->d.dt, r2, p->wabs, invcR,
+                                               amp, gdd, tod);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
 // Adjoint (reverse mode) of the 3D ERK4(3)-IP propagation for the Kerr +
 // self-steepening response with dispersion, diffraction, filter and absorber.
 // The plasma terms (without avalanche) are differentiated along each t-line in

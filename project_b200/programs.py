@@ -177,3 +177,67 @@ def multipass_program(air, crystal, n_passes, L_cavity, L_crystal, crystal_offse
         prog += air_seg(zb, zr)
         prog.append(mirror)
     return prog
+
+
+# ---------------------------------------------------------------------------
+# 3+1D: segment sequences through several media with mirrors
+# ---------------------------------------------------------------------------
+class Segment3D:
+    """Propagate L through ``solver`` (an ERK43IP_UPPE_3D_Optimized on the shared grid)."""
+
+    def __init__(self, solver, L, tol=1e-4, max_step=1e-2, min_step=1e-9):
+        self.solver, self.L, self.tol = solver, float(L), float(tol)
+        self.max_step, self.min_step = float(max_step), float(min_step)
+
+
+class Mirror3D:
+    """Reflection: sqrt(1 - loss), spectral phase and, with R, a curved mirror."""
+
+    def __init__(self, R=None, loss=0.0, gdd=0.0, tod=0.0):
+        self.R, self.loss, self.gdd, self.tod = R, float(loss), float(gdd), float(tod)
+
+
+def run_sequence_3d(ops, A0, callback=None):
+    """src/3+1D-ERK4(3)IP UPPE/sim.py:304-351 (run): segments through their media,
+    mirrors applied to the state of the last solver used.  The field stays on the
+    device between segments (each segment renormalises by its own max|A|, as each
+    propagate call of the reference does).  Returns the final time-domain field
+    (device) and the per-segment results; callback(k, op, solver) runs after each op."""
+    A = A0
+    last = None
+    results = []
+    for k, op in enumerate(ops):
+        if isinstance(op, Segment3D):
+            op.solver.propagate(A, op.L, tol=op.tol, max_step=op.max_step, min_step=op.min_step,
+                                return_gpu=True)
+            results.append(op.solver.last_result)
+            last = op.solver
+        else:
+            if last is None:
+                last = next(o.solver for o in ops if isinstance(o, Segment3D))
+                last.set_field(A)
+            last.mirror(op.R, op.loss, op.gdd, op.tod)
+            results.append(None)
+        A = last.field()
+        if callback is not None:
+            callback(k, op, last)
+    return A, results
+
+
+def mpc_cycles_3d(air, fs, cycles, d_air_1, d_fs, d_air_mid, d_air_last, R_concave, T_per_round,
+                  n_plates=4, air_tol=1e-4, fs_tol=1e-5, fs_max_step=20e-6):
+    """The multipass cycle of sim.py:304-331: forward (air, [fs, air] x n_plates with the
+    last air gap d_air_last), curved mirror, the same backward, flat-mirror transmission
+    T_per_round.  Air segments use max_step = min(d, 5 mm) (sim.py:125-127)."""
+    def air_seg(d):
+        return Segment3D(air, d, tol=air_tol, max_step=min(d, 5e-3))
+    fwd = [air_seg(d_air_1)]
+    for i in range(n_plates):
+        fwd.append(Segment3D(fs, d_fs, tol=fs_tol, max_step=fs_max_step))
+        fwd.append(air_seg(d_air_last if i == n_plates - 1 else d_air_mid))
+    bwd = [(air_seg(o.L) if o.solver is air else Segment3D(fs, o.L, tol=fs_tol, max_step=fs_max_step))
+           for o in fwd[::-1]]
+    ops = []
+    for _ in range(cycles):
+        ops += fwd + [Mirror3D(R=R_concave)] + bwd + [Mirror3D(loss=1.0 - T_per_round)]
+    return ops

@@ -134,6 +134,21 @@ class ERK43IP_UPPE_3D_Optimized:
                                               _lib.stream_ptr(stream)), 'uppe3d_get_field')
         return out
 
+    def mirror(self, R=None, loss=0.0, gdd=0.0, tod=0.0, stream=None):
+        """Reflect the current state: amplitude sqrt(1 - loss), spectral phase gdd w^2/2 +
+        tod w^3/6 and, for a curved mirror of radius R, the phase -k(omega) r^2 / R
+        (src/3+1D-ERK4(3)IP UPPE/sim.py:83-96, :331)."""
+        r2 = None
+        if R is not None:
+            if getattr(self, '_r2', None) is None:
+                x = torch.as_tensor(np.asarray(self.x, dtype=np.float64))
+                y = torch.as_tensor(np.asarray(self.y, dtype=np.float64))
+                self._r2 = (x[:, None] ** 2 + y[None, :] ** 2).reshape(-1).contiguous().to(self.device)
+            r2 = ctypes.c_void_p(self._r2.data_ptr())
+        _lib.check(self._lib.uppe3d_mirror(self._plan, r2, float(R) if R is not None else 0.0,
+                                           float(np.sqrt(1.0 - loss)), float(gdd), float(tod),
+                                           _lib.stream_ptr(stream)), 'uppe3d_mirror')
+
     def diagnostics(self, stream=None):
         """{'energy' [J], 'photons', 'peak_ionization'} of the current state (device)."""
         out = (ctypes.c_double * 3)()

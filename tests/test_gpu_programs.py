@@ -110,3 +110,42 @@ def test_program_mixed_precision_vs_fp64():
     fd, _, _ = ProgramRunner([prog], t, 'double').run([A0])
     fs, _, _ = ProgramRunner([prog], t, 'single').run([A0])
     assert rel_l2(fs[0], fd[0]) < 1e-4
+
+
+def test_sequence_3d_with_mirrors_matches_oracle_loop():
+    """sim.py:304-331 pattern on a small grid: air / plate / curved mirror / plate /
+    air / flat-mirror loss, two media (argon at 1 and 3 bar as stand-ins)."""
+    import torch
+    from oracle import uppe3d
+    from oracle.inputs import gaussian_beam_3d
+    from project_b200.media import Argon
+    from project_b200.programs import Mirror3D, Segment3D, run_sequence_3d
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x = np.linspace(-1.5e-3, 1.5e-3, 16)
+    t = np.linspace(-100e-15, 100e-15, 64)
+    A0 = gaussian_beam_3d(x, x, t, 0.5e-3, 1e-4, 40e-15)
+    sa = ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(LAM, 1.0, 'double', True), precision='double')
+    sf = ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(LAM, 3.0, 'double', True), precision='double')
+    oa = uppe3d.Solver3D(x, x, t, uppe3d.argon(LAM, 1.0, 'double', True), 'double')
+    of = uppe3d.Solver3D(x, x, t, uppe3d.argon(LAM, 3.0, 'double', True), 'double')
+    R, loss = 0.5, 0.05
+    ops = [Segment3D(sa, 0.02, max_step=5e-3), Segment3D(sf, 0.01, tol=1e-5, max_step=2e-3),
+           Mirror3D(R=R), Segment3D(sf, 0.01, tol=1e-5, max_step=2e-3), Segment3D(sa, 0.02, max_step=5e-3),
+           Mirror3D(loss=loss)]
+    A_dev, _ = run_sequence_3d(ops, torch.from_numpy(A0).cuda())
+    # the reference loop over the oracle
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    omega = 2 * np.pi * np.fft.fftfreq(len(t), t[1] - t[0])
+    k = (2 * np.pi * 299792458.0 / LAM + omega) / 299792458.0
+    mirror_phase = np.exp(-1j * k[None, None, :] * (X ** 2 + Y ** 2)[:, :, None] / R)
+    A = A0.copy()
+    for op in ops:
+        if isinstance(op, Segment3D):
+            os_ = oa if op.solver is sa else of
+            _, _, A_w, _ = os_.propagate(A, op.L, tol=op.tol, max_step=op.max_step, min_step=op.min_step)
+            A = np.fft.ifft(np.fft.ifftshift(A_w, axes=-1), axis=-1)
+        elif op.R is not None:
+            A = np.fft.ifft(np.fft.fft(A, axis=-1) * mirror_phase, axis=-1)
+        else:
+            A = A * np.sqrt(1 - op.loss)
+    assert rel_l2(A_dev.cpu().numpy(), A) < 1e-10
