@@ -334,7 +334,7 @@ def profile_kernels(sol, lib, n_attempts=3):
         for i in range(n.value):
             if byts[i] == 0:
                 continue
-            name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space'}.get(kind[i], 'scalar')
+            name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space', 4: 'k_ypass_tma'}.get(kind[i], 'scalar')
             a = agg.setdefault(name, [0.0, 0.0, 0])
             a[0] += ms[i]
             a[1] += byts[i]

@@ -30,7 +30,8 @@ enum {
 enum {
   UPPE_STATUS_NONFINITE = 1,     /* error or step size became NaN/inf: stopped   */
   UPPE_STATUS_MIN_STEP = 2,      /* a step was forced at min_step with err > tol */
-  UPPE_STATUS_MAX_ATTEMPTS = 4   /* attempt budget exhausted before z = L         */
+  UPPE_STATUS_MAX_ATTEMPTS = 4,  /* attempt budget exhausted before z = L         */
+  UPPE_STATUS_DEVICE_WAIT = 32   /* a bounded device wait ran out: run stopped     */
 };
 
 /* Attempt budget used when a caller passes max_attempts <= 0: every propagation
@@ -287,7 +288,7 @@ int uppe3d_adjoint(uppe3d_plan* plan, const double* hlog_host, int nsteps, int K
 int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,
  * bracketing each launch with CUDA events on `stream`.  Writes per launch its
- * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar) and algorithmic
+ * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar, 4 TMA-fed y-pass) and algorithmic
  * bytes (0 for launches the device state made exit early). */
 int uppe3d_profile_attempt(uppe3d_plan* plan, int cap, float* ms, int* kind, double* bytes,
                            int* n, uppe_stream_t stream);

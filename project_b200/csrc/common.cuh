@@ -201,13 +201,24 @@ struct Lut {
   int n;
   double x0, inv_dx;
   double zero_x;    // W is exactly 0 for clipped log10(I) <= zero_x (-inf if none)
+  double I_zero;    // W is exactly 0 for I < I_zero (no log10 needed)
 };
+
+// 10^(zero_x - 1e-3): the 1e-3 margin in log10 exceeds the rounding of log10 /
+// log10f at these magnitudes by orders, so I < I_zero implies clipped log10(I)
+// <= zero_x and lut_eval returns exactly 0.
+static inline double lut_zero_intensity(double zero_x) {
+  if (zero_x == -INFINITY) return 0.0;
+  if (zero_x == INFINITY) return INFINITY;
+  return pow(10.0, zero_x - 1e-3);
+}
 
 template <typename Rl>
 __device__ __forceinline__ Rl lut_eval(const Lut& L, Rl I) {
   const Rl* xp = reinterpret_cast<const Rl*>(L.x);
   const Rl* fp = reinterpret_cast<const Rl*>(L.w);
   const int n = L.n;
+  if ((double)I < L.I_zero) return (Rl)0;
   Rl x = (sizeof(Rl) == 8) ? (Rl)log10((double)I + 1e-30) : (Rl)log10f((float)I + 1e-30f);
   const Rl x0 = __ldg(xp), x1 = __ldg(xp + n - 1);
   x = x < x0 ? x0 : (x > x1 ? x1 : x);
@@ -265,6 +276,21 @@ struct AffineStep {
   }
 };
 
+// rho_step for w_av = 0 with the update's constants taken from AffineStep (the
+// same values: G = 0 * depl - rr = -rr exactly, so gdt, exp(gdt) and sf are
+// AffineStep's e and sf): no exp per sample.
+__device__ __forceinline__ double rho_step0(double& rho, double w_pi, const PlasmaConst& m,
+                                            const AffineStep& aff) {
+  double depl = (m.rho_nt - rho) / m.rho_nt;
+  if (depl < 0.0) depl = 0.0;
+  const double gen = w_pi * m.rho_nt * depl;
+  double r = rho * aff.e + gen * aff.sf;
+  if (r > m.rho_nt) r = m.rho_nt;
+  if (r < 0.0) r = 0.0;
+  rho = r;
+  return gen;
+}
+
 // ---------------------------------------------------------------------------
 // Reverse mode of the plasma term P(a) = c a (media_physics.py:165-203),
 //   c = -Ui gen / (2 I + 1e-30) - (sigma/2)(1 + i omega0 tau_c) rho,
@@ -279,6 +305,7 @@ __device__ __forceinline__ double lut_slope(const Lut& L, Rl I) {
   const Rl* xp = reinterpret_cast<const Rl*>(L.x);
   const Rl* fp = reinterpret_cast<const Rl*>(L.w);
   const int n = L.n;
+  if ((double)I < L.I_zero) return 0.0;
   const Rl x = (sizeof(Rl) == 8) ? (Rl)log10((double)I + 1e-30) : (Rl)log10f((float)I + 1e-30f);
   const Rl x0 = __ldg(xp), x1 = __ldg(xp + n - 1);
   if (!(x > x0) || !(x < x1)) return 0.0;

@@ -176,11 +176,13 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
       p->b.lut.zero_x = j0 < 0 ? -INFINITY
                        : (dbl ? d->lut_log10I[j0] : (double)(float)d->lut_log10I[j0]);
       if (j0 == n - 1) p->b.lut.zero_x = INFINITY;
+      p->b.lut.I_zero = lut_zero_intensity(p->b.lut.zero_x);
     }
   } else {
     p->b.lut.x = p->b.lut.w = nullptr;
     p->b.lut.n = 0;
     p->b.lut.zero_x = INFINITY;
+    p->b.lut.I_zero = INFINITY;
   }
   int dev = 0, nsm = 148;
   cudaGetDevice(&dev);

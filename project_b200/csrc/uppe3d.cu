@@ -24,6 +24,7 @@
 // then an error kernel and (in propagate mode) the step-size controller, all
 // on the device; every kernel reads the device state and exits early when the
 // propagation is done, so the whole attempt is one reusable CUDA graph.
+#include <cuda.h>            // CUtensorMap (encoded through the runtime's driver entry point)
 #include <cuda_runtime.h>
 #include <math.h>
 #include <stdio.h>
@@ -287,7 +288,8 @@ k_space(SpaceArgs a) {
       for (int i = 0; i < E; ++i) {
         const int e = tid + i * NTHR;
         const int n = e / kW, w = e % kW;   // n = x index, o = y index
-        const Rl ab = (Rl)exp(-a.tb.damp[(long long)n * Ny + o] * h);
+        const double dp = a.tb.damp[(long long)n * Ny + o];
+        const Rl ab = dp == 0.0 ? (Rl)1 : (Rl)exp(-dp * h);   // exp(-0 h) = 1 exactly
         const Rl f = (Rl)a.tb.filt[w0 + w];
         C v = s[idx(w, n)];
         v = cscale(cscale(cscale(v, nrm), f), ab);
@@ -514,7 +516,8 @@ k_xpass_sq(SpaceArgs a) {
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int x = j + R * i;   // output row = x index, o = y index
-      const Rl ab = (Rl)exp(-a.tb.damp[(long long)x * Ny + o] * h);
+      const double dp = a.tb.damp[(long long)x * Ny + o];
+      const Rl ab = dp == 0.0 ? (Rl)1 : (Rl)exp(-dp * h);   // exp(-0 h) = 1 exactly
       zc[gidx(i)] = cscale(cscale(cscale(v[i], nrm), f), ab);
     }
   }
@@ -733,13 +736,191 @@ k_tpass(TArgs a) {
 }
 
 // ---------------------------------------------------------------------------
+// y passes of the complex64 attempt with a TMA-fed stage tile (Ny <= 256).
+// Persistent CTAs (two per SM) walk the (kx, omega-tile) list; the tile to be
+// transformed (Ny rows x kW omega columns, 128-byte rows) arrives by
+// cp.async.bulk.tensor into one of two shared-memory buffers while the CTA
+// works on the other, and the operand fields of the stage algebra are loaded
+// into registers before the wait, so the HBM stream overlaps the FFTs.  One
+// instantiation per pass (MODE); same arithmetic, element by element, as the
+// y-pass branch of k_space.
+// ---------------------------------------------------------------------------
+struct YMaps {
+  CUtensorMap in;     // (omega, ky, kx) view of the pass input (tmp[1])
+  CUtensorMap acur;   // the same view of A = fft2(Z) (YMID1R transforms no input)
+};
+
+__device__ __forceinline__ unsigned smem_u32(const void* p) {
+  return (unsigned)__cvta_generic_to_shared(p);
+}
+
+// bounded wait on an mbarrier phase: false when the limit ran out
+__device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
+  for (int it = 0; it < (1 << 22); ++it) {
+    unsigned ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok) : "r"(bar), "r"(parity) : "memory");
+    if (ok) return true;
+  }
+  return false;
+}
+
+template <int N, int MODE>
+__global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
+  using C = float2;
+  using Rl = float;
+  constexpr int NTHR = 256;
+  constexpr int E = N * kW / NTHR;
+  constexpr int TILE = N * kW;
+  // the dynamic window starts at offset 0 (no static shared memory here); the
+  // buffers are TILE * 8 = 128 N bytes apart, so each starts 128-byte aligned
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int tid = threadIdx.x;
+  C* buf[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + TILE};
+  C* tw = buf[1] + TILE;
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);
+  State3D* st = a.st;
+  if (st->done) return;
+  if (MODE == YMID1R && st->fresh) return;
+  const int Nt = a.g.Nt, Ny = a.g.Ny;
+  const int ntw = Nt / kW;
+  const int total = a.g.Nx * ntw;
+  auto issue = [&](int tile, int b) {
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const unsigned bar = smem_u32(&mbar[b]);
+    const CUtensorMap* map = MODE == YMID1R ? &maps.acur : &maps.in;
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(bar), "r"((unsigned)(TILE * sizeof(C))) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"(smem_u32(buf[b])), "l"(reinterpret_cast<unsigned long long>(map)), "r"(w0), "r"(0), "r"(o),
+           "r"(bar)
+        : "memory");
+  };
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twy);
+    for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+
+  const C* __restrict__ acur = reinterpret_cast<const C*>(a.b.acur);
+  const C* __restrict__ k1b = reinterpret_cast<const C*>(a.b.k1);
+  C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
+  C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
+  C* __restrict__ out = reinterpret_cast<C*>(a.out);
+  C* __restrict__ su = reinterpret_cast<C*>(a.save_u);
+  const double h = st->h;
+  const double h2 = 0.5 * h;
+  const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
+  TileIdx<C> idx;
+  BlockSync sync;
+  double red = 0.0;
+  int k = 0;
+  for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
+    const int b = k & 1;
+    if (tid == 0 && tile + (int)gridDim.x < total) issue(tile + gridDim.x, b ^ 1);
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const long long base = (long long)o * Ny * Nt + w0;
+    // operands of this thread's elements (e = tid + i*NTHR), in flight during the wait and FFT
+    C opA[E], opB[E];
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int e = tid + i * NTHR;
+      const long long gi = base + (long long)(e / kW) * Nt + (e % kW);
+      if constexpr (MODE == YMID2 || MODE == YMID3) { opA[i] = __ldg(acur + gi); opB[i] = __ldg(tsum + gi); }
+      else if constexpr (MODE == YMID4) opB[i] = __ldg(tsum + gi);
+      else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
+      else opA[i] = __ldg(a4p + gi);   // YFWD5
+    }
+    const bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+    if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
+      if (tid == 0) { atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT); st->done = 1; }
+      return;
+    }
+    C* s = buf[b];
+    if constexpr (MODE != YMID1R) stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    const OmegaCol oc(a.tb, w0 + tid % kW);
+#pragma unroll
+    for (int i = 0; i < E; ++i) {
+      const int e = tid + i * NTHR;
+      const int n = e / kW, w = e % kW;     // n = ky, o = kx; s[e] = s[idx(w, n)]
+      const long long gi = base + (long long)n * Nt + w;
+      if constexpr (MODE == YFWD5) {
+        const C a5 = s[e], a4 = opA[i];
+        const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
+        const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+        red = (d > red || d != d) ? d : red;
+        continue;
+      }
+      if constexpr (MODE == YMID4) {
+        const C a4 = s[e];
+        const C A4 = cadd(opB[i], cscale(a4, h6R));
+        a4p[gi] = a4;
+        const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+        red = (m > red || m != m) ? m : red;
+        s[e] = A4;
+        continue;
+      }
+      const double qv = a.tb.q[(long long)o * Ny + n];
+      const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qv, h2);
+      C u;
+      if constexpr (MODE == YMID1R) {   // s = A tile, opB = k1
+        const C v = cmul(s[e], Ef);
+        const C a1 = cmul(opB[i], Ef);
+        tsum[gi] = a1;
+        u = cadd(v, cscale(a1, h2R));
+      } else if constexpr (MODE == YMID2) {
+        const C a2 = s[e];
+        const C v = cmul(opA[i], Ef);
+        tsum[gi] = cadd(opB[i], cscale(a2, (Rl)2));
+        u = cadd(v, cscale(a2, h2R));
+      } else {   // YMID3
+        const C a3 = s[e];
+        const C v = cmul(opA[i], Ef);
+        const C ts = cadd(opB[i], cscale(a3, (Rl)2));
+        tsum[gi] = cmul(cadd(v, cscale(ts, h6R)), Ef);
+        u = cmul(cadd(v, cscale(a3, hR)), Ef);
+      }
+      s[e] = u;
+      if (su) su[gi] = u;
+    }
+    if constexpr (MODE != YFWD5) {
+      __syncthreads();
+      stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+      store_tile<C, N, NTHR>(s, out, base, Nt, tid);
+    }
+    __syncthreads();   // buffer b is refilled at iteration k + 1
+  }
+  if constexpr (MODE == YMID4 || MODE == YFWD5) {
+    red = warp_max<32>(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+  }
+}
+
+template <int N>
+static size_t ytma_smem() {
+  return sizeof(float2) * (size_t)(2 * N * kW + N) + 2 * sizeof(unsigned long long);
+}
+
+// ---------------------------------------------------------------------------
 // Warp FFT of a t-line of NT = 32*E points held in registers (E = 16 or 32).
 // Natural layout: lane l holds x[l + 32 m], m < E.  Four-step layout: lane L
 // holds X[out_index(L, k)], k < E.  fwd_like: DFT_E in registers, twiddle
 // W_NT^(l k1), transpose through a padded shared buffer S, DFT_E, then (E = 16)
 // a radix-2 combine with the partner lane L^1.  bwd_like is the transposed
 // sequence (four-step -> natural).  With DIR=-1 fwd_like is the forward FFT;
-// with DIR=+1 bwd_like is the unnormalised inverse.
+// with DIR=+1 bwd_like is the unnormalised inverse.  tw is the four-step table
+// tw[k*32 + l] = W_NT^(l k).
 // ---------------------------------------------------------------------------
 template <int E> struct WarpFFT {
   static constexpr int G = 32 / E;                   // lanes per second-stage DFT
@@ -755,7 +936,7 @@ template <int E> struct WarpFFT {
       const bool r0 = (lane & 1) == 0;
 #pragma unroll
       for (int k = 0; k < E; ++k) {
-        C t = tw[k * E];                               // W_32^k = W_NT^(k E)
+        C t = tw[k * 32 + E];                          // W_32^k = W_NT^(k E)
         if (DIR > 0) t.y = -t.y;
         const C own = v[k];
         C oth;
@@ -771,7 +952,7 @@ template <int E> struct WarpFFT {
       const bool r0 = (lane & 1) == 0;
 #pragma unroll
       for (int k = 0; k < E; ++k) {
-        C t = tw[k * E];
+        C t = tw[k * 32 + E];
         if (DIR > 0) t.y = -t.y;
         const C own = v[k];
         C oth;
@@ -786,7 +967,7 @@ template <int E> struct WarpFFT {
     DFT<E, DIR, C>::run(v);
 #pragma unroll
     for (int k = 1; k < E; ++k) {
-      C t = tw[lane * k];
+      C t = tw[k * 32 + lane];
       if (DIR > 0) t.y = -t.y;
       v[k] = cmul(v[k], t);
     }
@@ -813,7 +994,7 @@ template <int E> struct WarpFFT {
     __syncwarp();
 #pragma unroll
     for (int k = 1; k < E; ++k) {
-      C t = tw[lane * k];
+      C t = tw[k * 32 + lane];
       if (DIR > 0) t.y = -t.y;
       v[k] = cmul(v[k], t);
     }
@@ -839,9 +1020,15 @@ k_tpass_w(TArgs a) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   C* S = tw + NT + warp * BUF;
   double* starts = reinterpret_cast<double*>(tw + NT + WPB * BUF) + warp * 32;
+  // rates of the line in time order (one pad per 32: conflict-free both ways)
+  float* sW = reinterpret_cast<float*>(reinterpret_cast<double*>(tw + NT + WPB * BUF) + WPB * 32) +
+              warp * (NT + NT / 32);
+  auto wpad = [](int t) { return t + (t >> 5); };
   {
+    // four-step twiddles tw[k*32 + l] = W_NT^(l k) (l < 32, k < E; l k < NT): the
+    // per-lane factors of a column k are consecutive (conflict-free loads)
     const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
-    for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[i];
+    for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[(i & 31) * (i >> 5)];
   }
   __syncthreads();
   State3D* st = a.st;
@@ -870,7 +1057,9 @@ k_tpass_w(TArgs a) {
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const C Ap = cscale(v[k], A_scaleR);
-      any_w |= (lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y) != (Rl)0);
+      const float w = (float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+      any_w |= (w != 0.f);
+      sW[wpad(lane + 32 * k)] = w;
     }
   }
   const bool plasma_line = m.plasma && (__any_sync(0xffffffffu, any_w) || m.ava != 0.0);
@@ -885,8 +1074,7 @@ k_tpass_w(TArgs a) {
     bool ok = (m.ava == 0.0);
     double cmap = 1.0, dmap = 0.0;
     for (int i = 0; i < E; ++i) {
-      const C Ap = cscale(S[tpad(t0 + i)], A_scaleR);
-      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+      const double w = (double)sW[wpad(t0 + i)];
       const double c = aff.e - w * aff.sf;
       ok &= (c >= 0.0);
       dmap = c * dmap + w * m.rho_nt * aff.sf;
@@ -910,7 +1098,7 @@ k_tpass_w(TArgs a) {
           if (t % E == 0) starts[t / E] = rho;
           const C Ap = cscale(S[tpad(t)], A_scaleR);
           const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
-          const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
+          const double w = (double)sW[wpad(t)];
           const double wa = (double)(float)(m.ava * (double)I);
           rho_step(rho, w, wa, m);
         }
@@ -925,12 +1113,13 @@ k_tpass_w(TArgs a) {
       const C av = S[tpad(t)];
       const C Ap = cscale(av, A_scaleR);
       const Rl I = Ap.x * Ap.x + Ap.y * Ap.y;
-      const double w = (double)(float)lut_eval<Rl>(a.tb.lut, I);
-      const double wa = (double)(float)(m.ava * (double)I);
+      const double w = (double)sW[wpad(t)];
       const double rho_t = rho;
       ion = fmax(ion, rho_t);
-      const double gen = rho_step(rho, w, wa, m);
-      const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
+      const double gen = m.ava == 0.0 ? rho_step0(rho, w, m, aff)
+                                      : rho_step(rho, w, (double)(float)(m.ava * (double)I), m);
+      // -(0 Ui) / x = -0 exactly: skip the division where nothing is generated
+      const double loss = gen != 0.0 ? -(gen * m.Ui) / (2.0 * (double)I + 1e-30) : -0.0;
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
       S[tpad(t)] = C{(Rl)cr * av.x - (Rl)ci * av.y, (Rl)cr * av.y + (Rl)ci * av.x};
@@ -1195,6 +1384,9 @@ struct uppe3d_plan {
   double pass_scale = 1.0;                          // plain y passes
   double* diag_buf = nullptr;     // per-block partial sums + 3 results
   cudaStream_t cap_stream = nullptr;
+  bool ytma = false;              // TMA-fed y passes (complex64, 64 <= Ny <= 256)
+  YMaps ymaps;
+  int nsm = 148;
 };
 
 #define UPPE_CK(x)                                                                 \
@@ -1252,6 +1444,36 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
   k_space<Rl, N><<<(unsigned)nblocks, SpaceCfg<N>::NTHR, smem, s>>>(a);
 }
 
+// the y passes of the attempt that k_ypass_tma serves (its `in` map is tmp[1])
+static bool use_ytma(const uppe3d_plan* p, int mode, const void* in) {
+  return p->ytma && (mode == YMID1R || ((mode == YMID2 || mode == YMID3 || mode == YMID4 || mode == YFWD5) &&
+                                        in == p->b.tmp[1]));
+}
+
+template <int N>
+static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
+  const dim3 g((unsigned)(2 * p->nsm));
+  const size_t sm = ytma_smem<N>();
+  switch (a.mode) {
+    case YMID1R: k_ypass_tma<N, YMID1R><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID2: k_ypass_tma<N, YMID2><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID3: k_ypass_tma<N, YMID3><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID4: k_ypass_tma<N, YMID4><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    default: k_ypass_tma<N, YFWD5><<<g, 256, sm, s>>>(a, p->ymaps); break;
+  }
+}
+
+template <int N>
+static cudaError_t set_ytma_attr() {
+  const int sm = (int)ytma_smem<N>();
+  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YFWD5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
+
 template <typename Rl>
 static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cudaStream_t s) {
   using C = typename CT<Rl>::T;
@@ -1260,6 +1482,15 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   a.save_u = (mode == YMID1 || mode == YMID1R) ? p->save_u[0]
            : mode == YMID2 ? p->save_u[1] : mode == YMID3 ? p->save_u[2] : nullptr;
   a.scale = p->pass_scale;
+  if (sizeof(Rl) == 4 && use_ytma(p, mode, in)) {
+    switch (p->g.Ny) {
+      case 64: launch_ytma_n<64>(p, a, s); break;
+      case 128: launch_ytma_n<128>(p, a, s); break;
+      case 256: launch_ytma_n<256>(p, a, s); break;
+      default: return UPPE_ERR_SIZE;
+    }
+    return 0;
+  }
   const bool xpass = mode <= XFWD_Z;
   const int N = xpass ? p->g.Nx : p->g.Ny;
   const long long nouter = xpass ? p->g.Ny : p->g.Nx;
@@ -1283,7 +1514,8 @@ template <int NT, typename Rl> struct TWarp {
   static constexpr int BUF = WarpFFT<(E < 16 ? 16 : E)>::SBUF > TCfg<NT>::PAD
                                  ? WarpFFT<(E < 16 ? 16 : E)>::SBUF : TCfg<NT>::PAD;
   static size_t smem() {
-    return (size_t)(NT + WPB * BUF) * sizeof(typename CT<Rl>::T) + (size_t)WPB * 32 * sizeof(double);
+    return (size_t)(NT + WPB * BUF) * sizeof(typename CT<Rl>::T) + (size_t)WPB * 32 * sizeof(double) +
+           (size_t)WPB * (NT + NT / 32) * sizeof(float);
   }
 };
 
@@ -1401,7 +1633,7 @@ struct Recorder {
   }
 };
 
-enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3 };
+enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3, KIND_YT = 4 };
 
 // the fixed pass sequence of one attempt (see the file header); the numbers are
 // the fields each launch reads + writes (algorithmic bytes / field bytes)
@@ -1411,11 +1643,12 @@ static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
   cudaStream_t s = r.s;
   void* const* t = p->b.tmp;
   const bool f = r.fresh != 0;
+  const int KY = p->ytma ? KIND_YT : KIND_Y;   // YMID1R..4, YFWD5 (k_ypass_tma)
   // eval 1 (skipped on device unless the state is fresh)
   rc |= r(KIND_T, 2, f, [&] { return launch_t<Rl, 0>(p, T_FROM_Z, nullptr, t[0], s); });
   rc |= r(KIND_X, 4, f, [&] { return launch_space<Rl>(p, XFWD_Z, t[0], t[1], s); });
   rc |= r(KIND_Y, 6, f, [&] { return launch_space<Rl>(p, YMID1, t[1], t[0], s); });
-  rc |= r(KIND_Y, 4, !f, [&] { return launch_space<Rl>(p, YMID1R, nullptr, t[0], s); });
+  rc |= r(KY, 4, !f, [&] { return launch_space<Rl>(p, YMID1R, nullptr, t[0], s); });
   // eval 2..4
   const int mids[3] = {YMID2, YMID3, YMID4};
   const double midb[3] = {5, 5, 4};
@@ -1423,16 +1656,59 @@ static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
     rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XINV, t[0], t[1], s); });
     rc |= r(KIND_T, 2, true, [&] { return launch_t<Rl, 0>(p, T_GENERAL, t[1], t[2], s); });
     rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XFWD, t[2], t[1], s); });
-    rc |= r(KIND_Y, midb[k], true, [&] { return launch_space<Rl>(p, mids[k], t[1], t[0], s); });
+    rc |= r(KY, midb[k], true, [&] { return launch_space<Rl>(p, mids[k], t[1], t[0], s); });
   }
   // eval 5 (+ candidate state) and the error reduction
   rc |= r(KIND_X, 3, true, [&] { return launch_space<Rl>(p, XINV_Z, t[0], t[1], s); });
   rc |= r(KIND_T, 2, true, [&] { return launch_t<Rl, 0>(p, T_GENERAL, t[1], t[2], s); });
   rc |= r(KIND_X, 2, true, [&] { return launch_space<Rl>(p, XFWD, t[2], t[1], s); });
-  rc |= r(KIND_Y, sizeof(Rl) == 8 ? 3 : 2, true,
+  rc |= r(KY, sizeof(Rl) == 8 ? 3 : 2, true,
           [&] { return launch_space<Rl>(p, YFWD5, t[1], nullptr, s); });
   rc |= r(KIND_SMALL, 0, true, [&] { k_err<<<1, 1, 0, s>>>(p->st); return 0; });
   return rc;
+}
+
+// (omega, ky, kx) tensor maps of the y passes' input field and of A for
+// k_ypass_tma: 8-byte elements, box kW x Ny x 1 (128-byte rows; omega
+// coordinates are multiples of kW, so every copy starts 16-byte aligned).
+// Without the driver entry point the y passes stay on k_space.
+typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                  const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int setup_ytma(uppe3d_plan* p) {
+  void* fn = nullptr;
+  cudaDriverEntryPointQueryResult q;
+  if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+      q != cudaDriverEntryPointSuccess || !fn) {
+    cudaGetLastError();
+    return 0;
+  }
+  EncodeTiledFn encode = reinterpret_cast<EncodeTiledFn>(fn);
+  const cuuint64_t dims[3] = {(cuuint64_t)p->g.Nt, (cuuint64_t)p->g.Ny, (cuuint64_t)p->g.Nx};
+  const cuuint64_t strides[2] = {(cuuint64_t)p->g.Nt * 8, (cuuint64_t)p->g.Ny * p->g.Nt * 8};
+  const cuuint32_t box[3] = {(cuuint32_t)kW, (cuuint32_t)p->g.Ny, 1};
+  const cuuint32_t es[3] = {1, 1, 1};
+  void* bufs[2] = {p->b.tmp[1], p->b.acur};
+  CUtensorMap* maps[2] = {&p->ymaps.in, &p->ymaps.acur};
+  for (int i = 0; i < 2; ++i) {
+    if (reinterpret_cast<uintptr_t>(bufs[i]) % 16) return 0;
+    if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, bufs[i], dims, strides, box, es,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+      return 0;
+  }
+  int dev = 0;
+  UPPE_CK(cudaGetDevice(&dev));
+  UPPE_CK(cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev));
+  switch (p->g.Ny) {
+    case 64: UPPE_CK(set_ytma_attr<64>()); break;
+    case 128: UPPE_CK(set_ytma_attr<128>()); break;
+    case 256: UPPE_CK(set_ytma_attr<256>()); break;
+    default: return 0;
+  }
+  p->ytma = true;
+  return 0;
 }
 
 static int build_graphs(uppe3d_plan* p) {
@@ -1539,6 +1815,7 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
       p->tb.lut.zero_x = j0 < 0 ? -INFINITY
                        : (dbl ? d->lut_log10I[j0] : (double)(float)d->lut_log10I[j0]);
       if (j0 == n - 1) p->tb.lut.zero_x = INFINITY;
+      p->tb.lut.I_zero = lut_zero_intensity(p->tb.lut.zero_x);
     }
   }
   p->md.gk = d->gamma_kerr;
@@ -1564,6 +1841,7 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
     p->allocs.push_back(*f);
   }
   UPPE_TRY(p->dbl ? set_attrs<double>(p->g) : set_attrs<float>(p->g));
+  if (!p->dbl && p->g.Ny >= 64 && p->g.Ny <= 256) UPPE_TRY(setup_ytma(p));
   UPPE_TRY(build_graphs(p));
 #undef UPPE_TRY
   *out = p;

@@ -108,19 +108,26 @@ def test_strong_ionisation_clamped_scan():
     assert rel_l2(sol.field().cpu().numpy() / osol.A_scale, A4o) < 1e-11
 
 
-def test_larger_grid_attempts_vs_oracle():
+@pytest.mark.parametrize('N,Nt,precision', [(64, 128, 'double'), (64, 128, 'single'),
+                                             (256, 64, 'single')])
+def test_larger_grid_attempts_vs_oracle(N, Nt, precision):
+    """Complex64 grids with Ny >= 64 run the TMA-fed y passes (k_ypass_tma)."""
     from project_b200.media import Argon
     from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
-    x, t, lam, A0, osol, lut = _oracle_case(N=64, Nt=128)
+    x, t, lam, A0, osol, lut = _oracle_case(N=N, Nt=Nt)
     z, freq, Ao, log = osol.propagate(A0, 0.02, tol=1e-5, max_attempts=6)
-    med = Argon(lam, 1.0, 'double', True, lut=lut)
-    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='double')
+    med = Argon(lam, 1.0, precision, True, lut=lut)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision=precision)
     sol.set_field(A0)
     for z0, h, err_o, acc in log:
         err = sol.attempt(h)
-        assert abs(err - err_o) <= 1e-8 * err_o + 1e-18
+        if precision == 'double':
+            assert abs(err - err_o) <= 1e-8 * err_o + 1e-18
+        else:   # FP32 fields: errors below ~1e-9 are rounding noise (tol is 1e-5)
+            assert abs(err - err_o) <= 1e-3 * err_o + 1e-9
         sol.commit(acc)
-    assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < 1e-10
+    assert sol.result().status == 0
+    assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < (1e-10 if precision == 'double' else 1e-4)
 
 
 @pytest.mark.parametrize('Nt,precision,W0', [(512, 'double', 3e9), (512, 'double', 1e15),
