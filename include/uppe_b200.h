@@ -260,6 +260,19 @@ int uppe1d_propagate_noalloc(const uppe1d_inst_desc* inst, int precision, const 
  * drivers compute from the returned field (src/3+1D-ERK4(3)IP UPPE/sim.py:140-249). */
 int uppe3d_diagnostics(uppe3d_plan* plan, double dx, double dy, double* out3, uppe_stream_t stream);
 
+/* Doubles in the output of uppe3d_beam_diagnostics: 10 Nt + Nx Ny. */
+long long uppe3d_beam_diag_elems(const uppe3d_plan* plan);
+/* Beam diagnostics of the current state in one device pass, the sums behind
+ * src/3+1D-ERK4(3)IP UPPE/sim.py:140-249 (energy, P(t), fluence and beam moments,
+ * full / centre / fibre-coupled spectra, centre and fibre-coupled intensity vs t).
+ * out (device, uppe3d_beam_diag_elems doubles), all of the normalised state Z =
+ * fft_t(A / A_scale) and a = ifft_t(Z): [0, Nt) sum_xy |Z|^2; [Nt, 3Nt) sum_xy m Z
+ * (re, im interleaved); [3Nt, 4Nt) sum_xy |a|^2; [4Nt, 6Nt) sum_xy m a; [6Nt, 8Nt)
+ * Z at (Nx/2, Ny/2); [8Nt, 10Nt) a there; then sum_t |a|^2 per (x, y), index
+ * ix*Ny+iy.  mode: device [Nx*Ny] fibre mode, or NULL (its sums stay 0).  omega
+ * in fft order. */
+int uppe3d_beam_diagnostics(uppe3d_plan* plan, const double* mode, double* out, uppe_stream_t stream);
+
 /* Mirror on the current state (x, y, omega): Z *= amp exp(i (gdd w^2/2 + tod w^3/6
  * - omega_abs r^2 / (c R))) with w = 2 pi fftfreq(Nt, dt), omega_abs = desc.omega_abs and
  * r2[ix*Ny+iy] = x^2 + y^2 (device; NULL for a flat mirror, R then ignored).  The curved

@@ -748,6 +748,7 @@ k_tpass(TArgs a) {
 struct YMaps {
   CUtensorMap in;     // (omega, ky, kx) view of the pass input (tmp[1])
   CUtensorMap acur;   // the same view of A = fft2(Z) (YMID1R transforms no input)
+  CUtensorMap z2;     // the same view of tmp[2] = fft_x(Z) (YMID1's second field)
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -778,13 +779,16 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
   // the dynamic window starts at offset 0 (no static shared memory here); the
   // buffers are TILE * 8 = 128 N bytes apart, so each starts 128-byte aligned
   extern __shared__ __align__(16) unsigned char smem_raw[];
+  constexpr bool TWO = MODE == YMID1;   // YMID1 also transforms fft_x(Z) (single-buffered tile)
   const int tid = threadIdx.x;
   C* buf[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + TILE};
-  C* tw = buf[1] + TILE;
-  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);
+  C* bufA = buf[1] + TILE;
+  C* tw = TWO ? bufA + TILE : buf[1] + TILE;
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);   // [2]: bufA
   State3D* st = a.st;
   if (st->done) return;
   if (MODE == YMID1R && st->fresh) return;
+  if (MODE == YMID1 && !st->fresh) return;
   const int Nt = a.g.Nt, Ny = a.g.Ny;
   const int ntw = Nt / kW;
   const int total = a.g.Nx * ntw;
@@ -801,9 +805,22 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
            "r"(bar)
         : "memory");
   };
+  auto issueA = [&](int tile) {
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const unsigned bar = smem_u32(&mbar[2]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(bar), "r"((unsigned)(TILE * sizeof(C))) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"(smem_u32(bufA)), "l"(reinterpret_cast<unsigned long long>(&maps.z2)), "r"(w0), "r"(0), "r"(o),
+           "r"(bar)
+        : "memory");
+  };
   if (tid == 0) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
     asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    if (TWO) asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[2])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   {
@@ -811,10 +828,13 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
     for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
   }
   __syncthreads();
-  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  if (tid == 0 && (int)blockIdx.x < total) {
+    issue(blockIdx.x, 0);
+    if (TWO) issueA(blockIdx.x);
+  }
 
-  const C* __restrict__ acur = reinterpret_cast<const C*>(a.b.acur);
-  const C* __restrict__ k1b = reinterpret_cast<const C*>(a.b.k1);
+  C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
+  C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
   C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
   C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
   C* __restrict__ out = reinterpret_cast<C*>(a.out);
@@ -840,15 +860,17 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
       if constexpr (MODE == YMID2 || MODE == YMID3) { opA[i] = __ldg(acur + gi); opB[i] = __ldg(tsum + gi); }
       else if constexpr (MODE == YMID4) opB[i] = __ldg(tsum + gi);
       else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
-      else opA[i] = __ldg(a4p + gi);   // YFWD5
+      else if constexpr (MODE == YFWD5) opA[i] = __ldg(a4p + gi);
     }
-    const bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+    bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+    if (TWO) ok = ok && mbar_wait(smem_u32(&mbar[2]), (unsigned)(k & 1));
     if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
       if (tid == 0) { atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT); st->done = 1; }
       return;
     }
     C* s = buf[b];
     if constexpr (MODE != YMID1R) stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    if constexpr (TWO) stockham<N, kW, NTHR, -1, 1, C>(bufA, tw, tid, idx, sync);
     const OmegaCol oc(a.tb, w0 + tid % kW);
 #pragma unroll
     for (int i = 0; i < E; ++i) {
@@ -879,6 +901,14 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
         const C a1 = cmul(opB[i], Ef);
         tsum[gi] = a1;
         u = cadd(v, cscale(a1, h2R));
+      } else if constexpr (MODE == YMID1) {   // s = k1 = N(A), bufA = A
+        const C A = bufA[e], k1 = s[e];
+        acur[gi] = A;
+        k1b[gi] = k1;
+        const C v = cmul(A, Ef);
+        const C a1 = cmul(k1, Ef);
+        tsum[gi] = a1;
+        u = cadd(v, cscale(a1, h2R));
       } else if constexpr (MODE == YMID2) {
         const C a2 = s[e];
         const C v = cmul(opA[i], Ef);
@@ -896,6 +926,8 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
     }
     if constexpr (MODE != YFWD5) {
       __syncthreads();
+      // bufA is free once every thread has read its elements: fetch the next tile's
+      if (TWO && tid == 0 && tile + (int)gridDim.x < total) issueA(tile + gridDim.x);
       stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
       store_tile<C, N, NTHR>(s, out, base, Nt, tid);
     }
@@ -908,8 +940,8 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
 }
 
 template <int N>
-static size_t ytma_smem() {
-  return sizeof(float2) * (size_t)(2 * N * kW + N) + 2 * sizeof(unsigned long long);
+static size_t ytma_smem(int mode) {
+  return sizeof(float2) * (size_t)((mode == YMID1 ? 3 : 2) * N * kW + N) + 3 * sizeof(unsigned long long);
 }
 
 // ---------------------------------------------------------------------------
@@ -1446,15 +1478,16 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
 
 // the y passes of the attempt that k_ypass_tma serves (its `in` map is tmp[1])
 static bool use_ytma(const uppe3d_plan* p, int mode, const void* in) {
-  return p->ytma && (mode == YMID1R || ((mode == YMID2 || mode == YMID3 || mode == YMID4 || mode == YFWD5) &&
-                                        in == p->b.tmp[1]));
+  return p->ytma && (mode == YMID1R || ((mode == YMID1 || mode == YMID2 || mode == YMID3 || mode == YMID4 ||
+                                         mode == YFWD5) && in == p->b.tmp[1]));
 }
 
 template <int N>
 static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
   const dim3 g((unsigned)(2 * p->nsm));
-  const size_t sm = ytma_smem<N>();
+  const size_t sm = ytma_smem<N>(a.mode);
   switch (a.mode) {
+    case YMID1: k_ypass_tma<N, YMID1><<<g, 256, sm, s>>>(a, p->ymaps); break;
     case YMID1R: k_ypass_tma<N, YMID1R><<<g, 256, sm, s>>>(a, p->ymaps); break;
     case YMID2: k_ypass_tma<N, YMID2><<<g, 256, sm, s>>>(a, p->ymaps); break;
     case YMID3: k_ypass_tma<N, YMID3><<<g, 256, sm, s>>>(a, p->ymaps); break;
@@ -1465,8 +1498,10 @@ static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t
 
 template <int N>
 static cudaError_t set_ytma_attr() {
-  const int sm = (int)ytma_smem<N>();
-  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const int sm = (int)ytma_smem<N>(YMID2);
+  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ytma_smem<N>(YMID1));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
@@ -1643,11 +1678,11 @@ static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
   cudaStream_t s = r.s;
   void* const* t = p->b.tmp;
   const bool f = r.fresh != 0;
-  const int KY = p->ytma ? KIND_YT : KIND_Y;   // YMID1R..4, YFWD5 (k_ypass_tma)
+  const int KY = p->ytma ? KIND_YT : KIND_Y;   // the y passes served by k_ypass_tma
   // eval 1 (skipped on device unless the state is fresh)
   rc |= r(KIND_T, 2, f, [&] { return launch_t<Rl, 0>(p, T_FROM_Z, nullptr, t[0], s); });
   rc |= r(KIND_X, 4, f, [&] { return launch_space<Rl>(p, XFWD_Z, t[0], t[1], s); });
-  rc |= r(KIND_Y, 6, f, [&] { return launch_space<Rl>(p, YMID1, t[1], t[0], s); });
+  rc |= r(KY, 6, f, [&] { return launch_space<Rl>(p, YMID1, t[1], t[0], s); });
   rc |= r(KY, 4, !f, [&] { return launch_space<Rl>(p, YMID1R, nullptr, t[0], s); });
   // eval 2..4
   const int mids[3] = {YMID2, YMID3, YMID4};
@@ -1689,9 +1724,9 @@ static int setup_ytma(uppe3d_plan* p) {
   const cuuint64_t strides[2] = {(cuuint64_t)p->g.Nt * 8, (cuuint64_t)p->g.Ny * p->g.Nt * 8};
   const cuuint32_t box[3] = {(cuuint32_t)kW, (cuuint32_t)p->g.Ny, 1};
   const cuuint32_t es[3] = {1, 1, 1};
-  void* bufs[2] = {p->b.tmp[1], p->b.acur};
-  CUtensorMap* maps[2] = {&p->ymaps.in, &p->ymaps.acur};
-  for (int i = 0; i < 2; ++i) {
+  void* bufs[3] = {p->b.tmp[1], p->b.acur, p->b.tmp[2]};
+  CUtensorMap* maps[3] = {&p->ymaps.in, &p->ymaps.acur, &p->ymaps.z2};
+  for (int i = 0; i < 3; ++i) {
     if (reinterpret_cast<uintptr_t>(bufs[i]) % 16) return 0;
     if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, bufs[i], dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -2057,6 +2092,125 @@ extern "C" int uppe3d_diagnostics(uppe3d_plan* p, double dx, double dy, double* 
   UPPE_CK(cudaStreamSynchronize(s));
   if (!p->wabs) out3[1] = NAN;
   return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Beam diagnostics of the current state in one pass: the quantities that
+// src/3+1D-ERK4(3)IP UPPE/sim.py:140-249 computes from a field copied back to
+// the host.  Per omega: sum_xy |Z|^2 and sum_xy m Z (m: a fibre mode); per t,
+// after the inverse t transform a = ifft_t(Z): sum_xy |a|^2 and sum_xy m a; per
+// (x, y): sum_t |a|^2; the centre line (Nx/2, Ny/2) in both domains.  Z is the
+// normalised state; the host applies A_scale, dx, dy, dt.  Per-block sums in
+// shared memory, one global atomic per bin and block.
+// ---------------------------------------------------------------------------
+namespace uppe {
+struct BeamDiagOut {
+  double *spec, *cw, *pt, *ct, *zc, *ac, *flu;
+};
+
+template <int NT, typename Rl> struct BDLaunch {
+  using C = typename CT<Rl>::T;
+  static constexpr size_t per_warp = (size_t)TCfg<NT>::PAD * sizeof(C);
+  static constexpr size_t fixed = NT * sizeof(C) + 6 * NT * sizeof(double);
+  static constexpr int WPB = (fixed + 8 * per_warp <= 160 * 1024) ? 8 : (fixed + 4 * per_warp <= 160 * 1024) ? 4
+                           : (fixed + 2 * per_warp <= 200 * 1024) ? 2 : 1;
+  static size_t smem() { return fixed + WPB * per_warp; }
+};
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+  return v;
+}
+
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_beam_diag(const State3D* st, Bufs3D b, Geom g, const void* twt,
+                                                      const double* mode, BeamDiagOut o) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int E = NT / 32;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  double* acc = reinterpret_cast<double*>(tw + NT);   // [6][NT]: |Z|^2, mZ re/im, |a|^2, ma re/im
+  C* sK = reinterpret_cast<C*>(acc + 6 * NT) + (threadIdx.x >> 5) * PAD;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(twt)[i];
+  for (int i = threadIdx.x; i < 6 * NT; i += WPB * 32) acc[i] = 0.0;
+  __syncthreads();
+  const C* Z = reinterpret_cast<const C*>(b.z[st->zidx]);
+  const long long nl = (long long)g.Nx * g.Ny;
+  const long long centre = (long long)(g.Nx / 2) * g.Ny + g.Ny / 2;
+  const double invN = 1.0 / NT;
+  for (long long line = (long long)blockIdx.x * WPB + warp; line < nl; line += (long long)gridDim.x * WPB) {
+    const double m = mode ? mode[line] : 0.0;
+    const C* zl = Z + line * NT;
+    for (int i = 0; i < E; ++i) {
+      const int w = lane + 32 * i;
+      const C v = zl[w];
+      sK[tpad(w)] = v;
+      const double vr = v.x, vi = v.y;
+      atomicAdd(&acc[w], vr * vr + vi * vi);
+      if (mode) { atomicAdd(&acc[NT + w], m * vr); atomicAdd(&acc[2 * NT + w], m * vi); }
+      if (line == centre) { o.zc[2 * w] = vr; o.zc[2 * w + 1] = vi; }
+    }
+    __syncwarp();
+    stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(sK, tw, lane, LineIdx(), WarpSync());
+    double f = 0.0;
+    for (int i = 0; i < E; ++i) {
+      const int t = lane + 32 * i;
+      const C v = sK[tpad(t)];
+      const double ar = (double)v.x * invN, ai = (double)v.y * invN;
+      const double pw = ar * ar + ai * ai;
+      f += pw;
+      atomicAdd(&acc[3 * NT + t], pw);
+      if (mode) { atomicAdd(&acc[4 * NT + t], m * ar); atomicAdd(&acc[5 * NT + t], m * ai); }
+      if (line == centre) { o.ac[2 * t] = ar; o.ac[2 * t + 1] = ai; }
+    }
+    f = warp_sum_d(f);
+    if (lane == 0) o.flu[line] = f;
+    __syncwarp();
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) {
+    atomicAdd(&o.spec[i], acc[i]);
+    atomicAdd(&o.pt[i], acc[3 * NT + i]);
+    if (mode) {
+      atomicAdd(&o.cw[2 * i], acc[NT + i]);
+      atomicAdd(&o.cw[2 * i + 1], acc[2 * NT + i]);
+      atomicAdd(&o.ct[2 * i], acc[4 * NT + i]);
+      atomicAdd(&o.ct[2 * i + 1], acc[5 * NT + i]);
+    }
+  }
+}
+}  // namespace uppe
+
+template <typename Rl, int NT>
+static int beam_diag_n(uppe3d_plan* p, const double* mode, const BeamDiagOut& o, cudaStream_t s) {
+  constexpr int WPB = BDLaunch<NT, Rl>::WPB;
+  const size_t sm = BDLaunch<NT, Rl>::smem();
+  UPPE_CK(cudaFuncSetAttribute(k_beam_diag<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+  k_beam_diag<Rl, NT, WPB><<<148 * 2, WPB * 32, sm, s>>>(p->st, p->b, p->g, p->tb.twt, mode, o);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" long long uppe3d_beam_diag_elems(const uppe3d_plan* p) {
+  return p ? 10LL * p->g.Nt + (long long)p->g.Nx * p->g.Ny : 0;
+}
+
+extern "C" int uppe3d_beam_diagnostics(uppe3d_plan* p, const double* mode, double* out, cudaStream_t s) {
+  if (!p || !out) return UPPE_ERR_ARG;
+  const long long Nt = p->g.Nt;
+  UPPE_CK(cudaMemsetAsync(out, 0, sizeof(double) * uppe3d_beam_diag_elems(p), s));
+  BeamDiagOut o;
+  o.spec = out; o.cw = out + Nt; o.pt = out + 3 * Nt; o.ct = out + 4 * Nt;
+  o.zc = out + 6 * Nt; o.ac = out + 8 * Nt; o.flu = out + 10 * Nt;
+  switch (p->g.Nt) {
+#define UPPE_BD(n) case n: return p->dbl ? beam_diag_n<double, n>(p, mode, o, s) : beam_diag_n<float, n>(p, mode, o, s);
+    UPPE_BD(32) UPPE_BD(64) UPPE_BD(128) UPPE_BD(256) UPPE_BD(512) UPPE_BD(1024) UPPE_BD(2048)
+#undef UPPE_BD
+    default: return UPPE_ERR_SIZE;
+  }
 }
 
 // ---------------------------------------------------------------------------

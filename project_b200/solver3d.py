@@ -149,6 +149,53 @@ class ERK43IP_UPPE_3D_Optimized:
                                            float(np.sqrt(1.0 - loss)), float(gdd), float(tod),
                                            _lib.stream_ptr(stream)), 'uppe3d_mirror')
 
+    def beam_diagnostics(self, w_mode=None, stream=None):
+        """Diagnostics of the current state (src/3+1D-ERK4(3)IP UPPE/sim.py:140-249),
+        the field-sized sums done on the device in one pass (uppe3d_beam_diagnostics)
+        and only O(Nt + Nx Ny) arrays copied back.  w_mode: waist of the Gaussian
+        fibre mode exp(-r^2 / w_mode^2) for the coupled spectrum and intensity.
+        Returns a dict with the keys of the reference's DIAG record."""
+        dev = self.device
+        mode_ptr = None
+        if w_mode is not None:
+            key = float(w_mode)
+            if getattr(self, '_mode_key', None) != key:
+                x = torch.as_tensor(np.asarray(self.x, dtype=np.float64))
+                y = torch.as_tensor(np.asarray(self.y, dtype=np.float64))
+                self._mode = torch.exp(-(x[:, None] ** 2 + y[None, :] ** 2) / key ** 2).reshape(-1).contiguous().to(dev)
+                self._mode_key = key
+            mode_ptr = ctypes.c_void_p(self._mode.data_ptr())
+        n = self._lib.uppe3d_beam_diag_elems(self._plan)
+        out = torch.empty(n, dtype=torch.float64, device=dev)
+        _lib.check(self._lib.uppe3d_beam_diagnostics(self._plan, mode_ptr, ctypes.c_void_p(out.data_ptr()),
+                                                     _lib.stream_ptr(stream)), 'uppe3d_beam_diagnostics')
+        o = out.cpu().numpy()
+        Nt = self.Nt
+        As2 = self.result(stream).A_scale ** 2
+        cplx = lambda v: v[0::2] + 1j * v[1::2]
+        spec, cw, pt, ct = o[:Nt], cplx(o[Nt:3 * Nt]), o[3 * Nt:4 * Nt], cplx(o[4 * Nt:6 * Nt])
+        zc, ac, flu = cplx(o[6 * Nt:8 * Nt]), cplx(o[8 * Nt:10 * Nt]), o[10 * Nt:].reshape(self.Nx, self.Ny)
+        dxdy = self.dx * self.dy
+        P_t = pt * dxdy * As2
+        fluence = flu * self.dt * As2
+        moments = beam_moments(self.x, self.y, fluence)
+        t = np.asarray(self.t, dtype=np.float64)
+        I_center = np.abs(ac) ** 2 * As2
+        I_smf = np.abs(ct) ** 2 * As2
+        freq_abs = self.freq_axis_hz + self.c / self.lambda0
+        wl_nm = np.zeros_like(freq_abs)
+        ok = freq_abs > 1e9
+        wl_nm[ok] = self.c / freq_abs[ok] * 1e9
+        return {'energy_total': float(pt.sum() * dxdy * self.dt * As2),
+                'x_mean_m': moments[0], 'y_mean_m': moments[1], 'wx_rms_m': moments[2], 'wy_rms_m': moments[3],
+                't_s': t, 'P_t': P_t, 'it_peak': int(np.argmax(P_t)), 'fluence': fluence,
+                'I_center_t': I_center, 'I_smf_t': I_smf,
+                'fwhm_center_s': fwhm(t, I_center), 'fwhm_smf_s': fwhm(t, I_smf),
+                'freq_abs_Hz': freq_abs, 'wl_nm': wl_nm,
+                'spec_full_incoh': np.fft.fftshift(spec * As2),
+                'spec_center': np.fft.fftshift(np.abs(zc) ** 2 * As2),
+                'spec_smf': np.fft.fftshift(np.abs(cw) ** 2 * As2)}
+
     def diagnostics(self, stream=None):
         """{'energy' [J], 'photons', 'peak_ionization'} of the current state (device)."""
         out = (ctypes.c_double * 3)()
@@ -253,3 +300,46 @@ def ip_operator_host(tb, kx_index=None):
     kz = np.sqrt((tb['k_sq'][None, None, :] - q).astype(np.complex128))
     D = 1j * (num / (kz + tb['k_ref'][None, None, :]))
     return D * tb['valid'][None, None, :]
+
+
+def beam_moments(x, y, fluence):
+    """Centroid and rms widths of a fluence map F[ix, iy] (sim.py:145-157)."""
+    X, Y = np.meshgrid(np.asarray(x, dtype=np.float64), np.asarray(y, dtype=np.float64), indexing='ij')
+    dxdy = float(x[1] - x[0]) * float(y[1] - y[0])
+    tot = float(np.sum(fluence)) * dxdy + 1e-30
+    xm = float(np.sum(X * fluence)) * dxdy / tot
+    ym = float(np.sum(Y * fluence)) * dxdy / tot
+    x2 = float(np.sum((X - xm) ** 2 * fluence)) * dxdy / tot
+    y2 = float(np.sum((Y - ym) ** 2 * fluence)) * dxdy / tot
+    return xm, ym, float(np.sqrt(x2)), float(np.sqrt(y2))
+
+
+def fwhm(t, I):
+    """Full width at half maximum of I(t) (sim.py:159-182): walk out from the peak
+    to the first samples below half, interpolate linearly on each side; NaN when
+    undefined."""
+    I = np.asarray(I, dtype=np.float64)
+    t = np.asarray(t, dtype=np.float64)
+    if I.size < 4:
+        return float('nan')
+    top = float(np.max(I))
+    if not np.isfinite(top) or top <= 0:
+        return float('nan')
+    half = 0.5 * top
+    k = int(np.argmax(I))
+    lo = k
+    while lo > 0 and I[lo] >= half:
+        lo -= 1
+    hi = k
+    while hi < I.size - 1 and I[hi] >= half:
+        hi += 1
+    if hi <= lo + 1:
+        return float('nan')
+
+    def cross(i, j):
+        return t[i] + (half - I[i]) * (t[j] - t[i]) / (I[j] - I[i] + 1e-30)
+
+    left = cross(lo, lo + 1)
+    right = cross(hi - 1, hi)
+    w = right - left
+    return float(w) if (w > 0 and np.isfinite(w)) else float('nan')

@@ -173,3 +173,24 @@ def test_diagnostics_vs_oracle():
     assert abs(d['energy'] - Eo) <= 1e-10 * Eo
     assert abs(d['photons'] - pho) <= 1e-10 * pho
     assert abs(d['peak_ionization'] - peak) <= 1e-8 * peak
+
+
+@pytest.mark.parametrize('precision,tol', [('double', 1e-10), ('single', 1e-4)])
+def test_beam_diagnostics_vs_oracle(precision, tol):
+    """sim.py:140-249 quantities from the device pass vs the oracle on the field."""
+    from oracle.diagnostics import beam_diagnostics
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(N=64, Nt=128)
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(lam, 1.0, precision, True, lut=lut), precision=precision)
+    sol.propagate(A0, 0.01, tol=1e-5)
+    d = sol.beam_diagnostics(w_mode=0.4e-3)
+    A = sol.field().cpu().numpy().astype(np.complex128)
+    o = beam_diagnostics(A, x, x, t, 0.4e-3, lam)
+    for k in ('energy_total', 'x_mean_m', 'y_mean_m', 'wx_rms_m', 'wy_rms_m', 'fwhm_center_s', 'fwhm_smf_s'):
+        scale = abs(o[k]) if k not in ('x_mean_m', 'y_mean_m') else o['wx_rms_m']
+        assert abs(d[k] - o[k]) <= tol * scale + 1e-30, k
+    for k in ('P_t', 'fluence', 'spec_smf', 'spec_full_incoh', 'spec_center', 'I_center_t', 'I_smf_t',
+              'freq_abs_Hz'):
+        assert rel_l2(d[k], o[k]) < tol, k
+    assert d['it_peak'] == o['it_peak']

@@ -152,3 +152,21 @@ def test_gas_cell_program_slices_follow_the_beam():
     # symmetric about the focus, largest at the centre
     g = np.array([s.gamma for s in prog])
     assert np.allclose(g, g[::-1], rtol=1e-12) and g.argmax() in (24, 25)
+
+
+def test_fwhm_and_moments_match_the_driver_formulas():
+    """project_b200.solver3d.fwhm / beam_moments vs the restated sim.py:145-182."""
+    from oracle.diagnostics import _fwhm, beam_diagnostics
+    from project_b200.solver3d import beam_moments, fwhm
+    rng = np.random.Generator(np.random.PCG64(5))
+    t = np.linspace(-200e-15, 200e-15, 256)
+    for _ in range(20):
+        w = rng.uniform(10e-15, 80e-15)
+        I = np.exp(-((t - rng.uniform(-50e-15, 50e-15)) / w) ** 2) + 0.05 * rng.random(256)
+        assert fwhm(t, I) == _fwhm(t, I)
+    assert np.isnan(fwhm(t, np.zeros(256))) and np.isnan(_fwhm(t, np.zeros(256)))
+    x = np.linspace(-1e-3, 1e-3, 32)
+    A = (rng.standard_normal((32, 32, 16)) + 1j * rng.standard_normal((32, 32, 16)))
+    o = beam_diagnostics(A, x, x, t[:16], 0.3e-3, 800e-9)
+    m = beam_moments(x, x, o['fluence'])
+    assert np.allclose(m, [o['x_mean_m'], o['y_mean_m'], o['wx_rms_m'], o['wy_rms_m']], rtol=1e-12, atol=1e-18)
