@@ -785,6 +785,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
   C* bufA = buf[1] + TILE;
   C* tw = TWO ? bufA + TILE : buf[1] + TILE;
   unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);   // [2]: bufA
+  double* qrow = reinterpret_cast<double*>(mbar + 3);   // k_perp^2 of the tile's kx row [N]
   State3D* st = a.st;
   if (st->done) return;
   if (MODE == YMID1R && st->fresh) return;
@@ -853,6 +854,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
     const long long base = (long long)o * Ny * Nt + w0;
     // operands of this thread's elements (e = tid + i*NTHR), in flight during the wait and FFT
     C opA[E], opB[E];
+    const double qn = (tid < N && MODE != YMID4 && MODE != YFWD5) ? __ldg(a.tb.q + (long long)o * Ny + tid) : 0.0;
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const int e = tid + i * NTHR;
@@ -862,6 +864,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
       else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
       else if constexpr (MODE == YFWD5) opA[i] = __ldg(a4p + gi);
     }
+    if (tid < N) qrow[tid] = qn;   // read after the barrier below
     bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
     if (TWO) ok = ok && mbar_wait(smem_u32(&mbar[2]), (unsigned)(k & 1));
     if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
@@ -893,8 +896,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
         s[e] = A4;
         continue;
       }
-      const double qv = a.tb.q[(long long)o * Ny + n];
-      const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qv, h2);
+      const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qrow[n], h2);
       C u;
       if constexpr (MODE == YMID1R) {   // s = A tile, opB = k1
         const C v = cmul(s[e], Ef);
@@ -941,7 +943,8 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
 
 template <int N>
 static size_t ytma_smem(int mode) {
-  return sizeof(float2) * (size_t)((mode == YMID1 ? 3 : 2) * N * kW + N) + 3 * sizeof(unsigned long long);
+  return sizeof(float2) * (size_t)((mode == YMID1 ? 3 : 2) * N * kW + N) + 3 * sizeof(unsigned long long) +
+         N * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -1053,14 +1056,19 @@ k_tpass_w(TArgs a) {
   C* S = tw + NT + warp * BUF;
   double* starts = reinterpret_cast<double*>(tw + NT + WPB * BUF) + warp * 32;
   // rates of the line in time order (one pad per 32: conflict-free both ways)
-  float* sW = reinterpret_cast<float*>(reinterpret_cast<double*>(tw + NT + WPB * BUF) + WPB * 32) +
-              warp * (NT + NT / 32);
+  float* sW0 = reinterpret_cast<float*>(reinterpret_cast<double*>(tw + NT + WPB * BUF) + WPB * 32);
+  float* sW = sW0 + warp * (NT + NT / 32);
+  // output factor per omega bin: shock factor (> 0) where omega_abs > 0, -1 where masked
+  Rl* shm = reinterpret_cast<Rl*>(sW0 + WPB * (NT + NT / 32));
   auto wpad = [](int t) { return t + (t >> 5); };
   {
     // four-step twiddles tw[k*32 + l] = W_NT^(l k) (l < 32, k < E; l k < NT): the
     // per-lane factors of a column k are consecutive (conflict-free loads)
     const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
-    for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = gtw[(i & 31) * (i >> 5)];
+    for (int i = threadIdx.x; i < NT; i += WPB * 32) {
+      tw[i] = gtw[(i & 31) * (i >> 5)];
+      shm[i] = a.tb.valid[i] ? (Rl)a.tb.shock[i] : (Rl)-1;
+    }
   }
   __syncthreads();
   State3D* st = a.st;
@@ -1180,9 +1188,10 @@ k_tpass_w(TArgs a) {
 #pragma unroll
   for (int k = 0; k < E; ++k) {
     const int wi = W::out_index(lane, k);
-    C o = cscale(v[k], (Rl)a.tb.shock[wi]);
+    const Rl sh = shm[wi];
+    C o = cscale(v[k], sh);
     if (plasma_line) o = cadd(o, pv[k]);
-    if (!a.tb.valid[wi]) o = C{0, 0};
+    if (sh < (Rl)0) o = C{0, 0};
     dst[wi] = o;
   }
 }
@@ -1550,7 +1559,7 @@ template <int NT, typename Rl> struct TWarp {
                                  ? WarpFFT<(E < 16 ? 16 : E)>::SBUF : TCfg<NT>::PAD;
   static size_t smem() {
     return (size_t)(NT + WPB * BUF) * sizeof(typename CT<Rl>::T) + (size_t)WPB * 32 * sizeof(double) +
-           (size_t)WPB * (NT + NT / 32) * sizeof(float);
+           (size_t)WPB * (NT + NT / 32) * sizeof(float) + (size_t)NT * sizeof(Rl);
   }
 };
 
