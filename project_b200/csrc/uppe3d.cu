@@ -509,16 +509,22 @@ k_xpass_sq(SpaceArgs a) {
 #pragma unroll
   for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
   if (mode == XINV_Z) {
-    // candidate state Z = ifft2(A4) * filter(omega) * exp(-damp(x,y) h)
+    // candidate state Z = ifft2(A4) * filter(omega) * exp(-damp(x,y) h); one
+    // absorber factor per x of this y (exp(-0 h) = 1 exactly), kept in the
+    // transpose buffer, which fft_sq has released
+    Rl* absx = reinterpret_cast<Rl*>(T);
+    for (int x = tid; x < N; x += NTHR) {
+      const double dp = a.tb.damp[(long long)x * Ny + o];
+      absx[x] = dp == 0.0 ? (Rl)1 : (Rl)exp(-dp * h);
+    }
+    __syncthreads();
     C* __restrict__ zc = reinterpret_cast<C*>(a.b.z[st->zidx ^ 1]);
     const Rl nrm = (Rl)(1.0 / ((double)a.g.Nx * (double)a.g.Ny));
     const Rl f = (Rl)a.tb.filt[w0 + w];
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int x = j + R * i;   // output row = x index, o = y index
-      const double dp = a.tb.damp[(long long)x * Ny + o];
-      const Rl ab = dp == 0.0 ? (Rl)1 : (Rl)exp(-dp * h);   // exp(-0 h) = 1 exactly
-      zc[gidx(i)] = cscale(cscale(cscale(v[i], nrm), f), ab);
+      zc[gidx(i)] = cscale(cscale(cscale(v[i], nrm), f), absx[x]);
     }
   }
   if (mode == XFWD_Z) {
