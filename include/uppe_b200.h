@@ -216,6 +216,15 @@ typedef struct {
 int uppe1d_run_programs(uppe1d_plan* plan, int nprog, const long long* op_begin, const uppe1d_op* ops,
                         void* fields, void* records, uppe1d_result* op_results, uppe_stream_t stream);
 
+/* Spectral amplitude of an input pulse from a measured spectrum (the per-sample part
+ * of generate_pulse_from_spectrum, erk43ip_method.py:599-764, FFT path): S(f) is the
+ * piecewise cubic coef[4j..4j+3] (power form in f - breaks[j], highest first) on
+ * ascending breaks[0..nb-1] (device arrays); out (device complex128 [Nt], fft order)
+ * = sqrt(max(S(f_k), 0)) exp(i (gdd w_k^2/2 + tod w_k^3/6)) with w_k = 2 pi
+ * fftfreq(Nt, dt)[k], f_k = w_k/(2 pi) + f0, S = 0 outside the breaks. */
+int uppe_spectrum_field(const double* breaks, const double* coef, int nb, int Nt, double dt, double f0,
+                        double gdd, double tod, void* out, uppe_stream_t stream);
+
 /* Workspace of uppe1d_adjoint, in complex128 elements. */
 long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K);
 /* Reverse-mode derivative of one instance's frozen-schedule propagation (complex128

@@ -74,3 +74,42 @@ def gaussian_beam_3d(x, y, t, w0, pulse_energy, pulse_fwhm):
     dx, dy, dt = x[1] - x[0], y[1] - y[0], t[1] - t[0]
     E = np.sum(np.abs(A) ** 2) * dx * dy * dt
     return (A * np.sqrt(pulse_energy / E)).astype(np.complex128)
+
+
+def pulse_from_spectrum(t, wavelengths_nm, intensities, pulse_energy, GDD=0.0, TOD=0.0,
+                        use_jacobian=True, interp_kind='cubic', center_wavelength=800e-9):
+    """Restatement of ``generate_pulse_from_spectrum`` (erk43ip_method.py:599-764),
+    FFT path: sort by wavelength, normalise, to frequency with the Jacobian
+    lambda^2/c (renormalised), drop duplicate frequencies, interpolate onto the
+    simulation grid (zero outside), sqrt, GDD/TOD phase, ifft, fftshift, energy
+    normalisation by the trapezoidal rule."""
+    from scipy.interpolate import interp1d
+    c = 299792458.0
+    t = np.asarray(t, dtype=np.float64)
+    idx = np.argsort(wavelengths_nm)                                       # :676
+    wl = np.asarray(wavelengths_nm, dtype=np.float64)[idx]
+    I = np.asarray(intensities, dtype=np.float64)[idx]
+    if np.max(I) > 0:                                                       # :681
+        I = I / np.max(I)
+    f = c / (wl * 1e-9)                                                     # :685
+    if use_jacobian:                                                        # :687-693
+        I = I * (wl * 1e-9) ** 2 / c
+        if np.max(I) > 0:
+            I = I / np.max(I)
+    uf, ui = np.unique(f, return_index=True)                                # :698-701
+    if len(uf) < len(f):
+        f, I = uf, I[ui]
+    if f[0] < f[-1]:                                                        # :704-706
+        f, I = f[::-1], I[::-1]
+    kind = 'linear' if interp_kind in ('cubic', 'quadratic') and len(f) < 4 else interp_kind
+    g = interp1d(f, I, kind=kind, bounds_error=False, fill_value=0.0)      # :715
+    N, dt = len(t), t[1] - t[0]
+    w = 2 * np.pi * fftfreq(N, dt)                                          # :719
+    S = g(w / (2 * np.pi) + c / center_wavelength)
+    S[S < 0] = 0
+    S[np.isnan(S)] = 0
+    A = fftshift(ifft(np.sqrt(S) * np.exp(1j * (0.5 * GDD * w ** 2 + (1.0 / 6.0) * TOD * w ** 3))))
+    E = np.trapz(np.abs(A) ** 2, t)                                         # :739
+    if E > 0:
+        A = A * np.sqrt(pulse_energy / E)
+    return A

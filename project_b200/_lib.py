@@ -88,6 +88,7 @@ SIGNATURES = {
     'uppe1d_propagate_logged': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe1d_propagate_schedule': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe3d_mirror': (_I, [_P, _P, _D, _D, _D, _D, _P]),
+    'uppe_spectrum_field': (_I, [_P, _P, _I, _I, _D, _D, _D, _D, _P, _P]),
     'uppe3d_beam_diag_elems': (_LL, [_P]),
     'uppe3d_beam_diagnostics': (_I, [_P, _P, _P, _P]),
     'uppe1d_run_programs': (_I, [_P, _I, ctypes.POINTER(_LL), ctypes.POINTER(Op1D), _P, _P,

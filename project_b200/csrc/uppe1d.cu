@@ -434,3 +434,48 @@ extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int 
   UPPE1_CK(launch_uppe1d_adjoint(a, p->smem, s));
   return 0;
 }
+
+// ---------------------------------------------------------------------------
+// Input pulse from a measured spectrum (erk43ip_method.py:599-764, FFT path):
+// the spectral density S(f), given as a piecewise cubic over ascending
+// breakpoints, is evaluated on the simulation grid f = w/(2 pi) + f0 (zero
+// outside the breakpoints, clipped at 0), and A_w = sqrt(S) exp(i (gdd w^2/2 +
+// tod w^3/6)) is written in fft order.
+// ---------------------------------------------------------------------------
+namespace uppe {
+__global__ void k_spectrum_field(const double* br, const double* cf, int nb, int n, double dt, double f0,
+                                 double gdd, double tod, double2* out) {
+  const double val = 1.0 / (n * dt);                  // fftfreq(n, dt) = k * val
+  const double twopi = 6.283185307179586476925286766559;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double w = twopi * ((k < (n + 1) / 2 ? k : k - n) * val);
+    const double f = w / twopi + f0;
+    double S = 0.0;
+    if (f >= br[0] && f <= br[nb - 1]) {
+      int lo = 0, hi = nb - 2;                        // last interval with br[j] <= f
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (br[mid] <= f) lo = mid; else hi = mid - 1;
+      }
+      const double x = f - br[lo];
+      const double* c = cf + 4 * (long long)lo;
+      S = ((c[0] * x + c[1]) * x + c[2]) * x + c[3];
+    }
+    if (!(S > 0.0)) S = 0.0;                          // negative or NaN -> 0
+    const double m = sqrt(S);
+    double sn, cs;
+    sincos(0.5 * gdd * w * w + (1.0 / 6.0) * tod * w * w * w, &sn, &cs);
+    out[k] = make_double2(m * cs, m * sn);
+  }
+}
+}  // namespace uppe
+
+extern "C" int uppe_spectrum_field(const double* breaks, const double* coef, int nb, int Nt, double dt,
+                                   double f0, double gdd, double tod, void* out, cudaStream_t s) {
+  if (!breaks || !coef || !out || nb < 2 || Nt < 1 || !(dt > 0.0)) return UPPE_ERR_ARG;
+  const int threads = 256;
+  const int blocks = (Nt + threads - 1) / threads < 1024 ? (Nt + threads - 1) / threads : 1024;
+  k_spectrum_field<<<blocks, threads, 0, s>>>(breaks, coef, nb, Nt, dt, f0, gdd, tod, (double2*)out);
+  UPPE1_CK(cudaGetLastError());
+  return 0;
+}

@@ -114,3 +114,66 @@ def zernike_basis(x, y, aperture_radius, jmax=15):
     rho = np.sqrt(X ** 2 + Y ** 2) / aperture_radius
     th = np.arctan2(Y, X)
     return np.stack([zernike(j, rho, th) for j in range(1, jmax + 1)])
+
+
+def spectrum_spline(wavelengths_nm, intensities, use_jacobian=True, interp_kind='cubic'):
+    """Host part of generate_pulse_from_spectrum (erk43ip_method.py:674-716): sort,
+    normalise, to frequency with the Jacobian lambda^2/c (renormalised), drop
+    duplicate frequencies, and the interpolant of interp1d(kind) as a piecewise
+    cubic: (breaks ascending [nb], coef [nb-1, 4] highest power first)."""
+    from scipy.interpolate import PPoly, make_interp_spline
+    idx = np.argsort(wavelengths_nm)
+    wl = np.asarray(wavelengths_nm, dtype=np.float64)[idx]
+    I = np.asarray(intensities, dtype=np.float64)[idx]
+    if np.max(I) > 0:
+        I = I / np.max(I)
+    f = C0 / (wl * 1e-9)
+    if use_jacobian:
+        I = I * (wl * 1e-9) ** 2 / C0
+        if np.max(I) > 0:
+            I = I / np.max(I)
+    uf, ui = np.unique(f, return_index=True)
+    if len(uf) < len(f):
+        f, I = uf, I[ui]
+    order = np.argsort(f)                      # interp1d sorts its abscissae
+    f, I = f[order], I[order]
+    k = {'linear': 1, 'quadratic': 2, 'cubic': 3}[interp_kind]
+    if k > 1 and len(f) < 4:
+        k = 1
+    pp = PPoly.from_spline(make_interp_spline(f, I, k=k))
+    br, c = pp.x, pp.c                         # c[m, j]: power (k - m) on interval j
+    keep = np.diff(br) > 0                     # drop the zero-length end intervals
+    coef = np.zeros((int(keep.sum()), 4))
+    coef[:, 4 - c.shape[0]:] = c[:, keep].T
+    brk = np.concatenate([br[:-1][keep], [br[1:][keep][-1]]])
+    return brk, coef
+
+
+def pulse_from_spectrum(t, wavelengths_nm, intensities, pulse_energy, GDD=0.0, TOD=0.0,
+                        use_jacobian=True, interp_kind='cubic', center_wavelength=800e-9,
+                        device=None):
+    """generate_pulse_from_spectrum (erk43ip_method.py:599-764, FFT path) with the
+    per-sample work on the device (uppe_spectrum_field): the interpolated spectral
+    density on the simulation grid, its square root and the GDD/TOD phase; then
+    ifft, fftshift and the trapezoidal energy normalisation.  Returns a complex128
+    torch tensor on the device."""
+    import ctypes
+    import torch
+    from . import _lib
+    lib = _lib.load()
+    dev = torch.device(device if device is not None else 'cuda')
+    t = np.asarray(t, dtype=np.float64)
+    brk, coef = spectrum_spline(wavelengths_nm, intensities, use_jacobian, interp_kind)
+    b = torch.from_numpy(np.ascontiguousarray(brk)).to(dev)
+    c = torch.from_numpy(np.ascontiguousarray(coef)).to(dev)
+    N, dt = len(t), float(t[1] - t[0])
+    Aw = torch.empty(N, dtype=torch.complex128, device=dev)
+    _lib.check(lib.uppe_spectrum_field(ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(c.data_ptr()), len(brk), N,
+                                       dt, C0 / center_wavelength, float(GDD), float(TOD),
+                                       ctypes.c_void_p(Aw.data_ptr()), _lib.stream_ptr()), 'uppe_spectrum_field')
+    A = torch.fft.fftshift(torch.fft.ifft(Aw))
+    P = (A.real ** 2 + A.imag ** 2)
+    E = float(torch.trapezoid(P, torch.from_numpy(t).to(dev)))
+    if E > 0:
+        A = A * np.sqrt(pulse_energy / E)
+    return A

@@ -225,6 +225,37 @@ def make_1d():
     sys.path.remove(REF_1D)
 
 
+def spectrum_case():
+    """Seeded synthetic measured-style spectrum: wavelengths [nm] and intensities."""
+    rng = np.random.Generator(np.random.PCG64(21))
+    wl = np.linspace(740.0, 860.0, 301)
+    I = np.exp(-((wl - 800.0) / 18.0) ** 2) * (1 + 0.2 * np.cos(2 * np.pi * (wl - 740.0) / 23.0))
+    I = I + 0.01 * rng.random(wl.size)
+    return wl, I
+
+
+def make_spectrum():
+    """generate_pulse_from_spectrum (erk43ip_method.py:599-764, FFT path): four
+    option sets; the third passes the spectrum in descending wavelength order."""
+    sys.path.insert(0, REF_1D)
+    erk = load(os.path.join(REF_1D, 'erk43ip_method.py'), 'erk43ip_method')
+    s = erk.ERK43IP_UPPE(material='argon_gas', n2=1.0e-23, beam_radius=0.65 * 125e-6,
+                         center_wavelength=800e-9)
+    wl, I = spectrum_case()
+    t = np.linspace(-0.5e-12, 0.5e-12, 2048)
+    cases = [('cubic', True, 0.0, 0.0, False), ('cubic', True, 300e-30, 2000e-45, False),
+             ('linear', False, -200e-30, 0.0, True), ('quadratic', True, 0.0, -1000e-45, False)]
+    out = {}
+    for k, (kind, jac, gdd, tod, rev) in enumerate(cases):
+        w, i = (wl[::-1].copy(), I[::-1].copy()) if rev else (wl, I)
+        out[f'A{k}'] = s.generate_pulse_from_spectrum(t, w, i, 50e-6, GDD=gdd, TOD=tod, use_jacobian=jac,
+                                                      interp_kind=kind)
+    save('ref1d_spectrum_pulse', t=t, wl=wl, I=I, E=50e-6, kinds=np.array([c[0] for c in cases]),
+         jac=np.array([c[1] for c in cases]), gdd=np.array([c[2] for c in cases]),
+         tod=np.array([c[3] for c in cases]), rev=np.array([c[4] for c in cases]), **out)
+    sys.path.remove(REF_1D)
+
+
 # ---------------------------------------------------------------------------
 # 3D fixtures
 # ---------------------------------------------------------------------------
@@ -329,5 +360,6 @@ if __name__ == '__main__':
     install_stand_ins()
     print('1D fixtures from', REF_1D)
     make_1d()
+    make_spectrum()
     print('3D fixtures from', REF_3D)
     make_3d()

@@ -138,3 +138,14 @@ def test_diagnostics_vs_oracle():
     assert abs(r.energy - Eo) <= 1e-10 * Eo
     assert abs(r.photons - pho) <= 1e-10 * pho
     assert abs(r.peak_ion - peak) <= 1e-8 * peak
+
+
+def test_pulse_from_spectrum_matches_reference():
+    """The device spectrum-to-field builder vs generate_pulse_from_spectrum run here."""
+    from project_b200.pulses import pulse_from_spectrum
+    g = golden('ref1d_spectrum_pulse')
+    for k in range(4):
+        w, i = (g['wl'][::-1], g['I'][::-1]) if g['rev'][k] else (g['wl'], g['I'])
+        A = pulse_from_spectrum(g['t'], w, i, float(g['E']), float(g['gdd'][k]), float(g['tod'][k]),
+                                bool(g['jac'][k]), str(g['kinds'][k]))
+        assert rel_l2(A.cpu().numpy(), g[f'A{k}']) < 1e-12

@@ -170,3 +170,28 @@ def test_fwhm_and_moments_match_the_driver_formulas():
     o = beam_diagnostics(A, x, x, t[:16], 0.3e-3, 800e-9)
     m = beam_moments(x, x, o['fluence'])
     assert np.allclose(m, [o['x_mean_m'], o['y_mean_m'], o['wx_rms_m'], o['wy_rms_m']], rtol=1e-12, atol=1e-18)
+
+
+@pytest.mark.parametrize('kind', ['cubic', 'quadratic', 'linear'])
+def test_spectrum_spline_matches_interp1d(kind):
+    """The piecewise cubic handed to the device equals interp1d(kind) of the
+    Jacobian-scaled spectrum (erk43ip_method.py:674-716), zero outside."""
+    from scipy.interpolate import interp1d
+    from conftest import golden
+    from project_b200.pulses import spectrum_spline
+    g = golden('ref1d_spectrum_pulse')
+    c = 299792458.0
+    brk, coef = spectrum_spline(g['wl'][::-1], g['I'][::-1], True, kind)
+    wl = np.sort(g['wl'])
+    I = g['I'][np.argsort(g['wl'])]
+    I = I / I.max()
+    f = c / (wl * 1e-9)
+    Ij = I * (wl * 1e-9) ** 2 / c
+    Ij = Ij / Ij.max()
+    x = np.linspace(brk[0] - 1e12, brk[-1] + 1e12, 4001)
+    j = np.clip(np.searchsorted(brk, x, side='right') - 1, 0, len(brk) - 2)
+    d = x - brk[j]
+    v = ((coef[j, 0] * d + coef[j, 1]) * d + coef[j, 2]) * d + coef[j, 3]
+    v[(x < brk[0]) | (x > brk[-1])] = 0
+    r = interp1d(f, Ij, kind=kind, bounds_error=False, fill_value=0.0)(x)
+    assert np.abs(v - r).max() < 1e-14

@@ -116,3 +116,16 @@ def test_3d_matches_reference(name):
     assert abs(z - float(g['z'])) < 1e-12
     assert np.array_equal(freq, g['freq'])
     assert rel_l2(A_w, g['A_w']) < (1e-12 if double else 1e-5)
+
+
+def test_pulse_from_spectrum_oracle_matches_reference():
+    """generate_pulse_from_spectrum (erk43ip_method.py:599-764) run here on a seeded
+    spectrum, four option sets (cubic / linear / quadratic, Jacobian on/off, GDD/TOD,
+    descending input order)."""
+    from oracle.inputs import pulse_from_spectrum
+    g = golden('ref1d_spectrum_pulse')
+    for k in range(4):
+        w, i = (g['wl'][::-1], g['I'][::-1]) if g['rev'][k] else (g['wl'], g['I'])
+        A = pulse_from_spectrum(g['t'], w, i, float(g['E']), float(g['gdd'][k]), float(g['tod'][k]),
+                                bool(g['jac'][k]), str(g['kinds'][k]))
+        assert rel_l2(A, g[f'A{k}']) < 1e-13
