@@ -250,6 +250,14 @@ def make_spectrum():
         w, i = (wl[::-1].copy(), I[::-1].copy()) if rev else (wl, I)
         out[f'A{k}'] = s.generate_pulse_from_spectrum(t, w, i, 50e-6, GDD=gdd, TOD=tod, use_jacobian=jac,
                                                       interp_kind=kind)
+    # analysis helpers on a propagated field (erk43ip_method.py:448-490, 766-808)
+    g = np.load(os.path.join(HERE, 'ref1d_argon.npz'))
+    A, ta = g['A_final'], g['t']
+    xl, xr, fw = s._calculate_fwhm_precise(ta, np.abs(A) ** 2)
+    ph = s.analyze_spectral_phase(A, ta, fit_order=4, plot_threshold=0.01)
+    ph3 = s.analyze_spectral_phase(A * np.exp(1j * 3e26 * (ta - 1e-13) ** 2), ta, fit_order=3, plot_threshold=0.05)
+    save('ref1d_analysis', t=ta, A=A, fwhm=np.array([xl, xr, fw]), chirp=3e26,
+         **{f'p4_{k}': v for k, v in ph.items()}, **{f'p3_{k}': v for k, v in ph3.items()})
     save('ref1d_spectrum_pulse', t=t, wl=wl, I=I, E=50e-6, kinds=np.array([c[0] for c in cases]),
          jac=np.array([c[1] for c in cases]), gdd=np.array([c[2] for c in cases]),
          tod=np.array([c[3] for c in cases]), rev=np.array([c[4] for c in cases]), **out)

@@ -195,3 +195,22 @@ def test_spectrum_spline_matches_interp1d(kind):
     v[(x < brk[0]) | (x > brk[-1])] = 0
     r = interp1d(f, Ij, kind=kind, bounds_error=False, fill_value=0.0)(x)
     assert np.abs(v - r).max() < 1e-14
+
+
+def test_analysis_helpers_match_reference():
+    """fwhm_precise / analyze_spectral_phase vs the reference's methods run on a
+    propagated field (erk43ip_method.py:448-490, 766-808)."""
+    from conftest import golden
+    from project_b200.analysis import analyze_spectral_phase, fwhm_precise
+    g = golden('ref1d_analysis')
+    t, A = g['t'], g['A']
+    xl, xr, fw = fwhm_precise(t, np.abs(A) ** 2)
+    assert np.allclose([xl, xr, fw], g['fwhm'], rtol=1e-12, atol=0)
+    w0 = 2 * np.pi * 299792458.0 / 800e-9
+    for tag, B, order, thr in (('p4', A, 4, 0.01),
+                               ('p3', A * np.exp(1j * float(g['chirp']) * (t - 1e-13) ** 2), 3, 0.05)):
+        r = analyze_spectral_phase(B, t, w0, order, thr)
+        for k in ('wavelength_nm', 'spectral_intensity', 'mask'):
+            assert np.array_equal(r[k], g[f'{tag}_{k}']) if k == 'mask' else np.allclose(r[k], g[f'{tag}_{k}'], rtol=1e-12)
+        band = g[f'{tag}_mask']
+        assert np.allclose(r['residual_phase'][band], g[f'{tag}_residual_phase'][band], rtol=1e-7, atol=1e-7)
