@@ -66,13 +66,34 @@ extern "C" void _launch_plasma_integration_kernel(unsigned grid, unsigned block,
 '''
 
 
+_LAUNCHER_RF = r'''
+extern "C" void _launch_plasma_integration_kernel(unsigned grid, unsigned block,
+    const float* E, const float* W_ion, const float* W_ava, double* J, double* rho,
+    float rate_rec, float dt, float rho_nt, float Ui, float e_charge, float m_e, float tau_c,
+    int Nt, int nsp) {
+  blockDim.x = block; blockDim.y = blockDim.z = 1;
+  for (unsigned b = 0; b < grid; ++b) {
+    blockIdx.x = b;
+    for (unsigned t = 0; t < block; ++t) {
+      threadIdx.x = t;
+      plasma_integration_kernel(E, W_ion, W_ava, J, rho, rate_rec, dt, rho_nt, Ui, e_charge, m_e,
+                                tau_c, Nt, nsp);
+    }
+  }
+}
+'''
+
+
 class _HostRawKernel:
-    """cp.RawKernel stand-in: compiles the reference's kernel source with g++."""
+    """cp.RawKernel stand-in: compiles the reference's kernel source with g++.  Two
+    sources exist under the same name: the envelope density kernel and the
+    real-field density + Drude current kernel (it takes the field and writes J)."""
 
     def __init__(self, code, name):
         assert name == 'plasma_integration_kernel', name
+        self.rf = 'J_out' in code
         os.makedirs(REF_BUILD, exist_ok=True)
-        src = _PRELUDE + code + _LAUNCHER
+        src = _PRELUDE + code + (_LAUNCHER_RF if self.rf else _LAUNCHER)
         tag = hashlib.sha1(src.encode()).hexdigest()[:12]
         cpp = os.path.join(REF_BUILD, f'plasma_kernel_{tag}.cpp')
         so = os.path.join(REF_BUILD, f'plasma_kernel_{tag}.so')
@@ -83,11 +104,27 @@ class _HostRawKernel:
         lib = ctypes.CDLL(so)
         fn = lib._launch_plasma_integration_kernel
         P = ctypes.c_void_p
-        fn.argtypes = [ctypes.c_uint, ctypes.c_uint, P, P, P, P, ctypes.c_float,
-                       ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int]
+        F = ctypes.c_float
+        if self.rf:
+            fn.argtypes = [ctypes.c_uint, ctypes.c_uint, P, P, P, P, P, F, F, F, F, F, F, F,
+                           ctypes.c_int, ctypes.c_int]
+        else:
+            fn.argtypes = [ctypes.c_uint, ctypes.c_uint, P, P, P, P, ctypes.c_float,
+                           ctypes.c_float, ctypes.c_float, ctypes.c_int, ctypes.c_int]
         self._fn = fn
 
     def __call__(self, grid, block, args):
+        if self.rf:
+            E, W_ion, W_ava, J, rho = args[:5]
+            for a in (E, W_ion, W_ava, J, rho):
+                assert a.flags['C_CONTIGUOUS']
+            # the kernel reads float32 fields (the reference's single precision)
+            assert E.dtype == np.float32 and W_ion.dtype == np.float32 and W_ava.dtype == np.float32
+            assert J.dtype == np.float64 and rho.dtype == np.float64
+            sc = [float(v) for v in args[5:12]]
+            self._fn(int(grid[0]), int(block[0]), E.ctypes.data, W_ion.ctypes.data, W_ava.ctypes.data,
+                     J.ctypes.data, rho.ctypes.data, *sc, int(args[12]), int(args[13]))
+            return
         W_ion, W_ava, rho, gen, rr, dt, rnt, Nt, nsp = args
         for a in (W_ion, W_ava, rho, gen):
             assert a.flags['C_CONTIGUOUS']
@@ -265,6 +302,50 @@ def make_spectrum():
 
 
 # ---------------------------------------------------------------------------
+# real-field 3+1D fixtures
+# ---------------------------------------------------------------------------
+REF_RF = os.path.join(REF, 'src', '3+1D-UPPE-ERK4(3)IP-real-field')
+
+
+def rf_input(x, y, t, lam, w0, E_peak, fwhm, phase=0.0):
+    """Real carrier field E(x, y, t) = E_peak exp(-r^2/w0^2) exp(-2 ln2 t^2/fwhm^2) cos(w t + phase)."""
+    X, Y = np.meshgrid(x, y, indexing='ij')
+    w = 2 * np.pi * 299792458.0 / lam
+    env = np.exp(-2 * np.log(2) * t ** 2 / fwhm ** 2) * np.cos(w * t + phase)
+    return (E_peak * np.exp(-(X ** 2 + Y ** 2) / w0 ** 2)[:, :, None] * env[None, None, :])
+
+
+def make_realfield():
+    sys.path.insert(0, REF_RF)
+    med = load(os.path.join(REF_RF, 'media_physics.py'), 'rf_media_physics')
+    sol = load(os.path.join(REF_RF, 'solver_3d.py'), 'rf_solver_3d')
+    lam = 800e-9
+    x = np.linspace(-0.4e-3, 0.4e-3, 16)
+    t = np.linspace(-60e-15, 60e-15, 256)
+    # the reference's solver runs in single precision only (its density kernel reads
+    # the field as float32); tol 1e-3: at 1e-4 its error estimate plateaus near 1e-4
+    # in float32 and the step size collapses
+    cases = [('argon', lambda: med.Argon(lam, 1.0, 'single'), 4e10, 3e-4, 1e-3),
+             ('silica', lambda: med.FusedSilica(lam, 'single'), 8e9, 2e-5, 1e-3),
+             ('xenon', lambda: med.Xenon(lam, 2.0, 'single'), 2e10, 2e-4, 1e-3)]
+    for name, mk, Ep, L, tol in cases:
+        m = mk()
+        s = sol.ERK43_RealField_UPPE_3D(x, x, t, m, precision='single')
+        E0 = rf_input(x, x, t, lam, 0.2e-3, Ep, 20e-15).astype(np.float32)
+        rec = []
+        log_attempts(s, 'erk43_step', rec, 1)
+        z, freq, Ew = s.propagate(E0, L, tol=tol, max_step=L / 4, min_step=1e-9)
+        # one attempt from the input with a fixed h (unit vector) and the medium's response
+        s.E_scale = float(np.max(np.abs(E0)))
+        E1, err1 = s.erk43_step(E0 / np.float32(s.E_scale), L / 8, tol)
+        P, J = m.calc_nonlinear_response(E0, float(t[1] - t[0]))
+        save(f'refrf_{name}', x=x, t=t, E0=E0, L=L, tol=tol, z=z, freq=freq, Ew=Ew,
+             attempts=np.array(rec[:-1]), step_h=L / 8, step_E=E1, step_err=err1, P=P, J=J,
+             lut_x=m.log10_I_cpu, lut_W=np.asarray(m.W_gpu))
+    sys.path.remove(REF_RF)
+
+
+# ---------------------------------------------------------------------------
 # 3D fixtures
 # ---------------------------------------------------------------------------
 def mpi_lut(log10_I, W0=3e9, I0=5e16, K=8):
@@ -369,5 +450,7 @@ if __name__ == '__main__':
     print('1D fixtures from', REF_1D)
     make_1d()
     make_spectrum()
+    print('real-field fixtures from', REF_RF)
+    make_realfield()
     print('3D fixtures from', REF_3D)
     make_3d()

@@ -129,3 +129,21 @@ def test_pulse_from_spectrum_oracle_matches_reference():
         A = pulse_from_spectrum(g['t'], w, i, float(g['E']), float(g['gdd'][k]), float(g['tod'][k]),
                                 bool(g['jac'][k]), str(g['kinds'][k]))
         assert rel_l2(A, g[f'A{k}']) < 1e-13
+
+
+@pytest.mark.parametrize('name', ['argon', 'silica', 'xenon'])
+def test_realfield_oracle_matches_reference(name):
+    """Real-field solver (src/3+1D-UPPE-ERK4(3)IP-real-field) run here: PPT table,
+    density + Drude current response, one step, and the adaptive run."""
+    from oracle import realfield as rf
+    g = golden(f'refrf_{name}')
+    m = {'argon': lambda: rf.argon(800e-9, 1.0), 'silica': lambda: rf.fused_silica(800e-9),
+         'xenon': lambda: rf.xenon(800e-9, 2.0)}[name]()
+    assert np.array_equal(m.W_gpu, g['lut_W'])
+    P, J = m.response(g['E0'], float(g['t'][1] - g['t'][0]))
+    assert np.array_equal(P, g['P']) and np.array_equal(J, g['J'])
+    s = rf.Solver(g['x'], g['x'], g['t'], m)
+    z, f, Ew, log = s.propagate(g['E0'], float(g['L']), tol=float(g['tol']), max_step=float(g['L']) / 4,
+                                min_step=1e-9)
+    assert np.allclose(np.array(log), g['attempts'], rtol=1e-6, atol=0)
+    assert rel_l2(Ew, g['Ew']) < 1e-6
