@@ -216,6 +216,46 @@ typedef struct {
 int uppe1d_run_programs(uppe1d_plan* plan, int nprog, const long long* op_begin, const uppe1d_op* ops,
                         void* fields, void* records, uppe1d_result* op_results, uppe_stream_t stream);
 
+/* ---- real-field 3+1D solver (src/3+1D-UPPE-ERK4(3)IP-real-field/solver_3d.py) ---- */
+typedef struct {
+  int Nx, Ny, Nt;          /* powers of two: Nx, Ny in [16, 512], Nt in [64, 2048]      */
+  int precision;           /* UPPE_C64 (float32 fields) or UPPE_C128                    */
+  double dt;
+  const double* kk;        /* [Nt/2+1] k(omega)^2, omega = 2 pi rfftfreq (solver_3d.py:56-71) */
+  const double* kref;      /* [Nt/2+1] k1 omega (:73-83)                               */
+  const double* w;         /* [Nt/2+1] omega                                           */
+  const double* filt;      /* [Nt/2+1] anti-alias filter (:50-52)                      */
+  const double* kperp2;    /* [Nx*Ny] kx^2+ky^2, index ix*Ny+iy                        */
+  const double* damp;      /* [Nx*Ny] absorber (:99-110)                               */
+  int lut_n;               /* PPT rate table over log10(I [W/m^2]) (media_physics.py:167-183) */
+  const double* lut_log10I;
+  const double* lut_W;
+  double I_coef;           /* 0.5 eps0 c n0: I_equiv = I_coef E^2 (:266)               */
+  double aval_coef;        /* W_ava = aval_coef I_equiv (0 for the gases)              */
+  double chi3e, chi5e;     /* eps0 chi3, eps0 chi5: P = chi3e E^3 + chi5e E^5 (:300-312) */
+  double rate_rec, rho_nt, Ui, e_charge, m_e, tau_c;   /* density / Drude constants (:11-118) */
+} uppe_rf_desc;
+
+typedef struct uppe_rf_plan uppe_rf_plan;
+/* Replaces ERK43_RealField_UPPE_3D.__init__: uploads the tables, allocates the
+ * spectral fields (rows of Nt/2 + 16 bins) and the two real state buffers. */
+int uppe_rf_plan_create(const uppe_rf_desc* desc, uppe_rf_plan** plan);
+int uppe_rf_plan_destroy(uppe_rf_plan* plan);
+/* Start of propagate (:177-185): E_scale = max|E0|, state = E0 / E_scale.  E0: device
+ * real field [Nx][Ny][Nt] in the plan's precision; E_scale (host, may be NULL) out. */
+int uppe_rf_set_field(uppe_rf_plan* plan, const void* E0, double* E_scale, uppe_stream_t stream);
+/* One erk43_step (:113-175) of size h from the accepted state into the candidate;
+ * err = max|E4 - E_low| / max|E4| (synchronises the stream). */
+int uppe_rf_attempt(uppe_rf_plan* plan, double h, double* err, uppe_stream_t stream);
+/* Accept (state <- candidate) or reject the last attempt. */
+int uppe_rf_commit(uppe_rf_plan* plan, int accept, uppe_stream_t stream);
+/* Physical field E * E_scale of the state (device real [Nx][Ny][Nt]). */
+int uppe_rf_get_field(uppe_rf_plan* plan, void* out, uppe_stream_t stream);
+/* rfft_t(E * E_scale) (:226-233) into out (device complex [Nx][Ny][uppe_rf_spec_bins]);
+ * bins >= Nt/2 + 1 are zero.  Uses the candidate buffer as scratch. */
+int uppe_rf_get_spectrum(uppe_rf_plan* plan, void* out, uppe_stream_t stream);
+int uppe_rf_spec_bins(const uppe_rf_plan* plan);
+
 /* Spectral amplitude of an input pulse from a measured spectrum (the per-sample part
  * of generate_pulse_from_spectrum, erk43ip_method.py:599-764, FFT path): S(f) is the
  * piecewise cubic coef[4j..4j+3] (power form in f - breaks[j], highest first) on

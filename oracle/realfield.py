@@ -267,6 +267,8 @@ class Solver:
                         break
                 En, err = self.step(E, h)
                 log.append((h, err))
+                if not np.isfinite(err):   # the reference would loop forever on NaN
+                    break
                 if err < tol or h <= min_step * 1.01:
                     fail = fail + 1 if (h <= min_step * 1.01 and err > tol) else 0
                     z += h

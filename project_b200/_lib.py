@@ -56,6 +56,14 @@ class Result1D(ctypes.Structure):
 STATUS_HIST_FULL = 8
 
 
+class DescRF(ctypes.Structure):
+    _fields_ = [('Nx', _I), ('Ny', _I), ('Nt', _I), ('precision', _I), ('dt', _D),
+                ('kk', _P), ('kref', _P), ('w', _P), ('filt', _P), ('kperp2', _P), ('damp', _P),
+                ('lut_n', _I), ('lut_log10I', _P), ('lut_W', _P), ('I_coef', _D), ('aval_coef', _D),
+                ('chi3e', _D), ('chi5e', _D), ('rate_rec', _D), ('rho_nt', _D), ('Ui', _D),
+                ('e_charge', _D), ('m_e', _D), ('tau_c', _D)]
+
+
 class Op1D(ctypes.Structure):
     _fields_ = [('inst', _I), ('record', _I), ('amp', _D), ('gdd', _D), ('tod', _D)]
 
@@ -88,6 +96,14 @@ SIGNATURES = {
     'uppe1d_propagate_logged': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe1d_propagate_schedule': (_I, [_P, _P, _P, _I, ctypes.POINTER(Result1D), _P]),
     'uppe3d_mirror': (_I, [_P, _P, _D, _D, _D, _D, _P]),
+    'uppe_rf_plan_create': (_I, [ctypes.POINTER(DescRF), ctypes.POINTER(_P)]),
+    'uppe_rf_plan_destroy': (_I, [_P]),
+    'uppe_rf_set_field': (_I, [_P, _P, ctypes.POINTER(_D), _P]),
+    'uppe_rf_attempt': (_I, [_P, _D, ctypes.POINTER(_D), _P]),
+    'uppe_rf_commit': (_I, [_P, _I, _P]),
+    'uppe_rf_get_field': (_I, [_P, _P, _P]),
+    'uppe_rf_get_spectrum': (_I, [_P, _P, _P]),
+    'uppe_rf_spec_bins': (_I, [_P]),
     'uppe_spectrum_field': (_I, [_P, _P, _I, _I, _D, _D, _D, _D, _P, _P]),
     'uppe3d_beam_diag_elems': (_LL, [_P]),
     'uppe3d_beam_diagnostics': (_I, [_P, _P, _P, _P]),

@@ -2740,3 +2740,537 @@ extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nstep
   return p->dbl ? adjoint_impl<double>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s)
                 : adjoint_impl<float>(p, hlog_host, nsteps, K, A0, Zbar, A0bar, work, s);
 }
+
+// ===========================================================================
+// Real-field 3+1D ERK4(3)-IP UPPE (src/3+1D-UPPE-ERK4(3)IP-real-field/
+// solver_3d.py, media_physics.py).  The accepted state is the real field
+// E(x, y, t) / E_scale; spectra live in (kx, ky, omega >= 0) with Nt/2 + 1 bins
+// stored in rows of Nw = Nt/2 + kW (the pad bins stay zero), so the plain x and
+// y transform passes of the envelope solver serve them.  t-line kernels (one
+// warp per (x, y) line, complex FFT in shared memory): real -> half spectrum,
+// the nonlinear response (half spectrum -> real E via the Hermitian extension,
+// PPT rate table, density + Drude current scan, Kerr + chi5 polarisation,
+// separate transforms of P and J, source coefficients P_c, J_c), and the
+// output (filter, inverse transform, absorber).  Stage algebra: one spectral
+// kernel with exp(s D) computed per element in FP64.
+// ===========================================================================
+
+namespace uppe {
+struct RfConst {
+  double I_coef, aval, chi3e, chi5e;           // I = I_coef E^2; W_ava = aval I; P = chi3e E^3 + chi5e E^5
+  double rr, dt, rho_nt, Ui, e2m, nu, exp_nu, step_J;   // density / Drude constants (float32-rounded inputs)
+  double E_scale;
+};
+
+struct RfTables {
+  const double* kk;      // k(omega)^2 [Nr]
+  const double* kref;    // k1 omega [Nr]
+  const double* w;       // omega [Nr]
+  const double* filt;    // [Nr]
+  const double* kp2;     // k_perp^2 [Nx*Ny]
+  const double* damp;    // [Nx*Ny]
+  Lut lut;
+};
+
+enum RfLine { RF_FROM_T = 0, RF_NL = 1, RF_OUT = 2 };
+
+// one t-line per warp; S: line buffer (PAD complex), R: real samples (NT)
+template <typename Rl, int NT, int WPB>
+__global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw,
+                                                    const void* in, void* out, const void* twt, double in_scale,
+                                                    double h) {
+  using C = typename CT<Rl>::T;
+  constexpr int PAD = TCfg<NT>::PAD;
+  constexpr int NR = NT / 2 + 1;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  C* S = tw + NT + warp * 2 * PAD;
+  Rl* R = reinterpret_cast<Rl*>(S + PAD);
+  for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(twt)[i];
+  __syncthreads();
+  const long long line = (long long)blockIdx.x * WPB + warp;
+  if (line >= (long long)g.Nx * g.Ny) return;
+  if (mode == RF_FROM_T) {   // real E_t -> bins 0..NT/2
+    const Rl* e = reinterpret_cast<const Rl*>(in) + line * NT;
+    for (int t = lane; t < NT; t += 32) S[tpad(t)] = C{e[t], (Rl)0};
+    __syncwarp();
+    stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());
+    C* o = reinterpret_cast<C*>(out) + line * Nw;
+    for (int k = lane; k < Nw; k += 32) o[k] = k < NR ? S[tpad(k)] : C{0, 0};
+    return;
+  }
+  // half spectrum (after the unnormalised inverse x, y transforms) -> Hermitian line
+  const C* src = reinterpret_cast<const C*>(in) + line * Nw;
+  const Rl sc = (Rl)in_scale;
+  for (int k = lane; k < NR; k += 32) {
+    C v = cscale(src[k], sc);
+    if (mode == RF_OUT) v = cscale(v, (Rl)tb.filt[k]);
+    // irfft takes the real parts of the DC and Nyquist bins
+    if (k == 0 || k == NT / 2) v.y = (Rl)0;
+    S[tpad(k)] = v;
+    if (k > 0 && k < NT / 2) S[tpad(NT - k)] = C{v.x, -v.y};
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(S, tw, lane, LineIdx(), WarpSync());
+  const Rl invN = (Rl)(1.0 / NT);
+  if (mode == RF_OUT) {
+    const double dp = tb.damp[line];
+    const Rl ab = dp == 0.0 ? (Rl)1 : (Rl)exp(-dp * h);
+    Rl* o = reinterpret_cast<Rl*>(out) + line * NT;
+    for (int t = lane; t < NT; t += 32) o[t] = (S[tpad(t)].x * invN) * ab;
+    return;
+  }
+  // ---- nonlinear response (media_physics.py:258-318 with the kernel :11-118) ----
+  const Rl Es = (Rl)rc.E_scale;
+  for (int t = lane; t < NT; t += 32) R[t] = (S[tpad(t)].x * invN) * Es;   // physical field
+  __syncwarp();
+  if (lane == 0) {   // density and Drude current, serial in t as the reference kernel
+    double rho = 0.0, Jf = 0.0;
+    const Rl Ic = (Rl)rc.I_coef, Av = (Rl)rc.aval;
+    for (int t = 0; t < NT; ++t) {
+      const Rl Ef = R[t];
+      const Rl I = Ic * (Ef * Ef);
+      const double E = (double)(float)Ef;
+      const double wp = (double)(float)lut_eval<Rl>(tb.lut, I);
+      const double wa = (double)(float)(Av * I);
+      double dep = (rc.rho_nt - rho) / rc.rho_nt;
+      if (dep < 0.0) dep = 0.0;
+      const double Se = wp * rc.rho_nt * dep;
+      const double Ge = wa * dep - rc.rr;
+      double gdt = Ge * rc.dt;
+      if (gdt > 10.0) gdt = 10.0;
+      if (gdt < -10.0) gdt = -10.0;
+      const double eg = exp(gdt);
+      const double sf = (fabs(gdt) < 1e-5) ? rc.dt * (1.0 + 0.5 * gdt) : (eg - 1.0) / Ge;
+      double nr = rho * eg + Se * sf;
+      if (nr > rc.rho_nt) nr = rc.rho_nt;
+      if (nr < 0.0) nr = 0.0;
+      const double gen = Se + wa * dep * rho;
+      const double nJ = Jf * rc.exp_nu + rc.e2m * rho * E * rc.step_J;
+      const double Jl = fabs(E) > 1e-10 ? (gen * rc.Ui * E) / (E * E + 1e-20) : 0.0;
+      S[tpad(t)].y = (Rl)(Jf + Jl) / Es;       // J (solver precision) / E_scale
+      rho = nr;
+      Jf = nJ;
+    }
+  }
+  __syncwarp();
+  const Rl c3 = (Rl)rc.chi3e, c5 = (Rl)rc.chi5e;
+  for (int t = lane; t < NT; t += 32) {
+    const Rl E = R[t];
+    Rl P = ((c3 * E) * E) * E;
+    if (rc.chi5e != 0.0) {
+      const Rl E2 = E * E;
+      P = P + ((c5 * E) * E2) * E2;
+    }
+    S[tpad(t)].x = P / Es;
+  }
+  __syncwarp();
+  // P and J are transformed separately: the polarisation can be many orders below
+  // the current, and a packed transform would bury its spectrum in J's rounding
+  C* S2 = reinterpret_cast<C*>(R);   // the field samples are no longer needed
+  for (int t = lane; t < NT; t += 32) {
+    const C pj = S[tpad(t)];
+    S[tpad(t)] = C{pj.x, (Rl)0};
+    S2[tpad(t)] = C{pj.y, (Rl)0};
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());    // F(P)
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S2, tw, lane, LineIdx(), WarpSync());   // F(J)
+  C* o = reinterpret_cast<C*>(out) + line * Nw;
+  const double kp2 = tb.kp2[line];
+  const double cpl = 1.0 / (2.0 * 8.85418781e-12 * 299792458.0 * 299792458.0);
+  for (int k = lane; k < Nw; k += 32) {
+    if (k == 0 || k >= NR) { o[k] = C{0, 0}; continue; }   // DC source zeroed (solver_3d.py:95-97)
+    const C zp = S[tpad(k)], zj = S2[tpad(k)];
+    const double Pr = zp.x, Pi = zp.y, Jr = zj.x, Ji = zj.y;
+    // kz: real root, or -i sqrt(|.|) for evanescent components; |kz| < 1e-10 -> 1e-10
+    const double kz2 = tb.kk[k] - kp2;
+    double kr, ki;
+    if (kz2 >= 0.0) { kr = sqrt(kz2); ki = 0.0; } else { kr = 0.0; ki = -sqrt(-kz2); }
+    if (sqrt(kr * kr + ki * ki) < 1e-10) { kr = 1e-10; ki = 0.0; }
+    const double w = tb.w[k];
+    const double den = kr * kr + ki * ki;
+    const double ir = kr / den, ii = -ki / den;            // 1 / kz
+    // Pc = -i w^2 cpl / kz ; Jc = -w cpl / kz
+    const double pr = w * w * cpl * ii, pim = -w * w * cpl * ir;
+    const double jr = -w * cpl * ir, ji = -w * cpl * ii;
+    o[k] = C{(Rl)(pr * Pr - pim * Pi + jr * Jr - ji * Ji), (Rl)(pr * Pi + pim * Pr + jr * Ji + ji * Jr)};
+  }
+}
+
+enum RfStage { RS_1 = 0, RS_2, RS_3, RS_4 };
+
+struct RfBufs {
+  void *ekw, *v, *a1, *u, *ts, *el, *na, *e4;
+};
+
+// stage algebra of erk43_step (solver_3d.py:143-167) in (kx, ky, omega)
+template <typename Rl>
+__global__ void k_rf_stage(int mode, RfTables tb, RfBufs b, int Nt, int Nw, long long n, double h,
+                           unsigned long long* red) {
+  using C = typename CT<Rl>::T;
+  const int NR = Nt / 2 + 1;
+  C *ekw = (C*)b.ekw, *v = (C*)b.v, *a1 = (C*)b.a1, *u = (C*)b.u, *ts = (C*)b.ts, *el = (C*)b.el,
+    *na = (C*)b.na, *e4 = (C*)b.e4;
+  const Rl h2 = (Rl)(h / 2), h6 = (Rl)(h / 6), hR = (Rl)h;
+  double mdiff = 0.0, mnorm = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const int k = (int)(i % Nw);
+    if (k >= NR) continue;
+    // exp((h/2) D), D = -i (kz - kref)
+    const double kz2 = tb.kk[k] - tb.kp2[i / Nw];
+    const double s = 0.5 * h;
+    double mag = 1.0, ph;
+    if (kz2 >= 0.0) ph = -(sqrt(kz2) - tb.kref[k]) * s;
+    else { mag = exp(-sqrt(-kz2) * s); ph = tb.kref[k] * s; }
+    double sn, cs;
+    sincos(ph, &sn, &cs);
+    const C E = C{(Rl)(mag * cs), (Rl)(mag * sn)};
+    if (mode == RS_1) {          // v = L(E_kw), a1 = L(k1), u = v + h/2 a1
+      const C vv = cmul(ekw[i], E), aa = cmul(na[i], E);
+      v[i] = vv;
+      a1[i] = aa;
+      u[i] = cadd(vv, cscale(aa, h2));
+    } else if (mode == RS_2) {   // u = v + h/2 a2, ts = a1 + 2 a2, el = v + h/2 a1 + h/2 a2
+      const C a2 = na[i], vv = v[i], aa = a1[i];
+      u[i] = cadd(vv, cscale(a2, h2));
+      ts[i] = cadd(aa, cscale(a2, (Rl)2));
+      el[i] = cadd(cadd(vv, cscale(aa, h2)), cscale(a2, h2));
+    } else if (mode == RS_3) {   // u = L(v + h a3), ts += 2 a3
+      const C a3 = na[i];
+      u[i] = cmul(cadd(v[i], cscale(a3, hR)), E);
+      ts[i] = cadd(ts[i], cscale(a3, (Rl)2));
+    } else {                     // E4 = L(v + h/6 ts) + h/6 a4; E_low = L(el)
+      const C E4 = cadd(cmul(cadd(v[i], cscale(ts[i], h6)), E), cscale(na[i], h6));
+      const C El = cmul(el[i], E);
+      e4[i] = E4;
+      const double dx = (double)E4.x - El.x, dy = (double)E4.y - El.y;
+      const double d = sqrt(dx * dx + dy * dy), m = sqrt((double)E4.x * E4.x + (double)E4.y * E4.y);
+      mdiff = (d > mdiff || d != d) ? d : mdiff;
+      mnorm = (m > mnorm || m != m) ? m : mnorm;
+    }
+  }
+  if (mode == RS_4) {
+    mdiff = warp_max<32>(mdiff);
+    mnorm = warp_max<32>(mnorm);
+    if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(&red[0], mdiff); atomic_max_nonneg(&red[1], mnorm); }
+  }
+}
+
+template <typename Rl>
+__global__ void k_rf_absmax(const Rl* e, long long n, unsigned long long* red) {
+  double m = 0.0;
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    const double a = fabs((double)e[i]);
+    m = a > m ? a : m;
+  }
+  m = warp_max<32>(m);
+  if ((threadIdx.x & 31) == 0) atomic_max_nonneg(red, m);
+}
+
+// float32 field arithmetic as the reference does it: E0 / float32(E_scale) and
+// E * float32(E_scale)
+__global__ void k_rf_div_f32(const float* in, float* out, long long n, float s) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i] / s;
+}
+__global__ void k_rf_mul_f32(const float* in, float* out, long long n, float s) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = in[i] * s;
+}
+
+template <typename Rl>
+__global__ void k_rf_scale(const Rl* in, Rl* out, long long n, double s) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+    out[i] = (Rl)((double)in[i] * s);
+}
+}  // namespace uppe
+
+struct uppe_rf_plan {
+  uppe_rf_desc d;
+  int dbl, Nw;
+  size_t csz, rsz;
+  long long nspec, nreal;
+  uppe3d_plan* xy;        // transform plan of the x and y passes (omega extent Nw)
+  RfTables tb;
+  RfConst rc;
+  RfBufs b;
+  void* state[2];         // accepted / candidate real field (normalised)
+  void* tmp[2];           // spectral temporaries
+  unsigned long long* red;
+  unsigned long long* red_host;
+  const void* twt;
+  std::vector<void*> allocs;
+  int cur = 0;
+  double h_last = 0.0;
+};
+
+static int rf_alloc(uppe_rf_plan* p, void** dst, size_t bytes, const void* src = nullptr) {
+  UPPE_CK(cudaMalloc(dst, bytes));
+  p->allocs.push_back(*dst);
+  if (src) UPPE_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+  else UPPE_CK(cudaMemset(*dst, 0, bytes));
+  return 0;
+}
+
+extern "C" int uppe_rf_plan_destroy(uppe_rf_plan* p) {
+  if (!p) return 0;
+  if (p->xy) uppe3d_plan_destroy(p->xy);
+  for (void* a : p->allocs) cudaFree(a);
+  if (p->red_host) cudaFreeHost(p->red_host);
+  delete p;
+  return 0;
+}
+
+template <typename Rl> static int rf_set_attrs(int Nx, int Ny, int Nt) {
+  cudaError_t e = cudaSuccess;
+  for (int N : {Nx, Ny}) {
+    switch (N) {
+      case 16: e = set_space_attr<Rl, 16>(); break;
+      case 32: e = set_space_attr<Rl, 32>(); break;
+      case 64: e = set_space_attr<Rl, 64>(); break;
+      case 128: e = set_space_attr<Rl, 128>(); break;
+      case 256: e = set_space_attr<Rl, 256>(); break;
+      case 512: e = set_space_attr<Rl, 512>(); break;
+      default: return UPPE_ERR_SIZE;
+    }
+    if (e != cudaSuccess) break;
+  }
+  UPPE_CK(e);
+  (void)Nt;
+  return 0;
+}
+
+extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
+  *out = nullptr;
+  g_uppe_err[0] = 0;
+  if (!d) return UPPE_ERR_ARG;
+  if (!is_pow2(d->Nx) || !is_pow2(d->Ny) || !is_pow2(d->Nt) || d->Nx < 16 || d->Ny < 16 || d->Nx > 512 ||
+      d->Ny > 512 || d->Nt < 64 || d->Nt > 2048) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err), "unsupported real-field grid %dx%dx%d", d->Nx, d->Ny, d->Nt);
+    return UPPE_ERR_SIZE;
+  }
+  if (d->precision != UPPE_C64 && d->precision != UPPE_C128) return UPPE_ERR_ARG;
+  if (d->precision == UPPE_C128 && (d->Nx > 256 || d->Ny > 256)) return UPPE_ERR_SIZE;
+  if (d->lut_n < 2 || !d->lut_log10I || !d->lut_W || !d->kk || !d->kref || !d->w || !d->filt || !d->kperp2 ||
+      !d->damp)
+    return UPPE_ERR_ARG;
+  uppe_rf_plan* p = new uppe_rf_plan();
+  p->d = *d;
+  p->dbl = d->precision == UPPE_C128;
+  p->csz = p->dbl ? 16 : 8;
+  p->rsz = p->dbl ? 8 : 4;
+  p->Nw = d->Nt / 2 + kW;
+  const int Nr = d->Nt / 2 + 1;
+  p->nspec = (long long)d->Nx * d->Ny * p->Nw;
+  p->nreal = (long long)d->Nx * d->Ny * d->Nt;
+  int rc = 0;
+#define RF_TRY(x) do { rc = (x); if (rc) { uppe_rf_plan_destroy(p); return rc; } } while (0)
+  // transform plan: geometry (Nx, Ny, Nw), twiddles, a device state that is never "done"
+  {
+    uppe3d_plan* q = new uppe3d_plan();
+    p->xy = q;
+    q->g.Nx = d->Nx; q->g.Ny = d->Ny; q->g.Nt = p->Nw;
+    q->g.npts = p->nspec;
+    q->dbl = p->dbl;
+    q->csz = p->csz;
+    cudaError_t e = cudaMalloc(&q->st, sizeof(State3D));
+    if (e != cudaSuccess) { uppe_rf_plan_destroy(p); return UPPE_ERR_CUDA; }
+    q->allocs.push_back(q->st);
+    e = cudaMallocHost(&q->st_host, sizeof(State3D));
+    if (e != cudaSuccess) { uppe_rf_plan_destroy(p); return UPPE_ERR_CUDA; }
+    memset(q->st_host, 0, sizeof(State3D));
+    e = cudaMemcpy(q->st, q->st_host, sizeof(State3D), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) { uppe_rf_plan_destroy(p); return UPPE_ERR_CUDA; }
+    void* ptr = nullptr;
+    auto tx = p->dbl ? twiddles<double>(d->Nx) : twiddles<float>(d->Nx);
+    auto ty = p->dbl ? twiddles<double>(d->Ny) : twiddles<float>(d->Ny);
+    auto tt = p->dbl ? twiddles<double>(d->Nt) : twiddles<float>(d->Nt);
+    RF_TRY(dev_upload(q, &ptr, tx.data(), tx.size())); q->tb.twx = ptr;
+    RF_TRY(dev_upload(q, &ptr, ty.data(), ty.size())); q->tb.twy = ptr;
+    RF_TRY(dev_upload(q, &ptr, tt.data(), tt.size())); p->twt = ptr;
+    RF_TRY(p->dbl ? rf_set_attrs<double>(d->Nx, d->Ny, d->Nt) : rf_set_attrs<float>(d->Nx, d->Ny, d->Nt));
+  }
+  void* ptr = nullptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * Nr, d->kk)); p->tb.kk = (const double*)ptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * Nr, d->kref)); p->tb.kref = (const double*)ptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * Nr, d->w)); p->tb.w = (const double*)ptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * Nr, d->filt)); p->tb.filt = (const double*)ptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * (size_t)d->Nx * d->Ny, d->kperp2)); p->tb.kp2 = (const double*)ptr;
+  RF_TRY(rf_alloc(p, &ptr, 8 * (size_t)d->Nx * d->Ny, d->damp)); p->tb.damp = (const double*)ptr;
+  {
+    const int n = d->lut_n;
+    std::vector<unsigned char> lx(n * p->rsz), lw(n * p->rsz);
+    for (int i = 0; i < n; ++i) {
+      if (p->dbl) { ((double*)lx.data())[i] = d->lut_log10I[i]; ((double*)lw.data())[i] = d->lut_W[i]; }
+      else { ((float*)lx.data())[i] = (float)d->lut_log10I[i]; ((float*)lw.data())[i] = (float)d->lut_W[i]; }
+    }
+    RF_TRY(rf_alloc(p, &ptr, lx.size(), lx.data())); p->tb.lut.x = ptr;
+    RF_TRY(rf_alloc(p, &ptr, lw.size(), lw.data())); p->tb.lut.w = ptr;
+    p->tb.lut.n = n;
+    const double x0 = p->dbl ? d->lut_log10I[0] : (double)(float)d->lut_log10I[0];
+    const double x1 = p->dbl ? d->lut_log10I[n - 1] : (double)(float)d->lut_log10I[n - 1];
+    p->tb.lut.x0 = x0;
+    p->tb.lut.inv_dx = (n - 1) / (x1 - x0);
+    int j0 = -1;
+    for (int i = 0; i < n; ++i) {
+      const double wv = p->dbl ? d->lut_W[i] : (double)(float)d->lut_W[i];
+      if (wv != 0.0) break;
+      j0 = i;
+    }
+    p->tb.lut.zero_x = j0 < 0 ? -INFINITY : (p->dbl ? d->lut_log10I[j0] : (double)(float)d->lut_log10I[j0]);
+    if (j0 == n - 1) p->tb.lut.zero_x = INFINITY;
+    p->tb.lut.I_zero = lut_zero_intensity(p->tb.lut.zero_x);
+  }
+  RfConst& c = p->rc;
+  c.I_coef = d->I_coef; c.aval = d->aval_coef; c.chi3e = d->chi3e; c.chi5e = d->chi5e;
+  c.rr = (double)(float)d->rate_rec; c.dt = (double)(float)d->dt; c.rho_nt = (double)(float)d->rho_nt;
+  c.Ui = (double)(float)d->Ui;
+  const double e = (double)(float)d->e_charge, me = (double)(float)d->m_e, tc = (double)(float)d->tau_c;
+  c.e2m = e * e / me;
+  c.nu = 1.0 / tc;
+  const double ndt = c.nu * c.dt;
+  c.exp_nu = exp(-ndt);
+  c.step_J = (fabs(ndt) < 1e-5) ? c.dt * (1.0 - 0.5 * ndt) : (1.0 - c.exp_nu) / c.nu;
+  c.E_scale = 1.0;
+  void** spec[8] = {&p->b.ekw, &p->b.v, &p->b.a1, &p->b.u, &p->b.ts, &p->b.el, &p->b.na, &p->b.e4};
+  for (int i = 0; i < 8; ++i) RF_TRY(rf_alloc(p, spec[i], p->csz * p->nspec));
+  RF_TRY(rf_alloc(p, &p->tmp[0], p->csz * p->nspec));
+  RF_TRY(rf_alloc(p, &p->tmp[1], p->csz * p->nspec));
+  RF_TRY(rf_alloc(p, &p->state[0], p->rsz * p->nreal));
+  RF_TRY(rf_alloc(p, &p->state[1], p->rsz * p->nreal));
+  RF_TRY(rf_alloc(p, &ptr, 4 * sizeof(unsigned long long))); p->red = (unsigned long long*)ptr;
+  if (cudaMallocHost(&p->red_host, 4 * sizeof(unsigned long long)) != cudaSuccess) { uppe_rf_plan_destroy(p); return UPPE_ERR_CUDA; }
+#undef RF_TRY
+  *out = p;
+  return 0;
+}
+
+template <typename Rl, int NT>
+static int rf_line_n(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
+  constexpr int WPB = TLaunch<NT, Rl>::WPB;
+  const size_t smem = TLaunch<NT, Rl>::smem();
+  UPPE_CK(cudaFuncSetAttribute(k_rf_line<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  Geom g;
+  g.Nx = p->d.Nx; g.Ny = p->d.Ny; g.Nt = p->d.Nt; g.npts = p->nreal;
+  const long long nl = (long long)g.Nx * g.Ny;
+  k_rf_line<Rl, NT, WPB><<<(unsigned)((nl + WPB - 1) / WPB), WPB * 32, smem, s>>>(mode, p->tb, p->rc, g, p->Nw, in, out,
+                                                                                  p->twt, in_scale, h);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename Rl>
+static int rf_line(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
+  switch (p->d.Nt) {
+#define UPPE_RL(n) case n: return rf_line_n<Rl, n>(p, mode, in, out, in_scale, h, s);
+    UPPE_RL(64) UPPE_RL(128) UPPE_RL(256) UPPE_RL(512) UPPE_RL(1024) UPPE_RL(2048)
+#undef UPPE_RL
+    default: return UPPE_ERR_SIZE;
+  }
+}
+
+// N(u) of solver_3d.py:120-141: u (kx, ky, omega) -> out
+template <typename Rl>
+static int rf_N(uppe_rf_plan* p, const void* u, void* out, cudaStream_t s) {
+  uppe3d_plan* q = p->xy;
+  int rc = 0;
+  rc |= adj_plain_y<Rl>(q, YPLAIN_INV, u, p->tmp[0], 1.0, s);
+  rc |= launch_space<Rl>(q, XINV, p->tmp[0], p->tmp[1], s);
+  rc |= rf_line<Rl>(p, RF_NL, p->tmp[1], p->tmp[0], 1.0 / ((double)p->d.Nx * p->d.Ny), 0.0, s);
+  rc |= launch_space<Rl>(q, XFWD, p->tmp[0], p->tmp[1], s);
+  rc |= adj_plain_y<Rl>(q, YPLAIN_FWD, p->tmp[1], out, 1.0, s);
+  return rc;
+}
+
+template <typename Rl>
+static int rf_stage(uppe_rf_plan* p, int mode, double h, cudaStream_t s) {
+  k_rf_stage<Rl><<<148 * 8, 256, 0, s>>>(mode, p->tb, p->b, p->d.Nt, p->Nw, p->nspec, h, p->red);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+template <typename Rl>
+static int rf_attempt(uppe_rf_plan* p, double h, double* err, cudaStream_t s) {
+  uppe3d_plan* q = p->xy;
+  int rc = 0;
+  // E_kw = fft2(rfft(E_t))
+  rc |= rf_line<Rl>(p, RF_FROM_T, p->state[p->cur], p->tmp[0], 1.0, 0.0, s);
+  rc |= launch_space<Rl>(q, XFWD, p->tmp[0], p->tmp[1], s);
+  rc |= adj_plain_y<Rl>(q, YPLAIN_FWD, p->tmp[1], p->b.ekw, 1.0, s);
+  rc |= rf_N<Rl>(p, p->b.ekw, p->b.na, s);                         // k1
+  rc |= rf_stage<Rl>(p, RS_1, h, s);
+  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha2
+  rc |= rf_stage<Rl>(p, RS_2, h, s);
+  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha3
+  rc |= rf_stage<Rl>(p, RS_3, h, s);
+  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha4'
+  UPPE_CK(cudaMemsetAsync(p->red, 0, 2 * sizeof(unsigned long long), s));
+  rc |= rf_stage<Rl>(p, RS_4, h, s);
+  // candidate: irfft(ifft2(E4) * filter) * exp(-damp h)
+  rc |= adj_plain_y<Rl>(q, YPLAIN_INV, p->b.e4, p->tmp[0], 1.0, s);
+  rc |= launch_space<Rl>(q, XINV, p->tmp[0], p->tmp[1], s);
+  rc |= rf_line<Rl>(p, RF_OUT, p->tmp[1], p->state[p->cur ^ 1], 1.0 / ((double)p->d.Nx * p->d.Ny), h, s);
+  UPPE_CK(cudaMemcpyAsync(p->red_host, p->red, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  double md, mn;
+  memcpy(&md, &p->red_host[0], 8);
+  memcpy(&mn, &p->red_host[1], 8);
+  *err = md / (mn + 1e-20);
+  p->h_last = h;
+  return rc;
+}
+
+extern "C" int uppe_rf_set_field(uppe_rf_plan* p, const void* E0, double* E_scale, cudaStream_t s) {
+  if (!p || !E0) return UPPE_ERR_ARG;
+  UPPE_CK(cudaMemsetAsync(p->red, 0, sizeof(unsigned long long), s));
+  if (p->dbl) k_rf_absmax<double><<<148 * 4, 256, 0, s>>>((const double*)E0, p->nreal, p->red);
+  else k_rf_absmax<float><<<148 * 4, 256, 0, s>>>((const float*)E0, p->nreal, p->red);
+  UPPE_CK(cudaMemcpyAsync(p->red_host, p->red, sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  double m;
+  memcpy(&m, &p->red_host[0], 8);
+  if (!p->dbl) m = (double)(float)m;   // max|E0| of the float32 field, as float32 (solver_3d.py:180)
+  double sc = m < 1e-30 ? 1.0 : m;
+  p->rc.E_scale = sc;
+  p->cur = 0;
+  // E = E0 / E_scale in the field precision
+  const double inv = p->dbl ? 1.0 / sc : 1.0;
+  if (p->dbl) k_rf_scale<double><<<148 * 4, 256, 0, s>>>((const double*)E0, (double*)p->state[0], p->nreal, inv);
+  else k_rf_div_f32<<<148 * 4, 256, 0, s>>>((const float*)E0, (float*)p->state[0], p->nreal, (float)sc);
+  UPPE_CK(cudaGetLastError());
+  if (E_scale) *E_scale = sc;
+  return 0;
+}
+
+extern "C" int uppe_rf_attempt(uppe_rf_plan* p, double h, double* err, cudaStream_t s) {
+  if (!p || !err || !(h > 0.0)) return UPPE_ERR_ARG;
+  return p->dbl ? rf_attempt<double>(p, h, err, s) : rf_attempt<float>(p, h, err, s);
+}
+
+extern "C" int uppe_rf_commit(uppe_rf_plan* p, int accept, cudaStream_t s) {
+  (void)s;
+  if (!p) return UPPE_ERR_ARG;
+  if (accept) p->cur ^= 1;
+  return 0;
+}
+
+extern "C" int uppe_rf_get_field(uppe_rf_plan* p, void* out, cudaStream_t s) {
+  if (!p || !out) return UPPE_ERR_ARG;
+  if (p->dbl) k_rf_scale<double><<<148 * 4, 256, 0, s>>>((const double*)p->state[p->cur], (double*)out, p->nreal, p->rc.E_scale);
+  else k_rf_mul_f32<<<148 * 4, 256, 0, s>>>((const float*)p->state[p->cur], (float*)out, p->nreal, (float)p->rc.E_scale);
+  UPPE_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe_rf_get_spectrum(uppe_rf_plan* p, void* out, cudaStream_t s) {
+  if (!p || !out) return UPPE_ERR_ARG;
+  // rfft(E * E_scale) per line into rows of Nw bins (the candidate buffer is scratch here)
+  int rc = uppe_rf_get_field(p, p->state[p->cur ^ 1], s);
+  if (rc) return rc;
+  return p->dbl ? rf_line<double>(p, RF_FROM_T, p->state[p->cur ^ 1], out, 1.0, 0.0, s)
+                : rf_line<float>(p, RF_FROM_T, p->state[p->cur ^ 1], out, 1.0, 0.0, s);
+}
+
+extern "C" int uppe_rf_spec_bins(const uppe_rf_plan* p) { return p ? p->Nw : 0; }
