@@ -300,6 +300,59 @@ def run_gradients(dev):
     return out
 
 
+def run_realfield(dev, cpu=True):
+    """Real-field 3+1D solver (src/3+1D-UPPE-ERK4(3)IP-real-field): argon 1 atm,
+    128 x 128 x 1024 real samples over 0.8 mm x 200 fs, 800 nm 20 fs pulse at
+    4e10 V/m, single precision (the reference's); time per ERK attempt over CUDA
+    events, bytes per attempt from the pass list (74 spectral fields of
+    Nx Ny (Nt/2 + 16) complex64 plus 3 real-field passes), and the oracle's step
+    on a 32 x 32 x 1024 sample on the host."""
+    import torch
+    from project_b200.realfield import Argon, ERK43_RealField_UPPE_3D
+    N, Nt = 128, 1024
+    x = np.linspace(-0.4e-3, 0.4e-3, N)
+    t = np.linspace(-100e-15, 100e-15, Nt)
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    w = 2 * np.pi * 299792458.0 / 800e-9
+    env = np.exp(-2 * np.log(2) * t ** 2 / (20e-15) ** 2) * np.cos(w * t)
+    E0 = (4e10 * np.exp(-(X ** 2 + Y ** 2) / (0.2e-3) ** 2)[:, :, None] * env[None, None, :]).astype(np.float32)
+    sol = ERK43_RealField_UPPE_3D(x, x, t, Argon(800e-9, 1.0), precision='single', device=dev)
+    sol.set_field(torch.from_numpy(E0).to(dev))
+    h = 1e-6
+    for _ in range(3):
+        sol.attempt(h)
+    n = 10
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    e0.record()
+    for _ in range(n):
+        sol.attempt(h)
+    e1.record()
+    torch.cuda.synchronize(dev)
+    ms = e0.elapsed_time(e1) / n
+    Nw = Nt // 2 + 16
+    Fs = N * N * Nw * 8
+    Fr = N * N * Nt * 4
+    byts = 74 * Fs + 3 * Fr
+    out = {'workload': 'real-field 3+1D ERK4(3)-IP attempt, argon 1 atm, 128x128x1024, 0.8 mm x 200 fs, '
+                       '20 fs 800 nm at 4e10 V/m, PPT + Drude current, single precision',
+           'ms_per_attempt': ms, 'value': N * N * Nt / (ms / 1e3), 'unit': 'pt-steps/s',
+           'achieved_gbs': byts / (ms / 1e3) / 1e9, 'bytes_model': '74 spectral + 3 real field passes per attempt'}
+    if cpu:
+        from oracle import realfield as orf
+        xs = np.linspace(-0.4e-3, 0.4e-3, 32)
+        Xs, Ys = np.meshgrid(xs, xs, indexing='ij')
+        Es = (4e10 * np.exp(-(Xs ** 2 + Ys ** 2) / (0.2e-3) ** 2)[:, :, None] * env[None, None, :]).astype(np.float32)
+        os_ = orf.Solver(xs, xs, t, orf.argon(800e-9, 1.0), 'single')
+        os_.E_scale = float(np.abs(Es).max())
+        t0 = time.perf_counter()
+        os_.step(Es / np.float32(os_.E_scale), h)
+        dt_ = time.perf_counter() - t0
+        out['cpu_baseline'] = {'value': 32 * 32 * Nt / dt_, 'unit': 'pt-steps/s', 'cores': 1, 'kind': 'port',
+                               'sample': f'one attempt on 32x32x1024 (numpy/scipy oracle): {dt_:.2f} s'}
+    return out
+
+
 def cpu_baseline_1d():
     """Oracle port of the reference 1D solver on one config-0 instance (Nt 4096, 2 GW 30 fs,
     argon 1 bar, 1 m, tol 1e-6, with the plasma term) on the host."""
@@ -442,6 +495,12 @@ def run_b200(args, rank, world, local_rank):
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             b1d['cpu_baseline'] = cpu_baseline_1d()
 
+    rfield = None
+    if rank == 0 and not args.no_realfield:
+        try:
+            rfield = run_realfield(dev, cpu=(world == 1 and not args.no_cpu_baseline))
+        except Exception as e:   # reported, never fatal
+            rfield = {'error': str(e)[:300]}
     grads = None
     if rank == 0 and not args.no_gradients:
         try:
@@ -480,6 +539,7 @@ def run_b200(args, rank, world, local_rank):
             'plain_gpu': plain,
             'batched_1d': b1d,
             'gradients': grads,
+            'realfield_3d': rfield,
             'gpu_launches': args.steps * lib.uppe3d_launches_per_step(sol._plan),
             'clocks': clk,
         }
@@ -522,6 +582,7 @@ def main():
     ap.add_argument('--no-plain-gpu', action='store_true')
     ap.add_argument('--no-batched-1d', action='store_true')
     ap.add_argument('--no-gradients', action='store_true')
+    ap.add_argument('--no-realfield', action='store_true')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
     args = ap.parse_args()

@@ -2774,6 +2774,17 @@ struct RfTables {
 
 enum RfLine { RF_FROM_T = 0, RF_NL = 1, RF_OUT = 2 };
 
+// the reference's density update for w_av = 0: Gamma = -rr exactly, so
+// exp(Gamma dt) and the step factor are the constants e_r and sf0
+__device__ __forceinline__ void rf_rho_step(double& rho, double wp, const RfConst& rc, double e_r, double sf0) {
+  double dep = (rc.rho_nt - rho) / rc.rho_nt;
+  if (dep < 0.0) dep = 0.0;
+  double r = rho * e_r + wp * rc.rho_nt * dep * sf0;
+  if (r > rc.rho_nt) r = rc.rho_nt;
+  if (r < 0.0) r = 0.0;
+  rho = r;
+}
+
 // one t-line per warp; S: line buffer (PAD complex), R: real samples (NT)
 template <typename Rl, int NT, int WPB>
 __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw,
@@ -2825,34 +2836,109 @@ __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfC
   const Rl Es = (Rl)rc.E_scale;
   for (int t = lane; t < NT; t += 32) R[t] = (S[tpad(t)].x * invN) * Es;   // physical field
   __syncwarp();
-  if (lane == 0) {   // density and Drude current, serial in t as the reference kernel
-    double rho = 0.0, Jf = 0.0;
+  // density and Drude current (media_physics.py:11-118).  Without avalanche and
+  // while no clamp binds the density update is affine in rho, and the free
+  // current J' = J exp(-nu dt) + (e^2/m) rho E step_J always is: chunks of E
+  // samples per lane, warp scans of the chunk maps, then each lane walks its
+  // chunk.  Otherwise lane 0 runs the reference's serial loop.
+  {
+    constexpr int EC = NT / 32;
+    const int t0 = lane * EC;
     const Rl Ic = (Rl)rc.I_coef, Av = (Rl)rc.aval;
-    for (int t = 0; t < NT; ++t) {
-      const Rl Ef = R[t];
-      const Rl I = Ic * (Ef * Ef);
-      const double E = (double)(float)Ef;
-      const double wp = (double)(float)lut_eval<Rl>(tb.lut, I);
-      const double wa = (double)(float)(Av * I);
-      double dep = (rc.rho_nt - rho) / rc.rho_nt;
-      if (dep < 0.0) dep = 0.0;
-      const double Se = wp * rc.rho_nt * dep;
-      const double Ge = wa * dep - rc.rr;
-      double gdt = Ge * rc.dt;
-      if (gdt > 10.0) gdt = 10.0;
-      if (gdt < -10.0) gdt = -10.0;
-      const double eg = exp(gdt);
-      const double sf = (fabs(gdt) < 1e-5) ? rc.dt * (1.0 + 0.5 * gdt) : (eg - 1.0) / Ge;
-      double nr = rho * eg + Se * sf;
-      if (nr > rc.rho_nt) nr = rc.rho_nt;
-      if (nr < 0.0) nr = 0.0;
-      const double gen = Se + wa * dep * rho;
-      const double nJ = Jf * rc.exp_nu + rc.e2m * rho * E * rc.step_J;
-      const double Jl = fabs(E) > 1e-10 ? (gen * rc.Ui * E) / (E * E + 1e-20) : 0.0;
-      S[tpad(t)].y = (Rl)(Jf + Jl) / Es;       // J (solver precision) / E_scale
-      rho = nr;
-      Jf = nJ;
+    const double e_r = exp(fmin(fmax(-rc.rr * rc.dt, -10.0), 10.0));   // exp(gdt) with w_av = 0
+    const double g0 = fmin(fmax(-rc.rr * rc.dt, -10.0), 10.0);
+    const double sf0 = (fabs(g0) < 1e-5) ? rc.dt * (1.0 + 0.5 * g0) : (e_r - 1.0) / (-rc.rr);
+    bool ok = rc.aval == 0.0;
+    double cm = 1.0, dm = 0.0;
+    for (int i = 0; i < EC; ++i) {
+      const Rl Ef = R[t0 + i];
+      const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+      const double c = e_r - wp * sf0;
+      ok &= (c >= 0.0);
+      dm = c * dm + wp * rc.rho_nt * sf0;
+      cm = c * cm;
     }
+    // no clamp binds if every chunk map keeps rho in [0, rho_nt] (c >= 0 and the
+    // composed value stays below rho_nt; checked on the scan result below)
+    if (__all_sync(0xffffffffu, ok)) {
+      double c = cm, d = dm;
+#pragma unroll
+      for (int off = 1; off < 32; off <<= 1) {
+        const double cp = __shfl_up_sync(0xffffffffu, c, off);
+        const double dp = __shfl_up_sync(0xffffffffu, d, off);
+        if (lane >= off) { d = c * dp + d; c = c * cp; }
+      }
+      const double ex = __shfl_up_sync(0xffffffffu, d, 1);
+      const double rho0 = lane == 0 ? 0.0 : ex;
+      const double rho_end = __shfl_sync(0xffffffffu, d, 31);
+      ok = rho_end <= rc.rho_nt;
+      if (__all_sync(0xffffffffu, ok)) {
+        // free-current chunk map: J_end = aJ J_start + bJ
+        double rho = rho0, aJ = 1.0, bJ = 0.0;
+        for (int i = 0; i < EC; ++i) {
+          const Rl Ef = R[t0 + i];
+          const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+          const double dJ = rc.e2m * rho * (double)(float)Ef * rc.step_J;
+          bJ = bJ * rc.exp_nu + dJ;
+          aJ = aJ * rc.exp_nu;
+          rf_rho_step(rho, wp, rc, e_r, sf0);
+        }
+        double a = aJ, b = bJ;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+          const double ap = __shfl_up_sync(0xffffffffu, a, off);
+          const double bp = __shfl_up_sync(0xffffffffu, b, off);
+          if (lane >= off) { b = a * bp + b; a = a * ap; }
+        }
+        const double exJ = __shfl_up_sync(0xffffffffu, b, 1);
+        double Jf = lane == 0 ? 0.0 : exJ;
+        rho = rho0;
+        for (int i = 0; i < EC; ++i) {
+          const int t = t0 + i;
+          const Rl Ef = R[t];
+          const double E = (double)(float)Ef;
+          const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+          double dep = (rc.rho_nt - rho) / rc.rho_nt;
+          if (dep < 0.0) dep = 0.0;
+          const double gen = wp * rc.rho_nt * dep;            // w_av = 0
+          const double Jl = fabs(E) > 1e-10 ? (gen * rc.Ui * E) / (E * E + 1e-20) : 0.0;
+          const double nJ = Jf * rc.exp_nu + rc.e2m * rho * E * rc.step_J;
+          S[tpad(t)].y = (Rl)(Jf + Jl) / Es;
+          rf_rho_step(rho, wp, rc, e_r, sf0);
+          Jf = nJ;
+        }
+        goto scan_done;
+      }
+    }
+    if (lane == 0) {   // the reference's serial loop
+      double rho = 0.0, Jf = 0.0;
+      for (int t = 0; t < NT; ++t) {
+        const Rl Ef = R[t];
+        const Rl I = Ic * (Ef * Ef);
+        const double E = (double)(float)Ef;
+        const double wp = (double)(float)lut_eval<Rl>(tb.lut, I);
+        const double wa = (double)(float)(Av * I);
+        double dep = (rc.rho_nt - rho) / rc.rho_nt;
+        if (dep < 0.0) dep = 0.0;
+        const double Se = wp * rc.rho_nt * dep;
+        const double Ge = wa * dep - rc.rr;
+        double gdt = Ge * rc.dt;
+        if (gdt > 10.0) gdt = 10.0;
+        if (gdt < -10.0) gdt = -10.0;
+        const double eg = exp(gdt);
+        const double sf = (fabs(gdt) < 1e-5) ? rc.dt * (1.0 + 0.5 * gdt) : (eg - 1.0) / Ge;
+        double nr = rho * eg + Se * sf;
+        if (nr > rc.rho_nt) nr = rc.rho_nt;
+        if (nr < 0.0) nr = 0.0;
+        const double gen = Se + wa * dep * rho;
+        const double nJ = Jf * rc.exp_nu + rc.e2m * rho * E * rc.step_J;
+        const double Jl = fabs(E) > 1e-10 ? (gen * rc.Ui * E) / (E * E + 1e-20) : 0.0;
+        S[tpad(t)].y = (Rl)(Jf + Jl) / Es;       // J (solver precision) / E_scale
+        rho = nr;
+        Jf = nJ;
+      }
+    }
+  scan_done:;
   }
   __syncwarp();
   const Rl c3 = (Rl)rc.chi3e, c5 = (Rl)rc.chi5e;
