@@ -204,11 +204,21 @@ def batched1d_instances(n=256, seed=2, L=1.0):
     return insts, fields
 
 
-def run_batched1d(dev):
-    """Whole sweep in one persistent launch; sims/s over CUDA events."""
+def run_batched1d(dev, rank=0, world=1):
+    """Whole sweep in one persistent launch per GPU; sims/s over CUDA events.  With
+    several ranks the instances are sharded (longest-processing-time balance on
+    Nt log Nt), the time is the max over ranks and the per-instance results are
+    gathered (no data-path collective)."""
     import torch
+    from project_b200.distributed import gather_results, instance_cost, partition_instances
     from project_b200.solver1d import BatchedPropagator
     insts, fields = batched1d_instances()
+    n_all = len(insts)
+    mine = list(range(n_all))
+    if world > 1:
+        costs = [instance_cost(i['desc'].Nt, i['desc'].L) for i in insts]
+        mine = partition_instances(costs, world)[rank]
+        insts, fields = [insts[i] for i in mine], [fields[i] for i in mine]
     bp = BatchedPropagator(insts, precision='single', device=dev)
     packed0 = bp.pack(fields)
     work = packed0.clone()
@@ -222,7 +232,15 @@ def run_batched1d(dev):
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     att = [r.attempts for r in res]
-    return {'value': len(insts) / sec, 'unit': 'sims/s', 'n_instances': len(insts), 'seconds': sec,
+    if world > 1:
+        import torch.distributed as dist
+        t = torch.tensor([sec], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        sec = float(t.item())
+        merged = gather_results([(i, {'attempts': r.attempts, 'status': r.status}) for i, r in zip(mine, res)])
+        att = [merged[i]['attempts'] for i in range(n_all)]
+        res = [type('R', (), merged[i]) for i in range(n_all)]
+    return {'value': n_all / sec, 'unit': 'sims/s', 'n_instances': n_all, 'seconds': sec, 'ranks': world,
             'attempts_total': int(sum(att)), 'attempts_max': int(max(att)),
             'status_nonzero': int(sum(1 for r in res if r.status)), 'dtype': 'c64',
             'workload': 'batched 1D sweep, 256 argon-capillary instances, L = 1 m, tol 1e-6, '
@@ -491,7 +509,7 @@ def run_b200(args, rank, world, local_rank):
         cpu = cpu_baseline(prec)
     b1d = None
     if not args.no_batched_1d:
-        b1d = run_batched1d(dev)
+        b1d = run_batched1d(dev, rank, world)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             b1d['cpu_baseline'] = cpu_baseline_1d()
 
