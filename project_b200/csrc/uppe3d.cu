@@ -2750,8 +2750,8 @@ extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nstep
 // warp per (x, y) line, complex FFT in shared memory): real -> half spectrum,
 // the nonlinear response (half spectrum -> real E via the Hermitian extension,
 // PPT rate table, density + Drude current scan, Kerr + chi5 polarisation,
-// separate transforms of P and J, source coefficients P_c, J_c), and the
-// output (filter, inverse transform, absorber).  Stage algebra: one spectral
+// P and J in one transform after per-line scaling, source coefficients
+// P_c, J_c), and the output (filter, inverse transform, absorber).  Stage algebra: one spectral
 // kernel with exp(s D) computed per element in FP64.
 // ===========================================================================
 
@@ -2785,18 +2785,29 @@ __device__ __forceinline__ void rf_rho_step(double& rho, double wp, const RfCons
   rho = r;
 }
 
+// launch shape of k_rf_line: per warp a line buffer (PAD complex) and the real
+// samples (NT), up to 8 warps while two blocks fit an SM
+template <int NT, typename Rl> struct RfLaunch {
+  using C = typename CT<Rl>::T;
+  static constexpr size_t per_warp = (size_t)TCfg<NT>::PAD * sizeof(C) + NT * sizeof(Rl);
+  static constexpr size_t fixed = NT * sizeof(C);
+  static constexpr int WPB = (fixed + 8 * per_warp <= 113 * 1024) ? 8 : (fixed + 4 * per_warp <= 113 * 1024) ? 4
+                           : (fixed + 2 * per_warp <= 200 * 1024) ? 2 : 1;
+  static size_t smem() { return fixed + WPB * per_warp; }
+};
+
 // one t-line per warp; S: line buffer (PAD complex), R: real samples (NT)
 template <typename Rl, int NT, int WPB>
-__global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw,
-                                                    const void* in, void* out, const void* twt, double in_scale,
-                                                    double h) {
+__global__ void __launch_bounds__(WPB * 32, (WPB * 32 * 2 <= 1024) ? 2 : 1)
+k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, void* out, const void* twt,
+          double in_scale, double h) {
   using C = typename CT<Rl>::T;
   constexpr int PAD = TCfg<NT>::PAD;
   constexpr int NR = NT / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* S = tw + NT + warp * 2 * PAD;
+  C* S = reinterpret_cast<C*>(smem_raw + RfLaunch<NT, Rl>::fixed + warp * RfLaunch<NT, Rl>::per_warp);
   Rl* R = reinterpret_cast<Rl*>(S + PAD);
   for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(twt)[i];
   __syncthreads();
@@ -2850,9 +2861,11 @@ __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfC
     const double sf0 = (fabs(g0) < 1e-5) ? rc.dt * (1.0 + 0.5 * g0) : (e_r - 1.0) / (-rc.rr);
     bool ok = rc.aval == 0.0;
     double cm = 1.0, dm = 0.0;
-    for (int i = 0; i < EC; ++i) {
+    for (int i = 0; i < EC; ++i) {   // rates cached in S.x (the samples now live in R)
       const Rl Ef = R[t0 + i];
-      const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+      const float wf = (float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+      S[tpad(t0 + i)].x = (Rl)wf;
+      const double wp = (double)wf;
       const double c = e_r - wp * sf0;
       ok &= (c >= 0.0);
       dm = c * dm + wp * rc.rho_nt * sf0;
@@ -2877,7 +2890,7 @@ __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfC
         double rho = rho0, aJ = 1.0, bJ = 0.0;
         for (int i = 0; i < EC; ++i) {
           const Rl Ef = R[t0 + i];
-          const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+          const double wp = (double)(float)S[tpad(t0 + i)].x;
           const double dJ = rc.e2m * rho * (double)(float)Ef * rc.step_J;
           bJ = bJ * rc.exp_nu + dJ;
           aJ = aJ * rc.exp_nu;
@@ -2897,7 +2910,7 @@ __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfC
           const int t = t0 + i;
           const Rl Ef = R[t];
           const double E = (double)(float)Ef;
-          const double wp = (double)(float)lut_eval<Rl>(tb.lut, Ic * (Ef * Ef));
+          const double wp = (double)(float)S[tpad(t)].x;
           double dep = (rc.rho_nt - rho) / rc.rho_nt;
           if (dep < 0.0) dep = 0.0;
           const double gen = wp * rc.rho_nt * dep;            // w_av = 0
@@ -2952,24 +2965,35 @@ __global__ void __launch_bounds__(WPB * 32) k_rf_line(int mode, RfTables tb, RfC
     S[tpad(t)].x = P / Es;
   }
   __syncwarp();
-  // P and J are transformed separately: the polarisation can be many orders below
-  // the current, and a packed transform would bury its spectrum in J's rounding
-  C* S2 = reinterpret_cast<C*>(R);   // the field samples are no longer needed
+  // P and J (both real) share one complex transform, each scaled by its own line
+  // maximum first: the polarisation can be many orders below the current, and an
+  // unscaled packing would bury its spectrum in J's rounding
+  Rl mp = (Rl)0, mj = (Rl)0;
   for (int t = lane; t < NT; t += 32) {
     const C pj = S[tpad(t)];
-    S[tpad(t)] = C{pj.x, (Rl)0};
-    S2[tpad(t)] = C{pj.y, (Rl)0};
+    mp = fmax(mp, fabs(pj.x));
+    mj = fmax(mj, fabs(pj.y));
+  }
+#pragma unroll
+  for (int off = 16; off > 0; off >>= 1) {
+    mp = fmax(mp, __shfl_xor_sync(0xffffffffu, mp, off));
+    mj = fmax(mj, __shfl_xor_sync(0xffffffffu, mj, off));
+  }
+  const Rl sP = mp > (Rl)0 ? mp : (Rl)1, sJ = mj > (Rl)0 ? mj : (Rl)1;
+  for (int t = lane; t < NT; t += 32) {
+    const C pj = S[tpad(t)];
+    S[tpad(t)] = C{pj.x / sP, pj.y / sJ};
   }
   __syncwarp();
-  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());    // F(P)
-  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S2, tw, lane, LineIdx(), WarpSync());   // F(J)
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());    // F(P/sP + i J/sJ)
   C* o = reinterpret_cast<C*>(out) + line * Nw;
   const double kp2 = tb.kp2[line];
   const double cpl = 1.0 / (2.0 * 8.85418781e-12 * 299792458.0 * 299792458.0);
   for (int k = lane; k < Nw; k += 32) {
     if (k == 0 || k >= NR) { o[k] = C{0, 0}; continue; }   // DC source zeroed (solver_3d.py:95-97)
-    const C zp = S[tpad(k)], zj = S2[tpad(k)];
-    const double Pr = zp.x, Pi = zp.y, Jr = zj.x, Ji = zj.y;
+    const C z1 = S[tpad(k)], z2 = S[tpad((NT - k) % NT)];
+    const double Pr = 0.5 * ((double)z1.x + z2.x) * sP, Pi = 0.5 * ((double)z1.y - z2.y) * sP;   // F(P)[k]
+    const double Jr = 0.5 * ((double)z1.y + z2.y) * sJ, Ji = -0.5 * ((double)z1.x - z2.x) * sJ;  // F(J)[k]
     // kz: real root, or -i sqrt(|.|) for evanescent components; |kz| < 1e-10 -> 1e-10
     const double kz2 = tb.kk[k] - kp2;
     double kr, ki;
@@ -3235,8 +3259,8 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
 
 template <typename Rl, int NT>
 static int rf_line_n(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
-  constexpr int WPB = TLaunch<NT, Rl>::WPB;
-  const size_t smem = TLaunch<NT, Rl>::smem();
+  constexpr int WPB = RfLaunch<NT, Rl>::WPB;
+  const size_t smem = RfLaunch<NT, Rl>::smem();
   UPPE_CK(cudaFuncSetAttribute(k_rf_line<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Geom g;
   g.Nx = p->d.Nx; g.Ny = p->d.Ny; g.Nt = p->d.Nt; g.npts = p->nreal;
