@@ -372,7 +372,7 @@ def run_realfield(dev, cpu=True):
 
 
 def cpu_baseline_1d():
-    """Oracle port of the reference 1D solver on one config-0 instance (Nt 4096, 2 GW 30 fs,
+    """Oracle port of the reference 1D solver on one argon-capillary instance (Nt 4096, 2 GW 30 fs,
     argon 1 bar, 1 m, tol 1e-6, with the plasma term) on the host."""
     from oracle import uppe1d as o1
     from oracle.inputs import gaussian_pulse
@@ -386,7 +386,7 @@ def cpu_baseline_1d():
     _, _, _, log = s.propagate(gaussian_pulse(t, 2e9 * fw * np.sqrt(np.pi / (4 * np.log(2))), fw), t, 1.0, tol=1e-6)
     dt = time.perf_counter() - t0
     return {'value': 1.0 / dt, 'unit': 'sims/s', 'cores': 1, 'kind': 'port',
-            'sample': f'one config-0 instance (Nt 4096, 1 m, {len(log)} attempts) on numpy/scipy: {dt:.2f} s'}
+            'sample': f'one argon-capillary instance (Nt 4096, 2 GW 30 fs, 1 m, {len(log)} attempts) on numpy/scipy: {dt:.2f} s'}
 
 
 def profile_kernels(sol, lib, n_attempts=3):
