@@ -140,15 +140,17 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     cudaError_t e = cudaMallocHost(&p->h_res, sizeof(Res1D) * p->ninst);
     if (e != cudaSuccess) { uppe1d_plan_destroy(p); return UPPE_ERR_CUDA; }
   }
-  // packed twiddles: for every N = 2^k <= nmax, exp(-2 pi i m / N) at offset N - 1
+  // packed per-pass twiddles of the line FFT: for every N = 2^k <= nmax, N slots at
+  // offset N - 1, slot j holding exp(-2 pi i m / N) for m = line_twiddle_source(N, j)
   {
     std::vector<unsigned char> tw(p->csz * (size_t)(2 * nmax));
     for (int n = 1; n <= nmax; n *= 2) {
-      for (int m = 0; m < n; ++m) {
+      for (int j = 0; j < n; ++j) {
+        const long long m = line_twiddle_source(n, j);
         const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)m / (long double)n;
         const double cr = (double)cosl(ang), ci = (double)sinl(ang);
-        if (dbl) { ((double2*)tw.data())[n - 1 + m] = make_double2(cr, ci); }
-        else { ((float2*)tw.data())[n - 1 + m] = make_float2((float)cr, (float)ci); }
+        if (dbl) { ((double2*)tw.data())[n - 1 + j] = make_double2(cr, ci); }
+        else { ((float2*)tw.data())[n - 1 + j] = make_float2((float)cr, (float)ci); }
       }
     }
     TRY1(up1(p, &ptr, tw.data(), tw.size())); p->b.tw = ptr;

@@ -100,12 +100,87 @@ template <int N> struct Cfg1 {
 };
 
 static __device__ __forceinline__ int pad1(int n) { return n + (n >> 5); }
-struct Idx1 {
-  __device__ __forceinline__ int operator()(int, int n) const { return pad1(n); }
-};
-struct Sync1 {
-  __device__ __forceinline__ void operator()() const { __syncthreads(); }
-};
+
+// The line FFT (one signal of N points, team of Cfg1<N>::FT threads) reads its
+// twiddles from a per-pass table: pass (Ns, R) owns (R-1)*Ns consecutive slots
+// after the passes before it, slot (r-1)*Ns + k holding exp(-2 pi i r k / (Ns R)).
+// Adjacent lanes have adjacent k, so a warp's twiddle load is one contiguous run
+// instead of 32 scattered lines of the plain exp(-2 pi i m / N) table; the values
+// are the same entries of that table, so the transform is unchanged bit for bit.
+// The slots sum to N - 1, so the tables pack like the plain ones (size N at N-1).
+__host__ __device__ constexpr int line_fft_team(int n) { return n / 2 < T1 ? n / 2 : T1; }
+__host__ __device__ constexpr int line_pick_radix(int rem, int e) {
+  return (rem % 16 == 0 && e % 16 == 0) ? 16 : (rem % 8 == 0 && e % 8 == 0) ? 8
+       : (rem % 4 == 0 && e % 4 == 0) ? 4 : 2;
+}
+// plain-table index m (exp(-2 pi i m / n)) held by slot `slot` of the size-n per-pass table
+__host__ __device__ inline long long line_twiddle_source(int n, int slot) {
+  if (n < 2) return 0;
+  const int e = n / line_fft_team(n);
+  int ns = 1, off = 0;
+  while (ns < n) {
+    const int r = line_pick_radix(n / ns, e);
+    const int cnt = (r - 1) * ns;
+    if (slot < off + cnt) {
+      const int rr = (slot - off) / ns + 1, k = (slot - off) % ns;
+      return (long long)(rr * k) * (n / (ns * r));
+    }
+    off += cnt;
+    ns *= r;
+  }
+  return 0;   // slot n - 1 is padding
+}
+
+template <int N, int NTHR, int DIR, int Ns, int OFF, typename C>
+__device__ __forceinline__ void stockham_line(C* s, const C* tw, int tid) {
+  if constexpr (Ns < N) {
+    constexpr int E = N / NTHR;
+    static_assert(E >= 2, "need at least two elements per thread");
+    constexpr int R = PickRadix<N / Ns, E>::v;
+    static_assert(R == line_pick_radix(N / Ns, E), "pass list and twiddle layout disagree");
+    constexpr int B = E / R;
+    constexpr int M = N / R;
+    C v[B][R];
+    const bool act = tid < NTHR;
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int j = tid + b * NTHR;
+        const int k = j & (Ns - 1);
+#pragma unroll
+        for (int r = 0; r < R; ++r) v[b][r] = s[pad1(j + r * M)];
+        if constexpr (Ns > 1) {
+#pragma unroll
+          for (int r = 1; r < R; ++r) {
+            C w = tw[OFF + (r - 1) * Ns + k];
+            if (DIR > 0) w.y = -w.y;
+            v[b][r] = cmul(v[b][r], w);
+          }
+        }
+        DFT<R, DIR, C>::run(v[b]);
+      }
+    }
+    __syncthreads();
+    if (act) {
+#pragma unroll
+      for (int b = 0; b < B; ++b) {
+        const int j = tid + b * NTHR;
+        const int k = j & (Ns - 1);
+        const int base = (j / Ns) * Ns * R + k;
+#pragma unroll
+        for (int r = 0; r < R; ++r) s[pad1(base + r * Ns)] = v[b][r];
+      }
+    }
+    __syncthreads();
+    stockham_line<N, NTHR, DIR, Ns * R, OFF + (R - 1) * Ns, C>(s, tw, tid);
+  }
+}
+// DIR=-1 forward, +1 inverse (unscaled) transform of the padded line s
+template <int N, int DIR, typename C>
+__device__ __forceinline__ void line_fft(C* s, const C* tw, int tid) {
+  static_assert(Cfg1<N>::FT == line_fft_team(N), "team size and twiddle layout disagree");
+  stockham_line<N, Cfg1<N>::FT, DIR, 1, 0, C>(s, tw, tid);
+}
 
 static __device__ __forceinline__ double warp_sum(double v) {
 #pragma unroll
@@ -156,7 +231,13 @@ enum In1 { IN_A = 0, IN_2, IN_3, IN_4, IN_5 };
 
 template <typename Rl> struct Ctx1 {
   using C = typename CT<Rl>::T;
-  C* s;
+  // the padded line at the start of the dynamic shared memory, named as a shared
+  // array so the stage functions (not inlined into the kernel) get shared-memory
+  // accesses that the compiler may reorder around the global stage arrays
+  __device__ __forceinline__ C* sm() const {
+    extern __shared__ __align__(16) unsigned char smem[];
+    return reinterpret_cast<C*>(smem);
+  }
   double* red;
   double* starts;
   const C* tw;
@@ -169,10 +250,10 @@ template <typename Rl> struct Ctx1 {
 };
 
 // Density at the start of each thread's chunk of the line (time-domain field in
-// GA): a block scan of the chunks' affine maps, or lane 0's exact serial update
-// when a clamp binds.  Returns false when the whole line has W_ion = 0 and no
-// avalanche (the density stays 0).
-template <typename Rl, int N>
+// GA, or with FROM_S in the padded shared line): a block scan of the chunks'
+// affine maps, or lane 0's exact serial update when a clamp binds.  Returns
+// false when the whole line has W_ion = 0 and no avalanche (the density stays 0).
+template <typename Rl, int N, bool FROM_S = false>
 __device__ bool density_starts(Ctx1<Rl>& c, double& rho0) {
   using C = typename CT<Rl>::T;
   constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
@@ -184,7 +265,7 @@ __device__ bool density_starts(Ctx1<Rl>& c, double& rho0) {
   double cm = 1.0, dm = 0.0;
   if (tid < NA) {
     for (int t = tid * CH; t < tid * CH + CH; ++t) {
-      const C a = c.GA[t];
+      const C a = FROM_S ? c.sm()[pad1(t)] : c.GA[t];
       const Rl I = (Rl)(((double)a.x * a.x + (double)a.y * a.y) / Aeff);
       const double w = (double)(float)lut_eval<Rl>(c.lut, I);
       any_w |= (w != 0.0);
@@ -231,7 +312,7 @@ __device__ bool density_starts(Ctx1<Rl>& c, double& rho0) {
       double rho = 0.0;
       for (int t = 0; t < N; ++t) {
         if (t % CH == 0) c.starts[t / CH] = rho;
-        const C a = c.GA[t];
+        const C a = FROM_S ? c.sm()[pad1(t)] : c.GA[t];
         const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
         const double w = (double)(float)lut_eval<Rl>(c.lut, (Rl)Id);
         const double wa = (double)(float)(m.ava * (double)(Rl)Id);
@@ -247,22 +328,26 @@ __device__ bool density_starts(Ctx1<Rl>& c, double& rho0) {
 
 // plasma term P(t) = (loss + defocus)(t) * a(t) into the shared line, from the
 // time-domain field in GA (media_physics.py:156-203 with I = |A|^2 / A_eff).
-// Returns false (nothing written) when the whole line has W_ion = 0 and no
-// avalanche, i.e. the term is identically zero.
+// The field is first copied into the shared line with coalesced loads, so the
+// per-thread chunks of the scan read shared memory, and each thread overwrites
+// only its own chunk.  Returns false (the shared line then holds the field) when
+// the whole line has W_ion = 0 and no avalanche, i.e. the term is identically zero.
 template <typename Rl, int N>
 __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
   using C = typename CT<Rl>::T;
   constexpr int CH = Cfg1<N>::CH, NA = Cfg1<N>::NA;
   const int tid = threadIdx.x;
+  for (int t = tid; t < N; t += T1) c.sm()[pad1(t)] = c.GA[t];
+  __syncthreads();
   double rho0 = 0.0;
-  if (!density_starts<Rl, N>(c, rho0)) return false;
+  if (!density_starts<Rl, N, true>(c, rho0)) return false;
   const PlasmaConst& m = c.in->pc;
   const double Aeff = c.in->A_eff;
   double ion = 0.0;
   if (tid < NA) {
     double rho = rho0;
     for (int t = tid * CH; t < tid * CH + CH; ++t) {
-      const C a = c.GA[t];
+      const C a = c.sm()[pad1(t)];
       const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
       const Rl I = (Rl)Id;
       const double w = (double)(float)lut_eval<Rl>(c.lut, I);
@@ -273,7 +358,7 @@ __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
       const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
-      c.s[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
+      c.sm()[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
     }
   }
   if (ion_out) {   // block max of rho/rho_nt (every thread gets it)
@@ -300,82 +385,143 @@ __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename
   const int tid = threadIdx.x;
   const Rl hR = (Rl)h, h2 = (Rl)(h / 2), h6 = (Rl)(h / 6);
   double nrm = 0.0;
-  for (int w = tid; w < N; w += T1) {
-    C u;
-    if (mode == IN_A) {
-      u = c.A[w];
-    } else if (mode == IN_5) {
-      u = cadd(c.T[w], cscale(c.A4P[w], h6));
-      c.A4[w] = u;
-      nrm += (double)u.x * u.x + (double)u.y * u.y;
-    } else {
-      const C E = EFac<Rl>::get(c.D[w], 0.5 * h);
-      const C v = cmul(c.A[w], E);
-      if (mode == IN_2) {
-        const C a1 = cmul(c.K1[w], E);
-        c.T[w] = a1;
-        u = cadd(v, cscale(a1, h2));
-      } else if (mode == IN_3) {
-        const C o = c.O[w];
-        c.T[w] = cadd(c.T[w], cscale(o, (Rl)2));
-        u = cadd(v, cscale(o, h2));
-      } else {   // IN_4
-        const C o = c.O[w];
-        const C ts = cadd(c.T[w], cscale(o, (Rl)2));
-        c.T[w] = cmul(cadd(v, cscale(ts, h6)), E);    // beta
-        u = cmul(cadd(v, cscale(o, hR)), E);
+  // The stage loops load UB iterations' operands before any store, so a thread
+  // waits on one round of L2 latency per UB elements (the stage arrays may alias
+  // as far as the compiler knows, which would otherwise serialise them).
+  constexpr int UB = 4;
+  if (mode == IN_A) {
+    for (int w = tid; w < N; w += T1) {
+      const C u = c.A[w];
+      c.sm()[pad1(w)] = u;
+      if (save_u) save_u[w] = u;
+    }
+  } else if (mode == IN_5) {
+    for (int w0 = tid; w0 < N; w0 += UB * T1) {
+      C xt[UB], xp[UB];
+#pragma unroll
+      for (int q = 0; q < UB; ++q) {
+        const int w = w0 + q * T1;
+        if (w < N) { xt[q] = c.T[w]; xp[q] = c.A4P[w]; }
+      }
+#pragma unroll
+      for (int q = 0; q < UB; ++q) {
+        const int w = w0 + q * T1;
+        if (w < N) {
+          const C u = cadd(xt[q], cscale(xp[q], h6));
+          c.A4[w] = u;
+          nrm += (double)u.x * u.x + (double)u.y * u.y;
+          c.sm()[pad1(w)] = u;
+          if (save_u) save_u[w] = u;
+        }
       }
     }
-    c.s[pad1(w)] = u;
-    if (save_u) save_u[w] = u;
+  } else {
+    const C* X = mode == IN_2 ? c.K1 : c.O;
+    for (int w0 = tid; w0 < N; w0 += UB * T1) {
+      C xa[UB], xx[UB], xt[UB];
+      double2 xd[UB];
+#pragma unroll
+      for (int q = 0; q < UB; ++q) {
+        const int w = w0 + q * T1;
+        if (w < N) {
+          xa[q] = c.A[w];
+          xx[q] = X[w];
+          xd[q] = c.D[w];
+          xt[q] = mode == IN_2 ? czero<C>() : c.T[w];
+        }
+      }
+#pragma unroll
+      for (int q = 0; q < UB; ++q) {
+        const int w = w0 + q * T1;
+        if (w < N) {
+          const C E = EFac<Rl>::get(xd[q], 0.5 * h);
+          const C v = cmul(xa[q], E);
+          C u;
+          if (mode == IN_2) {
+            const C a1 = cmul(xx[q], E);
+            c.T[w] = a1;
+            u = cadd(v, cscale(a1, h2));
+          } else if (mode == IN_3) {
+            const C o = xx[q];
+            c.T[w] = cadd(xt[q], cscale(o, (Rl)2));
+            u = cadd(v, cscale(o, h2));
+          } else {   // IN_4
+            const C o = xx[q];
+            const C ts = cadd(xt[q], cscale(o, (Rl)2));
+            c.T[w] = cmul(cadd(v, cscale(ts, h6)), E);    // beta
+            u = cmul(cadd(v, cscale(o, hR)), E);
+          }
+          c.sm()[pad1(w)] = u;
+          if (save_u) save_u[w] = u;
+        }
+      }
+    }
   }
   __syncthreads();
   if (input_only) return 0.0;     // stage input formed (and saved) only
-  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  line_fft<N, +1>(c.sm(), c.tw, tid);
   const Rl invN = (Rl)(1.0 / N);
   const bool raman = c.in->raman, plasma = c.in->plasma;
   for (int t = tid; t < N; t += T1) {
-    const C a = cscale(c.s[pad1(t)], invN);
+    const C a = cscale(c.sm()[pad1(t)], invN);
     if (raman || plasma) c.GA[t] = a;
     if (hist_t) hist_t[t] = a;
     if (raman) {
-      c.s[pad1(t)] = C{a.x * a.x + a.y * a.y, (Rl)0};
+      c.sm()[pad1(t)] = C{a.x * a.x + a.y * a.y, (Rl)0};
     } else {
       const Rl I = a.x * a.x + a.y * a.y;
-      c.s[pad1(t)] = cscale(a, I);
+      c.sm()[pad1(t)] = cscale(a, I);
     }
   }
   __syncthreads();
   if (raman) {
     // I_eff = (1 - f_R) I + f_R ifft(H_R fft(I))   (erk43ip_method.py:208-215)
-    stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    line_fft<N, -1>(c.sm(), c.tw, tid);
     for (int w = tid; w < N; w += T1) {
       const double2 Hw = c.H[w];
-      c.s[pad1(w)] = cmul(c.s[pad1(w)], C{(Rl)Hw.x, (Rl)Hw.y});
+      c.sm()[pad1(w)] = cmul(c.sm()[pad1(w)], C{(Rl)Hw.x, (Rl)Hw.y});
     }
     __syncthreads();
-    stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    line_fft<N, +1>(c.sm(), c.tw, tid);
     const Rl fR = (Rl)c.in->f_R, g1 = (Rl)(1.0 - c.in->f_R);
     for (int t = tid; t < N; t += T1) {
       const C a = c.GA[t];
       const Rl I = a.x * a.x + a.y * a.y;
-      const C Id = cscale(c.s[pad1(t)], invN);
+      const C Id = cscale(c.sm()[pad1(t)], invN);
       const C Ieff = C{g1 * I + fR * Id.x, fR * Id.y};
-      c.s[pad1(t)] = cmul(a, Ieff);
+      c.sm()[pad1(t)] = cmul(a, Ieff);
     }
     __syncthreads();
   }
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int w = tid; w < N; w += T1) {
-    const C p = c.s[pad1(w)];
-    const Rl g = (Rl)c.G[w];
-    out[w] = C{-g * p.y, g * p.x};     // i gamma U(w) P_NL(w)
+  line_fft<N, -1>(c.sm(), c.tw, tid);
+  for (int w0 = tid; w0 < N; w0 += UB * T1) {
+    double g[UB];
+#pragma unroll
+    for (int q = 0; q < UB; ++q) g[q] = w0 + q * T1 < N ? c.G[w0 + q * T1] : 0.0;
+#pragma unroll
+    for (int q = 0; q < UB; ++q) {
+      const int w = w0 + q * T1;
+      if (w < N) {
+        const C p = c.sm()[pad1(w)];
+        const Rl gr = (Rl)g[q];
+        out[w] = C{-gr * p.y, gr * p.x};     // i gamma U(w) P_NL(w)
+      }
+    }
   }
   __syncthreads();
   if (plasma) {
     if (plasma_line<Rl, N>(c, ion_out)) {
-      stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-      for (int w = tid; w < N; w += T1) out[w] = cadd(out[w], c.s[pad1(w)]);
+      line_fft<N, -1>(c.sm(), c.tw, tid);
+      for (int w0 = tid; w0 < N; w0 += UB * T1) {
+        C o[UB];
+#pragma unroll
+        for (int q = 0; q < UB; ++q) if (w0 + q * T1 < N) o[q] = out[w0 + q * T1];
+#pragma unroll
+        for (int q = 0; q < UB; ++q) {
+          const int w = w0 + q * T1;
+          if (w < N) out[w] = cadd(o[q], c.sm()[pad1(w)]);
+        }
+      }
       __syncthreads();
     }
   }
@@ -531,7 +677,6 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   const int tid = threadIdx.x;
   const Inst1D& in = b.inst[i];
   Ctx1<Rl> c;
-  c.s = reinterpret_cast<C*>(smem);
   c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
   c.starts = c.red + 64;
   c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
@@ -550,13 +695,13 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   // A0 -> history slot 0, state = fft(A0)
   for (int t = tid; t < N; t += T1) {
     const C a = field[t];
-    c.s[pad1(t)] = a;
+    c.sm()[pad1(t)] = a;
     if (hist) hist[t] = a;
   }
   if (zh && tid == 0) zh[0] = 0.0;
   __syncthreads();
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
+  line_fft<N, -1>(c.sm(), c.tw, tid);
+  for (int w = tid; w < N; w += T1) c.A[w] = c.sm()[pad1(w)];
   __syncthreads();
   double ion_peak = 0.0;
   nl_eval<Rl, N>(c, IN_A, 0.0, c.K1, nullptr, nullptr, false, &ion_peak);   // k1 = N(A)
@@ -571,11 +716,11 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   double en, ph;
   energy_photons<Rl, N>(c, in, en, ph);
   // final state back to the time domain
-  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+  for (int w = tid; w < N; w += T1) c.sm()[pad1(w)] = c.A[w];
   __syncthreads();
-  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  line_fft<N, +1>(c.sm(), c.tw, tid);
   const Rl invN = (Rl)(1.0 / N);
-  for (int t = tid; t < N; t += T1) field[t] = cscale(c.s[pad1(t)], invN);
+  for (int t = tid; t < N; t += T1) field[t] = cscale(c.sm()[pad1(t)], invN);
   if (tid == 0) {
     Res1D r;
     r.z = z; r.h = h; r.err = err; r.attempts = attempts; r.accepted = accepted;
@@ -599,7 +744,6 @@ __device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
   const int tid = threadIdx.x;
   const Prog1D& pg = b.prog[p];
   Ctx1<Rl> c;
-  c.s = reinterpret_cast<C*>(smem);
   c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
   c.starts = c.red + 64;
   c.tw = reinterpret_cast<const C*>(b.tw) + (N - 1);
@@ -610,10 +754,10 @@ __device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
   C* field = reinterpret_cast<C*>(b.field) + pg.field_off;
   C* rec = b.records ? reinterpret_cast<C*>(b.records) + pg.rec_off : nullptr;
   const Rl invN = (Rl)(1.0 / N);
-  for (int t = tid; t < N; t += T1) c.s[pad1(t)] = field[t];
+  for (int t = tid; t < N; t += T1) c.sm()[pad1(t)] = field[t];
   __syncthreads();
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int w = tid; w < N; w += T1) c.A[w] = c.s[pad1(w)];
+  line_fft<N, -1>(c.sm(), c.tw, tid);
+  for (int w = tid; w < N; w += T1) c.A[w] = c.sm()[pad1(w)];
   __syncthreads();
   for (long long o = pg.op_begin; o < pg.op_end; ++o) {
     const Op1D op = b.ops[o];
@@ -653,10 +797,10 @@ __device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
       r.photons = NAN;
     }
     if (op.record && rec) {
-      for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+      for (int w = tid; w < N; w += T1) c.sm()[pad1(w)] = c.A[w];
       __syncthreads();
-      stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-      for (int t = tid; t < N; t += T1) rec[t] = cscale(c.s[pad1(t)], invN);
+      line_fft<N, +1>(c.sm(), c.tw, tid);
+      for (int t = tid; t < N; t += T1) rec[t] = cscale(c.sm()[pad1(t)], invN);
       rec += N;
       r.hist_count = 1;
       __syncthreads();
@@ -664,10 +808,10 @@ __device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
     if (tid == 0) b.op_res[o] = r;
     __syncthreads();
   }
-  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = c.A[w];
+  for (int w = tid; w < N; w += T1) c.sm()[pad1(w)] = c.A[w];
   __syncthreads();
-  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int t = tid; t < N; t += T1) field[t] = cscale(c.s[pad1(t)], invN);
+  line_fft<N, +1>(c.sm(), c.tw, tid);
+  for (int t = tid; t < N; t += T1) field[t] = cscale(c.sm()[pad1(t)], invN);
   __syncthreads();
 }
 
@@ -748,7 +892,7 @@ __device__ bool plasma_vjp1(Ctx1<double>& c, double2* acc, double* gpl) {
     }
     for (int i = CH - 1; i >= 0; --i) {
       const int t = tid * CH + i;
-      const C a = c.GA[t], q = c.s[pad1(t)];
+      const C a = c.GA[t], q = c.sm()[pad1(t)];
       const double I = (a.x * a.x + a.y * a.y) / Aeff;
       double A, B;
       plasma_rev<false>(m, aff, alpha, cur[i], (double)(float)lut_eval<double>(c.lut, I),
@@ -786,7 +930,7 @@ __device__ bool plasma_vjp1(Ctx1<double>& c, double2* acc, double* gpl) {
   if (tid < NA) {
     for (int i = CH - 1; i >= 0; --i) {
       const int t = tid * CH + i;
-      const C a = c.GA[t], q = c.s[pad1(t)];
+      const C a = c.GA[t], q = c.sm()[pad1(t)];
       const double I = (a.x * a.x + a.y * a.y) / Aeff;
       double A, B, oar, oai;
       plasma_rev<true>(m, aff, alpha, cur[i], (double)(float)lut_eval<double>(c.lut, I),
@@ -813,50 +957,50 @@ __device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const d
   const int tid = threadIdx.x;
   const double invN = 1.0 / N;
   const bool pl = c.in->plasma;
-  for (int w = tid; w < N; w += T1) c.s[pad1(w)] = u[w];
+  for (int w = tid; w < N; w += T1) c.sm()[pad1(w)] = u[w];
   __syncthreads();
-  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  line_fft<N, +1>(c.sm(), c.tw, tid);
   for (int t = tid; t < N; t += T1) {
-    const C a = cscale(c.s[pad1(t)], invN);
+    const C a = cscale(c.sm()[pad1(t)], invN);
     c.GA[t] = a;
-    if (!pl) c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
+    if (!pl) c.sm()[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
   }
   __syncthreads();
   bool pl_any = false;
   if (pl) {   // plasma term: q = F*(nb) (time domain), field cotangent into A4P
-    for (int w = tid; w < N; w += T1) c.s[pad1(w)] = nb[w];
+    for (int w = tid; w < N; w += T1) c.sm()[pad1(w)] = nb[w];
     __syncthreads();
-    stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+    line_fft<N, +1>(c.sm(), c.tw, tid);
     pl_any = plasma_vjp1<N>(c, c.A4P, gpl);
     __syncthreads();
     for (int t = tid; t < N; t += T1) {
       const C a = c.GA[t];
-      c.s[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
+      c.sm()[pad1(t)] = cscale(a, a.x * a.x + a.y * a.y);
     }
     __syncthreads();
   }
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  line_fft<N, -1>(c.sm(), c.tw, tid);
   for (int w = tid; w < N; w += T1) {
-    const C ph = c.s[pad1(w)];
+    const C ph = c.sm()[pad1(w)];
     const C n = nb[w];
     gG[w] += -n.x * ph.y + n.y * ph.x;
     const double g = c.G[w];
-    c.s[pad1(w)] = C{g * n.y, -g * n.x};          // -i G nb
+    c.sm()[pad1(w)] = C{g * n.y, -g * n.x};          // -i G nb
   }
   __syncthreads();
-  stockham<N, 1, FT, +1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
+  line_fft<N, +1>(c.sm(), c.tw, tid);
   for (int t = tid; t < N; t += T1) {
     const C a = c.GA[t];
-    const C pb = c.s[pad1(t)];
+    const C pb = c.sm()[pad1(t)];
     const double I2 = 2.0 * (a.x * a.x + a.y * a.y);
     const C a2 = cmul(a, a);
     C ab = cadd(cscale(pb, I2), cmul(a2, cconj(pb)));
     if (pl_any) ab = cadd(ab, c.A4P[t]);
-    c.s[pad1(t)] = ab;
+    c.sm()[pad1(t)] = ab;
   }
   __syncthreads();
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int w = tid; w < N; w += T1) out[w] = cscale(c.s[pad1(w)], invN);
+  line_fft<N, -1>(c.sm(), c.tw, tid);
+  for (int w = tid; w < N; w += T1) out[w] = cscale(c.sm()[pad1(w)], invN);
   __syncthreads();
 }
 
@@ -882,7 +1026,6 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
   const int tid = threadIdx.x;
   const Inst1D& in = a.b.inst[a.inst];
   Ctx1<double> c;
-  c.s = reinterpret_cast<C*>(smem);
   c.red = reinterpret_cast<double*>(smem + sizeof(C) * Cfg1<N>::PAD);
   c.starts = c.red + 64;
   c.tw = reinterpret_cast<const C*>(a.b.tw) + (N - 1);
@@ -910,10 +1053,10 @@ __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
     C* t1 = c.K1; c.K1 = c.O; c.O = t1;
   };
   // forward replay with checkpoints every K steps
-  for (int t = tid; t < N; t += T1) c.s[pad1(t)] = a.A0[t];
+  for (int t = tid; t < N; t += T1) c.sm()[pad1(t)] = a.A0[t];
   __syncthreads();
-  stockham<N, 1, FT, -1, 1, C>(c.s, c.tw, tid, Idx1(), Sync1());
-  for (int x = tid; x < N; x += T1) { c.A[x] = c.s[pad1(x)]; a.gD[x] = C{0, 0}; a.gG[x] = 0.0; }
+  line_fft<N, -1>(c.sm(), c.tw, tid);
+  for (int x = tid; x < N; x += T1) { c.A[x] = c.sm()[pad1(x)]; a.gD[x] = C{0, 0}; a.gG[x] = 0.0; }
   if (tid < 3 && a.gPl) a.gPl[tid] = 0.0;
   __syncthreads();
   copy(CK, c.A);

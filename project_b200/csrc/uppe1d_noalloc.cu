@@ -46,15 +46,16 @@ static __device__ __align__(256) unsigned char g_noalloc_scratch[UPPE_NOALLOC_SC
 constexpr int kMaxDevices = 64;
 static void* g_scratch_addr[kMaxDevices];   // device address per device ordinal
 
-// Packed twiddles exp(-2 pi i m / n) for n = 1, 2, 4, ..., nmax at offset n - 1,
-// written straight into the static array (this kernel names it directly).
+// Packed per-pass line-FFT twiddles for n = 1, 2, 4, ..., nmax at offset n - 1 (slot j
+// of size n holds exp(-2 pi i m / n), m = line_twiddle_source(n, j)), written
+// straight into the static array (this kernel names it directly).
 template <typename C>
 __global__ void k_noalloc_twiddles(size_t byte_off, int nmax) {
   C* tw = reinterpret_cast<C*>(g_noalloc_scratch + byte_off);
   const int total = 2 * nmax - 1;
   for (int p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += gridDim.x * blockDim.x) {
     const int n = 1 << (31 - __clz(p + 1));   // largest power of two <= p + 1
-    const int m = p + 1 - n;
+    const long long m = line_twiddle_source(n, p + 1 - n);
     double s, c;
     sincospi(-2.0 * (double)m / (double)n, &s, &c);
     tw[p].x = (decltype(tw[p].x))c;
