@@ -343,6 +343,8 @@ __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
   if (!density_starts<Rl, N, true>(c, rho0)) return false;
   const PlasmaConst& m = c.in->pc;
   const double Aeff = c.in->A_eff;
+  const AffineStep aff(m);
+  const bool no_ava = (m.ava == 0.0);
   double ion = 0.0;
   if (tid < NA) {
     double rho = rho0;
@@ -354,7 +356,8 @@ __device__ bool plasma_line(Ctx1<Rl>& c, double* ion_out) {
       const double wa = (double)(float)(m.ava * (double)I);
       const double rho_t = rho;
       ion = fmax(ion, rho_t);
-      const double gen = rho_step(rho, w, wa, m);
+      // without avalanche the exp-free step gives the same values (rho_step0)
+      const double gen = no_ava ? rho_step0(rho, w, m, aff) : rho_step(rho, w, wa, m);
       const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
