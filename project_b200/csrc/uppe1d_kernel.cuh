@@ -384,7 +384,6 @@ __device__ __noinline__ double nl_eval(Ctx1<Rl>& c, int mode, double h, typename
                           typename CT<Rl>::T* hist_t, typename CT<Rl>::T* save_u = nullptr,
                           bool input_only = false, double* ion_out = nullptr) {
   using C = typename CT<Rl>::T;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const Rl hR = (Rl)h, h2 = (Rl)(h / 2), h6 = (Rl)(h / 6);
   double nrm = 0.0;
@@ -676,7 +675,6 @@ __device__ __forceinline__ void energy_photons(Ctx1<Rl>& c, const Inst1D& in, do
 template <typename Rl, int N>
 __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   using C = typename CT<Rl>::T;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const Inst1D& in = b.inst[i];
   Ctx1<Rl> c;
@@ -743,7 +741,6 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
 template <typename Rl, int N>
 __device__ void run_program(const Batch1D& b, int p, unsigned char* smem) {
   using C = typename CT<Rl>::T;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const Prog1D& pg = b.prog[p];
   Ctx1<Rl> c;
@@ -956,7 +953,6 @@ template <int N>
 __device__ __noinline__ void vjp_eval(Ctx1<double>& c, const double2* u, const double2* nb,
                                       double2* out, double* gG, double* gpl) {
   using C = double2;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const double invN = 1.0 / N;
   const bool pl = c.in->plasma;
@@ -1025,7 +1021,6 @@ struct Adj1D {
 template <int N>
 __device__ void adjoint_instance(const Adj1D& a, unsigned char* smem) {
   using C = double2;
-  constexpr int FT = Cfg1<N>::FT;
   const int tid = threadIdx.x;
   const Inst1D& in = a.b.inst[a.inst];
   Ctx1<double> c;
