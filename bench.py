@@ -5,14 +5,18 @@ Workload: 256 x 256 x 512 grid (6 mm x 6 mm x 400 fs), collimated Gaussian beam
 1 bar (n2 = 1e-23 m^2/W, GVD 20 fs^2/m, ADK ionisation, plasma defocusing and
 loss, self-steepening), L = 2 m, tol = 1e-5; mixed precision by default.
 
-A "step" is one ERK4(3) attempt of the adaptive propagation starting at z = 0,
-with acceptance and step-size control on the device (one CUDA-graph launch per
-attempt).  value = grid points x attempts x ranks / (max over ranks of the
-CUDA-event time of the timed attempts).  Every field (268 MB in complex64) is
-larger than the 126 MB L2, so no L2 flush is inserted.
+A "step" is one ERK4(3) attempt of that adaptive propagation, with acceptance and
+step-size control on the device (one CUDA-graph launch per attempt).  The timed
+attempts start at z = 1 m, where the beam collapses into a filament: the step
+size falls, attempts are rejected and the first lines ionise.  value = grid
+points x attempts x ranks / (max over ranks of the CUDA-event time of the timed
+attempts).  Every field (268 MB in complex64) is larger than the 126 MB L2, so
+no L2 flush is inserted.  The whole 2 m run is timed as well (config1_full), and
+e2e runs it through the public propagate() call with host buffers.
 
 --impl reference times the CPU oracle port of the reference's algorithm on the
-host cores (rank 0 only) on a bounded sample of the same workload.
+host cores (rank 0 only), one ERK attempt of the same 256 x 256 x 512 workload
+per step.
 """
 import argparse
 import ctypes
@@ -36,8 +40,14 @@ ENERGY = 2e-3
 W0 = 1e-3
 L_PROP = 2.0
 TOL = 1e-5
-SAMPLE_N = 128       # CPU sample: 128 x 128 x 512
 LAM_1D = 800e-9
+Z_TIMED = 1.0        # the timed attempts start here: onset of the collapse
+Z_ION_TIMED = 1.0    # with the multiphoton table: start of the ionising filament
+H_FIRST = 2e-3       # first step of the 2 m run: min(max_step, L/1000) (solver_3d.py:173)
+
+
+CONFIG_WORKLOAD = ('3+1D UPPE envelope ERK4(3)-IP, argon 1 bar, ADK + plasma, self-steepening, '
+                   '256x256x512, 6 mm x 400 fs, 2 mJ 40 fs, w0 1 mm, 1% speckle, L 2 m, tol 1e-5')
 
 
 def grids(n=NX, nt=NT):
@@ -120,58 +130,64 @@ class ClockSampler:
                 'reasons': sorted(reasons), 'samples': len(sm)}
 
 
-def cpu_baseline(precision='single'):
-    """Oracle port (the reference algorithm on numpy/scipy) on a bounded sample:
-    one ERK attempt on a 128 x 128 x 512 grid, scipy.fft using every host core."""
-    import scipy.fft
+def _oracle_attempt_setup(precision='single'):
+    """The oracle port's solver and normalised input at the full 256 x 256 x 512 grid."""
     from oracle import uppe3d
-    cores = len(os.sched_getaffinity(0))
-    x, y, t = grids(SAMPLE_N, NT)
+    x, y, t = grids()
     med = argon_medium(precision, oracle=True)
     sol = uppe3d.Solver3D(x, y, t, med, precision)
     A0 = make_input(x, y, t, np.complex64 if precision == 'single' else np.complex128)
     sol.A_scale = float(np.max(np.abs(A0)))
-    A = (A0 / sol.A_scale).astype(sol.complex_dtype)
-    with scipy.fft.set_workers(cores):
-        t0 = time.perf_counter()
-        sol.erk43_step(A, 2e-3)
-        dt = time.perf_counter() - t0
-    pts = SAMPLE_N * SAMPLE_N * NT
-    return {'value': pts / dt, 'unit': 'pt-steps/s', 'cores': cores, 'kind': 'port',
-            'sample': f'one ERK attempt on {SAMPLE_N}x{SAMPLE_N}x{NT} (c64, numpy/scipy, '
-                      f'{cores} FFT workers): {dt:.2f} s'}
+    return sol, (A0 / sol.A_scale).astype(sol.complex_dtype)
+
+
+def cpu_baseline(precision='single'):
+    """Oracle port (the reference algorithm on numpy/scipy) on the host: one ERK
+    attempt of the full 256 x 256 x 512 workload with scipy.fft using every host
+    core, and one with a single FFT worker (the reference's default)."""
+    import scipy.fft
+    cores = len(os.sched_getaffinity(0))
+    sol, A = _oracle_attempt_setup(precision)
+    pts = NX * NY * NT
+    out = {}
+    for workers in (cores, 1):
+        with scipy.fft.set_workers(workers):
+            t0 = time.perf_counter()
+            sol.erk43_step(A, H_FIRST)
+            out[workers] = time.perf_counter() - t0
+    return {'value': pts / out[cores], 'unit': 'pt-steps/s', 'cores': cores, 'kind': 'port',
+            'sample': f'one ERK attempt of the full {NX}x{NY}x{NT} workload (c64, numpy/scipy oracle '
+                      f'port, {cores} FFT workers): {out[cores]:.2f} s',
+            'single_worker': {'value': pts / out[1], 'unit': 'pt-steps/s', 'cores': 1,
+                              'sample': f'the same attempt with 1 FFT worker: {out[1]:.2f} s'}}
 
 
 def run_reference(args, rank):
+    """The reference's algorithm (oracle port of solver_3d.py:100-160 with
+    media_physics.py:156-205, numpy/scipy) on the host cores, rank 0 only: each step
+    is one ERK attempt of the same 256 x 256 x 512 c64 workload the GPU arm runs.
+    One untimed warm-up attempt (FFT planning); the CPU path has no other warm-up."""
     if rank != 0:
         return 0
     import scipy.fft
-    from oracle import uppe3d
     cores = len(os.sched_getaffinity(0))
-    x, y, t = grids(SAMPLE_N, NT)
-    med = argon_medium('single', oracle=True)
-    sol = uppe3d.Solver3D(x, y, t, med, 'single')
-    A0 = make_input(x, y, t, np.complex64)
-    sol.A_scale = float(np.max(np.abs(A0)))
-    A = (A0 / sol.A_scale).astype(sol.complex_dtype)
-    pts = SAMPLE_N * SAMPLE_N * NT
+    sol, A = _oracle_attempt_setup('single')
+    pts = NX * NY * NT
     with scipy.fft.set_workers(cores):
-        for _ in range(args.warmup):
-            sol.erk43_step(A, 2e-3)
+        sol.erk43_step(A, H_FIRST)
         t0 = time.perf_counter()
         for _ in range(args.steps):
-            A4, err, _, _ = sol.erk43_step(A, 2e-3)
+            sol.erk43_step(A, H_FIRST)
         dt = time.perf_counter() - t0
     v = pts * args.steps / dt
-    sample = (f'{args.steps} ERK attempts on {SAMPLE_N}x{SAMPLE_N}x{NT} (c64, oracle port of '
-              f'solver_3d.py:100-160 + media_physics.py, {cores} FFT workers)')
+    sample = (f'{args.steps} ERK attempts of the full {NX}x{NY}x{NT} workload from z = 0 (c64, oracle '
+              f'port of solver_3d.py:100-160 + media_physics.py, {cores} FFT workers), 1 warm-up attempt')
     print(json.dumps({
         'impl': 'reference', 'metric': METRIC, 'value': v, 'unit': 'pt-steps/s',
-        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup,
+        'n_gpus': args.gpus, 'steps': args.steps, 'warmup': args.warmup, 'warmup_attempts_run': 1,
         'ms_per_step': 1e3 * dt / args.steps, 'higher_is_better': True, 'scaling': 'weak',
         'vs_baseline': None, 'dtype': 'c64', 'data': 'synthetic',
-        'config': {'workload': '3+1D UPPE envelope ERK4(3)-IP, argon 1 bar, bounded CPU sample',
-                   'grid': [SAMPLE_N, SAMPLE_N, NT]},
+        'config': {'workload': CONFIG_WORKLOAD, 'grid': [NX, NY, NT], 'same_config': True},
         'cpu_baseline': {'value': v, 'unit': 'pt-steps/s', 'cores': cores, 'kind': 'port',
                          'sample': sample},
         'e2e': {'value': v, 'unit': 'pt-steps/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
@@ -204,7 +220,7 @@ def batched1d_instances(n=256, seed=2, L=1.0):
     return insts, fields
 
 
-def run_batched1d(dev, rank=0, world=1):
+def run_batched1d(dev, rank=0, world=1, accuracy=False):
     """Whole sweep in one persistent launch per GPU; sims/s over CUDA events.  With
     several ranks the instances are sharded (longest-processing-time balance on
     Nt log Nt), the time is the max over ranks and the per-instance results are
@@ -225,13 +241,19 @@ def run_batched1d(dev, rank=0, world=1):
     bp.run_packed(work)                      # warm-up (first launch)
     work.copy_(packed0)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0, e1 = _events()
     e0.record()
     res = bp.run_packed(work)
     e1.record()
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     att = [r.attempts for r in res]
+    acc = None
+    if accuracy and world == 1:
+        try:
+            acc = batched1d_accuracy(bp, insts, packed0, work, dev)
+        except Exception as e:   # reported, never fatal
+            acc = {'error': str(e)[:300]}
     if world > 1:
         import torch.distributed as dist
         t = torch.tensor([sec], device=dev, dtype=torch.float64)
@@ -244,10 +266,78 @@ def run_batched1d(dev, rank=0, world=1):
             'attempts_total': int(sum(att)), 'attempts_max': int(max(att)),
             'status_nonzero': int(sum(1 for r in res if r.status)), 'dtype': 'c64',
             'workload': 'batched 1D sweep, 256 argon-capillary instances, L = 1 m, tol 1e-6, '
-                        'one persistent launch'}
+                        'one persistent launch', 'accuracy': acc}
 
 
-def run_gradients(dev):
+def batched1d_accuracy(bp, insts, packed0, final64, dev):
+    """Each instance's mixed-precision final field against the complex128 run of the
+    same instance (each with its own adaptive steps at the sweep's tol 1e-6); every
+    instance the complex128 kernel supports.  A frozen-step replay is not used
+    here: the stiffest instances (1 mJ at 3 bar) are ill-conditioned, and a step
+    sequence accepted in one precision can be unstable in the other."""
+    import torch
+    from project_b200.solver1d import BatchedPropagator
+    n = len(insts)
+    sub = [k for k in range(n) if insts[k]['desc'].Nt <= 8192]
+    bd = BatchedPropagator([insts[k] for k in sub], precision='double', device=dev)
+    off = bp.offsets
+    f128 = torch.cat([packed0[off[k]:off[k + 1]] for k in sub]).to(torch.complex128).contiguous()
+    r2 = bd.run_packed(f128)
+    res64 = getattr(bp, 'last_results', None)
+    rels, dE = [], []
+    for j, k in enumerate(sub):
+        a = final64[off[k]:off[k + 1]]
+        b = f128[bd.offsets[j]:bd.offsets[j + 1]]
+        rels.append(_rel(a, b))
+        e64 = float((a.abs().double() ** 2).sum()) * insts[k]['desc'].dt
+        dE.append(abs(e64 - r2[j].energy) / r2[j].energy)
+    rels = np.array(rels)
+    worst = [{'Nt': int(insts[sub[j]]['desc'].Nt), 'attempts_c128': int(r2[j].attempts),
+              'relL2': float(rels[j])} for j in np.argsort(rels)[::-1][:3]]
+    # the same comparison on the same steps: complex128 replays of each instance's
+    # complex64 step log; a replay whose energy leaves the complex64 run's by more
+    # than 1 % (a step accepted in one precision is unstable in the other) is counted
+    # apart, since its difference measures that instability, not the precision
+    import ctypes
+    from project_b200 import _lib
+    lib = _lib.load()
+    cap = 8192
+    hlog = torch.zeros(n * cap, dtype=torch.float64, device=dev)
+    w64 = packed0.clone()
+    r64 = (_lib.Result1D * n)()
+    _lib.check(lib.uppe1d_propagate_logged(bp._plan, ctypes.c_void_p(w64.data_ptr()),
+                                           ctypes.c_void_p(hlog.data_ptr()), cap, r64, _lib.stream_ptr()), 'log')
+    nsched = max(int(r64[k].accepted) for k in sub)
+    sched = torch.zeros(len(sub), nsched, dtype=torch.float64, device=dev)
+    hv = hlog.view(n, cap)
+    for j, k in enumerate(sub):         # zero-length steps leave a state unchanged
+        sched[j, :int(r64[k].accepted)] = hv[k, :int(r64[k].accepted)]
+    f2 = torch.cat([packed0[off[k]:off[k + 1]] for k in sub]).to(torch.complex128).contiguous()
+    r3 = (_lib.Result1D * len(sub))()
+    _lib.check(lib.uppe1d_propagate_schedule(bd._plan, ctypes.c_void_p(f2.data_ptr()),
+                                             ctypes.c_void_p(sched.data_ptr()), nsched, r3, _lib.stream_ptr()),
+               'uppe1d_propagate_schedule')
+    rr, unstable = [], 0
+    for j, k in enumerate(sub):
+        e64, e128 = r64[k].energy, r3[j].energy
+        if not np.isfinite(e128) or abs(e128 - e64) > 0.01 * e64:
+            unstable += 1
+            continue
+        rr.append(_rel(w64[off[k]:off[k + 1]], f2[bd.offsets[j]:bd.offsets[j + 1]]))
+    rr = np.array(rr)
+    same_steps = {'relL2_median': float(np.median(rr)), 'relL2_p90': float(np.percentile(rr, 90)),
+                  'relL2_max': float(rr.max()), 'within_1e-4': int(np.sum(rr <= 1e-4)),
+                  'replays_unstable': unstable}
+    return {'instances_compared': len(sub), 'instances_not_compared': n - len(sub), 'worst': worst,
+            'why_not': 'Nt = 16384 in complex128 needs the cluster line kernel',
+            'relL2_median': float(np.median(rels)), 'relL2_p90': float(np.percentile(rels, 90)),
+            'relL2_max': float(rels.max()), 'within_1e-4': int(np.sum(rels <= 1e-4)),
+            'energy_rel_diff_max': float(max(dE)), 'tolerance': 1e-4,
+            'note': 'free-running in both precisions at tol 1e-6: differences include the adaptive '
+                    'steps\' own O(tol) discretisation differences', 'same_steps': same_steps}
+
+
+def run_gradients(dev, accuracy=False):
     """Gradient evaluations through the device adjoints (forward with step log +
     reverse pass, checkpoint every 32 steps), wall time with the device synchronised:
     (1) 1D capillary compression, Nt 8192 over 2 ps, 2 GW 30 fs + one-photon noise,
@@ -255,7 +345,10 @@ def run_gradients(dev):
     pressure and length; (2) 3+1D filament, 128 x 128 x 1024 over 4 mm x 500 fs, 1.5 mJ
     50 fs, w0 1 mm, 15 Zernike coefficients (sigma 0.1 rad, seed 4, aperture 2 mm) +
     input GDD, argon 1.5 bar with ADK plasma, 1.5 m, tol 1e-4, mixed precision.
-    Peak memory = plan allocations + torch's peak (workspace, checkpoints, tensors)."""
+    Peak memory = plan allocations + torch's peak (workspace, checkpoints, tensors).
+    Beside the adjoint values: the loss, central differences of the frozen-step map
+    (the map the adjoint differentiates) for one Zernike coefficient and the GDD,
+    and (accuracy) the mixed-precision exit field against complex128 on the same steps."""
     import torch
     from project_b200.adjoint import CapillaryCompression, FilamentZernike, Propagate1D, Propagate3D
     from project_b200.media import Argon
@@ -282,6 +375,7 @@ def run_gradients(dev):
     t2 = time.perf_counter()
     out['capillary_1d'] = {'forward_s': t1 - t0, 'adjoint_s': t2 - t1, 'steps': len(Propagate1D.last_steps),
                            'checkpoint_every': 32, 'params': 66, 'dtype': 'c128',
+                           'loss_W': float(loss.detach()),
                            'torch_peak_gb': torch.cuda.max_memory_allocated(dev) / 1e9,
                            'grad_norm_knots': float(gk.norm()), 'dL_dP': float(gP), 'dL_dL': float(gL)}
     N, Nt3 = 128, 1024
@@ -307,14 +401,57 @@ def run_gradients(dev):
     torch.cuda.synchronize(dev)
     t2 = time.perf_counter()
     r = sol.last_result
-    out['filament_3d'] = {'forward_s': t1 - t0, 'adjoint_s': t2 - t1, 'steps': int(r.accepted),
-                          'attempts': int(r.attempts), 'checkpoint_every': 32, 'params': 16,
-                          'dtype': 'c64 bulk, FP64 phase/error/controller',
-                          'workspace_gb': Propagate3D.workspace_bytes / 1e9,
-                          'peak_memory_gb': (plan_bytes + torch.cuda.max_memory_allocated(dev) - base) / 1e9,
-                          'plan_gb': plan_bytes / 1e9,
-                          'peak_ionization': sol.diagnostics()['peak_ionization'],
-                          'grad_norm_zernike': float(gc.norm()), 'dL_dGDD': float(gg)}
+    steps = np.array(Propagate3D.last_steps)
+    f3 = {'forward_s': t1 - t0, 'adjoint_s': t2 - t1, 'steps': int(r.accepted),
+          'attempts': int(r.attempts), 'checkpoint_every': 32, 'params': 16,
+          'dtype': 'c64 bulk, FP64 phase/error/controller',
+          'workspace_gb': Propagate3D.workspace_bytes / 1e9,
+          'peak_memory_gb': (plan_bytes + torch.cuda.max_memory_allocated(dev) - base) / 1e9,
+          'plan_gb': plan_bytes / 1e9,
+          'peak_ionization': sol.diagnostics()['peak_ionization'],
+          'loss_J_per_m2': float(loss.detach()), 'grad_norm_zernike': float(gc.norm()),
+          'dL_dGDD_per_fs2': float(gg) * 1e-30}
+
+    def frozen_loss(cv, gv, solver):
+        with torch.no_grad():
+            A = solver.replay(obj.input_field(cv, gv).to(solver.complex_dtype), steps)
+            a = A[obj.ix, obj.iy, :].to(torch.complex128)
+            return float(-(a.real ** 2 + a.imag ** 2).sum() * solver.dt)
+
+    # central differences and the c64/c128 comparison on a shorter cell (0.25 m, well
+    # before the collapse near 0.5 m): at 1.5 m the beam has collapsed, the exit fluence
+    # is ill-conditioned (|grad| ~ 1e11-1e15 per rad) and a perturbed input can make
+    # a frozen step unstable, so differences there measure the collapse, not the adjoint
+    Lfd = 0.25
+    loss_fd = obj.loss(c, gdd, Lfd, tol=1e-4, K=32)
+    gc, gg = torch.autograd.grad(loss_fd, [c, gdd])
+    steps = np.array(Propagate3D.last_steps)
+    f3['check_L_m'] = Lfd
+    f3['check_loss_J_per_m2'] = float(loss_fd.detach())
+    j = int(torch.argmax(gc.abs()))
+    dc, dg = 1e-3, 10e-30
+    e = torch.zeros_like(c)
+    e[j] = dc
+    cd = c.detach()
+    fd_c = (frozen_loss(cd + e, gdd.detach(), sol) - frozen_loss(cd - e, gdd.detach(), sol)) / (2 * dc)
+    fd_g = (frozen_loss(cd, gdd.detach() + dg, sol) - frozen_loss(cd, gdd.detach() - dg, sol)) / (2 * dg)
+    f3['central_difference'] = {
+        'map': 'frozen accepted steps (the map the adjoint differentiates), mixed precision',
+        'zernike_index': j, 'step_rad': dc, 'adjoint': float(gc[j]), 'fd': fd_c,
+        'gdd_step_fs2': dg * 1e30, 'adjoint_gdd_per_fs2': float(gg) * 1e-30, 'fd_gdd_per_fs2': fd_g * 1e-30}
+    if accuracy:
+        s128 = ERK43IP_UPPE_3D_Optimized(x, x, t3, Argon(LAM_1D, 1.5, 'double', True), precision='double',
+                                         device=dev)
+        with torch.no_grad():
+            Ain = obj.input_field(cd, gdd.detach())
+            o64 = sol.replay(Ain.to(torch.complex64), steps)
+            o128 = s128.replay(Ain.to(torch.complex128), steps)
+            f3['accuracy'] = {'L_m': Lfd, 'relL2_exit_c64_vs_c128_same_steps': _rel(o64, o128), 'tolerance': 1e-4,
+                              'loss_c64': frozen_loss(cd, gdd.detach(), sol),
+                              'loss_c128': frozen_loss(cd, gdd.detach(), s128)}
+        del s128
+        torch.cuda.empty_cache()
+    out['filament_3d'] = f3
     return out
 
 
@@ -414,6 +551,204 @@ def profile_kernels(sol, lib, n_attempts=3):
     return agg
 
 
+def _events():
+    import torch
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_chunks(sol, nmax, chunk, stop=None):
+    """Graph launches (one attempt each) in chunks, CUDA events around each chunk;
+    stops when the run is over (the attempt count no longer moves), after nmax
+    launches, or when stop(result) holds.  Returns (device ms, result)."""
+    import torch
+    from project_b200 import _lib
+    lib, s = sol._lib, _lib.stream_ptr()
+    ms, done = 0.0, 0
+    r = sol.result()
+    while done < nmax:
+        n = min(chunk, nmax - done)
+        e0, e1 = _events()
+        e0.record()
+        _lib.check(lib.uppe3d_run_steps(sol._plan, n, s), 'uppe3d_run_steps')
+        e1.record()
+        torch.cuda.synchronize()
+        ms += e0.elapsed_time(e1)
+        done += n
+        r1 = sol.result()
+        finished = r1.attempts == r.attempts
+        r = r1
+        if finished or (stop is not None and stop(r)):
+            break
+    return ms, r
+
+
+def line_stats(sol, med):
+    """From the current field: the fraction of (x, y) lines on which the t-line kernel
+    runs the plasma terms (peak intensity above the last zero of the float32 rate
+    table) and the fraction on which the density scan leaves its affine form (rate
+    x dt above exp(-dt/tau_rec) at the peak: one sample can saturate the density)."""
+    A = sol.field()
+    Ipk = (A.real.float() ** 2 + A.imag.float() ** 2).amax(dim=2).double().cpu().numpy().ravel()
+    lx = np.asarray(med.lut_log10I, dtype=np.float64)
+    lw = np.asarray(med.lut_W, dtype=np.float32).astype(np.float64)
+    nz = np.nonzero(lw)[0]
+    I_on = 10.0 ** lx[nz[0] - 1] if len(nz) and nz[0] > 0 else (0.0 if len(nz) else np.inf)
+    W = np.interp(np.clip(np.log10(Ipk + 1e-30), lx[0], lx[-1]), lx, lw)
+    dt = float(sol.dt)
+    return {'plasma_lines': float(np.mean(Ipk > I_on)),
+            'saturating_lines': float(np.mean(W * dt > np.exp(-dt / med.tau_rec))),
+            'peak_intensity_Wm2': float(Ipk.max())}
+
+
+def full_run(sol, A_dev, hlog=None):
+    """The whole adaptive 2 m propagation from A_dev on the device, CUDA-event timed."""
+    import ctypes
+    from project_b200 import _lib
+    lib, s = sol._lib, _lib.stream_ptr()
+    sol.set_field(A_dev)
+    if hlog is not None:
+        _lib.check(lib.uppe3d_set_step_log(sol._plan, ctypes.c_void_p(hlog.data_ptr()), hlog.numel(), s), 'log')
+    _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'uppe3d_begin')
+    ms, r = run_chunks(sol, 10 ** 7, 16)
+    if hlog is not None:
+        _lib.check(lib.uppe3d_set_step_log(sol._plan, None, 0, s), 'log')
+    d = sol.diagnostics()
+    npts = sol.Nx * sol.Ny * sol.Nt
+    return {'device_s': ms / 1e3, 'attempts': int(r.attempts), 'accepted': int(r.accepted),
+            'rejected': int(r.attempts - r.accepted), 'z_m': r.z, 'status': int(r.status),
+            'value': npts * r.attempts / (ms / 1e3), 'unit': 'pt-steps/s',
+            'energy_J': d['energy'], 'photons': d['photons'], 'peak_ionization': d['peak_ionization']}
+
+
+def _rel(a, b):
+    import torch
+    a = a.to(torch.complex128)
+    b = b.to(torch.complex128)
+    return float(torch.linalg.vector_norm(a - b) / torch.linalg.vector_norm(b))
+
+
+def accuracy_config1(sol64, x, y, t, A0, steps, a_T, state_T, final64, dev, early=None):
+    """Mixed precision against the complex128 device path (pinned to the oracle and
+    the reference's own runs at small grids) on the same accepted step sequence:
+    rel-L2 of the field at the end of the timed attempts and at z = 2 m, energy,
+    photon number and peak ionisation of both; one attempt from the same state in
+    both precisions; and the complex128 run from the complex64-rounded input, which
+    shows how far the dynamics alone amplify an input difference of that size."""
+    import torch
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    s128 = ERK43IP_UPPE_3D_Optimized(x, y, t, argon_medium('double'), precision='double', device=dev)
+    marks = {a_T, len(steps)} | ({k for k in early} if early else set())
+
+    def replay(Ain):
+        s128.set_field(Ain)
+        snaps = {}
+        for k, h in enumerate(steps):
+            s128.attempt(float(h))
+            s128.commit(True)
+            if k + 1 in marks:
+                snaps[k + 1] = s128.field()
+        return snaps
+
+    A128 = torch.from_numpy(make_input(x, y, t, np.complex128)).to(dev)   # exact input
+    base = replay(A128)
+    d128 = s128.diagnostics()
+    d64 = sol64.diagnostics()
+    rounded = replay(A128.to(torch.complex64).to(torch.complex128))
+    out = {'grid': [NX, NY, NT], 'steps_replayed': len(steps), 'tolerance': 1e-4,
+           'relL2_after_timed': _rel(state_T, base[a_T]), 'z_after_timed_m': float(np.sum(steps[:a_T])),
+           'relL2_end': _rel(final64, base[len(steps)]),
+           'relL2_earlier': [{'accepted_steps': k, 'z_m': float(np.sum(steps[:k])),
+                              'relL2': _rel(early[k], base[k])} for k in sorted(early)] if early else None,
+           'c128_from_c64_rounded_input_relL2_after_timed': _rel(rounded[a_T], base[a_T]),
+           'c128_from_c64_rounded_input_relL2_end': _rel(rounded[len(steps)], base[len(steps)]),
+           'energy_J': {'c64': d64['energy'], 'c128': d128['energy']},
+           'photons': {'c64': d64['photons'], 'c128': d128['photons']},
+           'peak_ionization': {'c64': d64['peak_ionization'], 'c128': d128['peak_ionization']}}
+    # one attempt from the complex128 state at the timed window's end, in both precisions
+    snap = base[a_T]
+    h = float(steps[a_T]) if a_T < len(steps) else float(steps[-1])
+    s128.set_field(snap)
+    s128.attempt(h)
+    s128.commit(True)
+    o128 = s128.field()
+    sol64.set_field(snap.to(torch.complex64))
+    sol64.attempt(h)
+    sol64.commit(True)
+    o64 = sol64.field()
+    out['one_attempt_relL2'] = _rel(o64, o128)
+    out['one_attempt_input_rounding_relL2'] = _rel(snap.to(torch.complex64), snap)
+    del s128
+    torch.cuda.empty_cache()
+    return out
+
+
+def mpi_argon(precision, P=1.0):
+    """Argon with the reference's own multiphoton rate as the ionisation table:
+    W = sigma_K I^K, K = 11, sigma_K = 1e-188 P (media_physics.py:139-142, 410-417),
+    on the reference's grid (:121-126), without the tunnel term whose +1e-20
+    denominator makes it 1e15 1/s at every intensity.  Taylor GVD as argon_medium."""
+    from project_b200.media import Argon
+    m0 = Argon(LAM, P, precision, True)
+    lx = m0._lut_grid()
+    W = 1.0e-188 * P * (10.0 ** lx) ** 11
+    n0 = float(m0.refractive_index(np.array([m0.omega0]))[0])
+    return Argon(LAM, P, precision, True, dispersion=('taylor', n0, 20e-30, 0.0), lut=(lx, W))
+
+
+def run_ionising(args, x, y, t, A_dev, dev):
+    """The same 2 m run with the multiphoton table: the filament ionises (the
+    intensity clamps), so the density scan, plasma loss and defocusing and the
+    plasma transform run on the lines of the filament.  Timed: K attempts from
+    z = Z_ION_TIMED and the whole run (CUDA events)."""
+    import torch
+    from project_b200 import _lib
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    med = mpi_argon('single')
+    sol = ERK43IP_UPPE_3D_Optimized(x, y, t, med, precision='single', device=dev)
+    lib, s = sol._lib, _lib.stream_ptr()
+    npts = NX * NY * NT
+    sol.set_field(A_dev)
+    _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'begin')
+    ms_pos, _ = run_chunks(sol, 10 ** 6, 4, stop=lambda r: r.z >= Z_ION_TIMED)
+    ms_w, _ = run_chunks(sol, args.warmup, args.warmup)
+    r0 = sol.result()
+    lines0 = line_stats(sol, med)
+    ms_t, r1 = run_chunks(sol, args.steps, args.steps)
+    lines1 = line_stats(sol, med)
+    agg = profile_kernels(sol, lib)
+    ms_rest, r2 = run_chunks(sol, 10 ** 7, 16)
+    d = sol.diagnostics()
+    prof = {k: v[0] / 3 for k, v in agg.items()}
+    total_ms = ms_pos + ms_w + ms_t + ms_rest + sum(v[0] for v in agg.values())
+    del sol
+    torch.cuda.empty_cache()
+    return {'table': 'multiphoton sigma_K I^K, K = 11, sigma_K = 1e-188 m^22/W^11/s (reference media_physics.py)',
+            'timed': {'attempts': int(r1.attempts - r0.attempts), 'accepted': int(r1.accepted - r0.accepted),
+                      'z_m': [r0.z, r1.z], 'ms_per_attempt': ms_t / max(r1.attempts - r0.attempts, 1),
+                      'value': npts * (r1.attempts - r0.attempts) / (ms_t / 1e3), 'unit': 'pt-steps/s',
+                      'lines_at_start': lines0, 'lines_at_end': lines1},
+            'kernel_ms_per_attempt': prof,
+            'full_run': {'device_s': total_ms / 1e3, 'attempts': int(r2.attempts), 'accepted': int(r2.accepted),
+                         'z_m': r2.z, 'status': int(r2.status), 'value': npts * r2.attempts / (total_ms / 1e3),
+                         'unit': 'pt-steps/s', 'energy_J': d['energy'], 'photons': d['photons'],
+                         'peak_ionization': d['peak_ionization'],
+                         'note': 'includes 3 attempts run launch by launch for the kernel split'}}
+
+
+def plan_tuning(sol):
+    """The launch configuration the plan's tuner picked, with the candidates' times."""
+    import ctypes
+    from project_b200 import _lib
+    cfg = (ctypes.c_int * 5)()
+    ms = (ctypes.c_float * 8)()
+    _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
+    names = ['tma 2/SM', 'tma 1/SM', 'tma late 3/SM', 'tma late 2/SM']
+    return {'y_pass': ('plain' if not cfg[0] else f"tma{' late' if cfg[2] else ''} {cfg[1]}/SM"),
+            't_lines_per_block': cfg[3], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[4]],
+            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:4]) if v > 0},
+            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[5:7]) if v > 0}}
+
+
 def run_b200(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -429,17 +764,30 @@ def run_b200(args, rank, world, local_rank):
     sol = ERK43IP_UPPE_3D_Optimized(x, y, t, med, precision=prec, device=dev)
     lib = sol._lib
     A_dev = torch.from_numpy(A0).to(dev)
-    sol.set_field(A_dev)
     s = _lib.stream_ptr()
+    npts = NX * NY * NT
+    tuning = plan_tuning(sol)
+
+    # (1) the timed attempts: position the run at the collapse (untimed), warm up, time K
+    want_acc = rank == 0 and prec == 'single' and not args.no_accuracy
+    sol.set_field(A_dev)
     _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'begin')
+    early = {}
+    r20 = run_chunks(sol, 10 ** 6, 1, stop=lambda r: r.accepted >= 20)[1]
+    if want_acc:
+        early[int(r20.accepted)] = sol.field().clone()       # the first 20 steps from z = 0
+    rpre = run_chunks(sol, 10 ** 6, 4, stop=lambda r: r.z >= Z_TIMED)[1]
+    if want_acc:
+        early[int(rpre.accepted)] = sol.field().clone()      # the onset of the collapse
     _lib.check(lib.uppe3d_run_steps(sol._plan, args.warmup, s), 'warmup')
     torch.cuda.synchronize()
     r0 = sol.result()
+    lines0 = line_stats(sol, med)
     if world > 1:
         dist.barrier()
     clocks = ClockSampler(local_rank)
     clocks.start()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    ev0, ev1 = _events()
     torch.cuda.synchronize()
     if world > 1:
         dist.barrier()
@@ -454,14 +802,18 @@ def run_b200(args, rank, world, local_rank):
     r1 = sol.result()
     attempts = r1.attempts - r0.attempts
     accepted = r1.accepted - r0.accepted
+    if attempts != args.steps:
+        raise RuntimeError(f'the run ended inside the timed window ({attempts} of {args.steps} attempts)')
+    state_T = sol.field().clone() if want_acc else None
+    a_T = int(r1.accepted)
+    lines1 = line_stats(sol, med)
     ms_t = torch.tensor([ms], device=dev, dtype=torch.float64)
     if world > 1:
         dist.all_reduce(ms_t, op=dist.ReduceOp.MAX)
     ms_max = float(ms_t.item())
-    npts = NX * NY * NT
     value = npts * args.steps * world / (ms_max / 1e3)
 
-    # per-kernel roofline (CUDA events around each launch of whole attempts)
+    # per-kernel roofline (CUDA events around each launch of 3 attempts at this state)
     agg = profile_kernels(sol, lib)
     peak, peak_kind = peaks()
     dom = max((k for k in agg if k != 'scalar'), key=lambda k: agg[k][0])
@@ -476,17 +828,25 @@ def run_b200(args, rank, world, local_rank):
     step_bytes = 64.0 * (8 if prec == 'single' else 16) * npts     # 64 s N per attempt
     step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
 
-    # e2e: public API call with host buffers (pinned), copies inside the timed region
-    e2e_attempts = 8
+    # (2) the whole 2 m propagation on the device, with the accepted steps logged
+    hlog = torch.zeros(1 << 16, dtype=torch.float64, device=dev)
+    full = full_run(sol, A_dev, hlog)
+    steps = hlog[:full['accepted']].cpu().numpy()
+    final64 = sol.field().clone() if want_acc else None
+    full['lines_at_timed_start'] = lines0
+    full['lines_at_timed_end'] = lines1
+
+    # (3) e2e: the public propagate() call with pinned host buffers, the whole 2 m run;
+    # one host->device copy of A0 and one device->host copy of the spectrum per call
     A_host = torch.from_numpy(A0).pin_memory()
     out_host = torch.empty(A_host.shape, dtype=A_host.dtype).pin_memory()
-    sol.propagate(A_host, L_PROP, tol=TOL, max_attempts=e2e_attempts, out=out_host)  # warm
+    sol.propagate(A_host, L_PROP, tol=TOL, out=out_host)      # warm
     torch.cuda.synchronize()
-    reps = 3
+    reps = 2
     t0 = time.perf_counter()
     done = 0
     for _ in range(reps):
-        sol.propagate(A_host, L_PROP, tol=TOL, max_attempts=e2e_attempts, out=out_host)
+        sol.propagate(A_host, L_PROP, tol=TOL, out=out_host)
         done += sol.last_result.attempts
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
@@ -494,7 +854,25 @@ def run_b200(args, rank, world, local_rank):
     if world > 1:
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_v = npts * done * world / float(e2e_t.item())
+    per_call = done / reps
     fbytes = A0.nbytes
+
+    accuracy = None
+    if want_acc:
+        try:
+            accuracy = accuracy_config1(sol, x, y, t, A0, steps, a_T, state_T, final64, dev, early)
+        except Exception as e:   # reported, never fatal
+            accuracy = {'error': str(e)[:300]}
+        del state_T, final64
+        early.clear()
+        torch.cuda.empty_cache()
+
+    ionising = None
+    if rank == 0 and not args.no_ionising:
+        try:
+            ionising = run_ionising(args, x, y, t, A_dev, dev)
+        except Exception as e:   # reported, never fatal
+            ionising = {'error': str(e)[:300]}
 
     plain = None
     if rank == 0 and not args.no_plain_gpu:
@@ -509,7 +887,7 @@ def run_b200(args, rank, world, local_rank):
         cpu = cpu_baseline(prec)
     b1d = None
     if not args.no_batched_1d:
-        b1d = run_batched1d(dev, rank, world)
+        b1d = run_batched1d(dev, rank, world, accuracy=want_acc)
         if rank == 0 and world == 1 and not args.no_cpu_baseline:
             b1d['cpu_baseline'] = cpu_baseline_1d()
 
@@ -522,7 +900,7 @@ def run_b200(args, rank, world, local_rank):
     grads = None
     if rank == 0 and not args.no_gradients:
         try:
-            grads = run_gradients(dev)
+            grads = run_gradients(dev, accuracy=want_acc)
         except Exception as e:   # reported, never fatal
             grads = {'error': str(e)[:300]}
 
@@ -532,14 +910,14 @@ def run_b200(args, rank, world, local_rank):
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': ms_max / args.steps,
             'higher_is_better': True, 'scaling': 'weak', 'vs_baseline': None,
             'dtype': 'c64' if prec == 'single' else 'c128', 'data': 'synthetic',
-            'config': {'workload': '3+1D UPPE envelope ERK4(3)-IP step, argon 1 bar, ADK + plasma, '
-                                   'self-steepening, 256x256x512, 6 mm x 400 fs, 2 mJ 40 fs, w0 1 mm, '
-                                   '1% speckle, L 2 m, tol 1e-5',
+            'config': {'workload': CONFIG_WORKLOAD,
                        'grid': [NX, NY, NT], 'precision': prec,
                        'mixed_precision': 'complex64 bulk; FP64 phase (mod 2pi), density scan, '
                                           'error norm, controller' if prec == 'single' else None,
+                       'timed_window': f'attempts {int(r0.attempts)}..{int(r1.attempts)} of the 2 m run, '
+                                       f'z = {r0.z:.4f} -> {r1.z:.4f} m (collapse onset)',
                        'attempts_timed': attempts, 'accepted_timed': accepted,
-                       'z_after_timed_m': r1.z, 'parallelism': f'replicas x{world}',
+                       'parallelism': f'replicas x{world}',
                        'l2': 'every field (268 MB c64) exceeds the 126 MB L2; no flush'},
             'roofline': {'bound': 'hbm', 'kernel': dom, 'achieved': achieved, 'peak': peak,
                          'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
@@ -549,11 +927,17 @@ def run_b200(args, rank, world, local_rank):
             'roofline_step': {'model': '64*s*N bytes per attempt', 'achieved': step_achieved,
                               'peak': peak, 'unit': 'GB/s', 'frac': step_achieved / peak},
             'kernel_ms_per_attempt': {k: v[0] / 3 for k, v in agg.items()},
+            'tuning': tuning,
+            'config1_full': full,
+            'accuracy': accuracy,
+            'ionising': ionising,
             'cpu_baseline': cpu,
-            'e2e': {'value': e2e_v, 'unit': 'pt-steps/s', 'h2d_bytes_per_step': fbytes,
-                    'd2h_bytes_per_step': fbytes,
-                    'how': f'propagate(host pinned A0) over {e2e_attempts} attempts per call, '
-                           'spectrum copied back to pinned host memory'},
+            'e2e': {'value': e2e_v, 'unit': 'pt-steps/s',
+                    'h2d_bytes_per_step': fbytes / per_call, 'd2h_bytes_per_step': fbytes / per_call,
+                    'h2d_bytes_per_call': fbytes, 'd2h_bytes_per_call': fbytes,
+                    'attempts_per_call': per_call, 'seconds_per_call': e2e_s / reps,
+                    'how': 'propagate(host pinned A0, L = 2 m) -> spectrum in pinned host memory: one '
+                           'call is the whole configured run; bytes per step = bytes per call / attempts'},
             'plain_gpu': plain,
             'batched_1d': b1d,
             'gradients': grads,
@@ -601,6 +985,8 @@ def main():
     ap.add_argument('--no-batched-1d', action='store_true')
     ap.add_argument('--no-gradients', action='store_true')
     ap.add_argument('--no-realfield', action='store_true')
+    ap.add_argument('--no-accuracy', action='store_true')
+    ap.add_argument('--no-ionising', action='store_true')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
     args = ap.parse_args()

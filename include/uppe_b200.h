@@ -31,6 +31,8 @@ enum {
   UPPE_STATUS_NONFINITE = 1,     /* error or step size became NaN/inf: stopped   */
   UPPE_STATUS_MIN_STEP = 2,      /* a step was forced at min_step with err > tol */
   UPPE_STATUS_MAX_ATTEMPTS = 4,  /* attempt budget exhausted before z = L         */
+  UPPE_STATUS_RETRIED = 64,      /* an attempt came out non-finite and was retried with
+                                    a tenth of the step (the reference loops on h = NaN) */
   UPPE_STATUS_DEVICE_WAIT = 32   /* a bounded device wait ran out: run stopped     */
 };
 
@@ -127,7 +129,9 @@ int uppe3d_get_field(uppe3d_plan* plan, void* out, uppe_stream_t stream);
  * erk43ip_method.py:288-369).  Many instances with different Nt and parameters
  * run in one persistent launch. */
 typedef struct {
-  int Nt;                  /* power of two: [64,16384] complex64, [64,8192] complex128 */
+  int Nt;                  /* power of two: [64,16384]; complex128 above 8192 only when
+                              every line of the plan is 2048..16384 points, without Raman
+                              or history (the four-CTA cluster kernel)                 */
   double dt;               /* t[1]-t[0]                                                */
   double L, tol, max_step, min_step;   /* propagate() arguments (:288)                */
   long long max_attempts;  /* <= 0: UPPE_DEFAULT_MAX_ATTEMPTS                          */
@@ -138,6 +142,7 @@ typedef struct {
   double Ui, sigma_drude, omega0_tau_c, rate_rec, rho_nt, ava_coef;   /* plasma constants */
   int hist_cap;            /* history slots (the reference saves <= 1501); 0 = none   */
   double omega0;           /* carrier angular frequency (photon number; 0: not computed) */
+  double cost;             /* expected cost for the work queue (longest first); <= 0: Nt L */
 } uppe1d_inst_desc;
 
 typedef struct {
@@ -265,6 +270,25 @@ int uppe_rf_spec_bins(const uppe_rf_plan* plan);
 int uppe_spectrum_field(const double* breaks, const double* coef, int nb, int Nt, double dt, double f0,
                         double gdd, double tod, void* out, uppe_stream_t stream);
 
+/* One complex128 line transform on the device, N a power of two (2 .. 2^24):
+ * out = scale * fftshift?(F(ifftshift?(in))) with F the forward (dir = -1) or
+ * unnormalised inverse (dir = +1) DFT; shift_in / shift_out apply the
+ * half-length rotations.  work: device, 2 N complex128; in may equal out.  The
+ * numpy fft/ifft/fftshift calls of the reference's pulse builders
+ * (erk43ip_method.py:415-429, 750-753). */
+int uppe_fft_c128(const void* in, void* out, void* work, int N, int dir, double scale, int shift_in,
+                  int shift_out, uppe_stream_t stream);
+/* field (device complex128 [N], fft order) *= exp(i (gdd w^2/2 + tod w^3/6)), w = 2 pi
+ * fftfreq(N, dt): the dispersion phase of generate_dispersed_pulse
+ * (erk43ip_method.py:417-421). */
+int uppe_spectral_phase(void* field, int N, double dt, double gdd, double tod, uppe_stream_t stream);
+/* The direct Fourier sum of _exact_fourier_transform (erk43ip_method.py:583-596):
+ * out[(i + Nt/2) mod Nt] = sum_k amp[k] exp(-i omega[k] t[i]) (the sum then the
+ * fftshift), with amp[k] = Simpson weight x sqrt(S_k) x exp(i phase_k) on the dense
+ * frequency grid (device arrays; amp complex128). */
+int uppe_exact_ft(const double* t, int Nt, const double* omega, const void* amp, int Nf, void* out,
+                  uppe_stream_t stream);
+
 /* Workspace of uppe1d_adjoint, in complex128 elements. */
 long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K);
 /* Reverse-mode derivative of one instance's frozen-schedule propagation (complex128
@@ -291,9 +315,11 @@ int uppe1d_adjoint(uppe1d_plan* plan, int inst, const double* hlog, int nsteps, 
  * time domain).  The per-call device state lives in one static device array of
  * UPPE_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until exit;
  * Nt above UPPE_NOALLOC_MAX_NT_C64 / _C128 is rejected with UPPE_ERR_SIZE, and
- * hist_cap must be 0.  The first call on a device looks up the array's address
- * (make it before any stream capture).  Calls share the array: calls that overlap
- * on the GPU race.  Synchronises the stream when result is not NULL. */
+ * hist_cap must be 0.  The ionisation grid must increase; its ends are read on
+ * the device.  The first call on a device looks up the array's address (make it
+ * before any stream capture).  Calls share the array: calls that overlap on the
+ * GPU race.  Synchronises the stream only when result is not NULL (to copy the
+ * result record back). */
 #define UPPE_NOALLOC_MAX_NT_C64 16384
 #define UPPE_NOALLOC_MAX_NT_C128 8192
 #define UPPE_NOALLOC_SCRATCH_BYTES (1024ull + 9ull * UPPE_NOALLOC_MAX_NT_C128 * 16ull)
@@ -345,6 +371,31 @@ long long uppe3d_adjoint_work_bytes(const uppe3d_plan* plan, int nsteps, int K);
  * segments.  Overwrites the plan's state.  No reference counterpart. */
 int uppe3d_adjoint(uppe3d_plan* plan, const double* hlog_host, int nsteps, int K, const void* A0,
                    const void* Zbar, void* A0bar, void* work, uppe_stream_t stream);
+
+/* Line transform along t of a device field of the plan's grid and precision:
+ * out = scale * fft_t(in) for dir = -1, out = scale * (unnormalised inverse) for
+ * dir = +1; in and out may be the same buffer.  The reference applies cuFFT's
+ * fft/ifft along t (solver_3d.py:101, 155, 216); this is the same transform with
+ * the plan's own kernel, e.g. for the cotangent of a differentiable objective. */
+int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, double scale,
+                       uppe_stream_t stream);
+
+/* Launch configuration chosen for the plan's shape by the tuner that runs in
+ * uppe3d_plan_create (no reference counterpart: the reference leaves kernel
+ * choice to cuFFT).  Candidates: y passes on the TMA-fed kernel (stage operands
+ * loaded before the tile's wait with 1 or 2 CTAs per SM, or where they are used
+ * with 3 or 2; complex64 plans with 64 <= Ny <= 256), and 4 or 8 t-lines per
+ * block of the warp t-line kernel.  All candidates compute identical bits (the
+ * plain tile kernel, which rounds differently, serves the other shapes).  cfg5 =
+ * {TMA y passes, CTAs per SM, late operand loads, t-lines per block, 1 timed / 2
+ * from the process cache / 0 defaults (UPPE_TUNE=0)}; ms8 (may be NULL):
+ * per-attempt time of the y passes for the four y candidates [0..3] and of the t
+ * passes for 8 and 4 lines per block [5..6], in ms (0 when not timed). */
+int uppe3d_tuning(const uppe3d_plan* plan, int* cfg5, float* ms8);
+/* Force a launch configuration (y_tma 0 selects the plain tile kernel; y_ctas
+ * 1..3, t_wpb 4 or 8) and re-capture the attempt graphs; for comparing the
+ * candidates. */
+int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int t_wpb);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);

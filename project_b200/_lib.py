@@ -13,7 +13,9 @@ LIB_PATH = os.path.join(_HERE, 'libuppe_b200.so')
 _lib = None
 
 UPPE_C64, UPPE_C128 = 0, 1
-STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS = 1, 2, 4
+STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS, STATUS_RETRIED = 1, 2, 4, 64
+# line limits of uppe1d_propagate_noalloc (its static device array)
+UPPE_NOALLOC_MAX_NT_C64, UPPE_NOALLOC_MAX_NT_C128 = 16384, 8192
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -40,7 +42,7 @@ class InstDesc1D(ctypes.Structure):
                 ('min_step', _D), ('max_attempts', _LL), ('raman', _I), ('plasma', _I),
                 ('f_R', _D), ('A_eff', _D), ('Ui', _D), ('sigma_drude', _D),
                 ('omega0_tau_c', _D), ('rate_rec', _D), ('rho_nt', _D), ('ava_coef', _D),
-                ('hist_cap', _I), ('omega0', _D)]
+                ('hist_cap', _I), ('omega0', _D), ('cost', _D)]
 
 
 class Desc1D(ctypes.Structure):
@@ -113,6 +115,12 @@ SIGNATURES = {
     'uppe1d_adjoint': (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     'uppe1d_propagate_noalloc': (_I, [ctypes.POINTER(InstDesc1D), _I, _P, _P, _P, _I, _P, _P, _P,
                                       ctypes.POINTER(Result1D), _P]),
+    'uppe_fft_c128': (_I, [_P, _P, _P, _I, _I, _D, _I, _I, _P]),
+    'uppe_spectral_phase': (_I, [_P, _I, _D, _D, _D, _P]),
+    'uppe_exact_ft': (_I, [_P, _I, _P, _P, _I, _P, _P]),
+    'uppe3d_transform_t': (_I, [_P, _P, _P, _I, _D, _P]),
+    'uppe3d_tuning': (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
+    'uppe3d_set_tuning': (_I, [_P, _I, _I, _I, _I]),
     'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),
                                     ctypes.POINTER(_D), ctypes.POINTER(_I), _P]),
 }

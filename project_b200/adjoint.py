@@ -225,7 +225,11 @@ class Propagate3D(torch.autograd.Function):
         lib = _lib.load()
         Nt = sol.Nt
         A_scale = float(A0.abs().max())
-        Zbar = (torch.fft.fft(gA.to(sol.complex_dtype), dim=-1) * (A_scale / Nt)).contiguous()
+        # Zbar = fft_t(gA) * A_scale / Nt with the plan's own t-line transform
+        Zbar = gA.to(sol.complex_dtype).contiguous().clone()
+        _lib.check(lib.uppe3d_transform_t(sol._plan, ctypes.c_void_p(Zbar.data_ptr()),
+                                          ctypes.c_void_p(Zbar.data_ptr()), -1, A_scale / Nt,
+                                          _lib.stream_ptr()), 'uppe3d_transform_t')
         nb = lib.uppe3d_adjoint_work_bytes(sol._plan, len(ctx.steps), ctx.K)
         work = torch.empty(nb, dtype=torch.uint8, device=A0.device)
         A0bar = torch.empty_like(A0)

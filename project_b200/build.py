@@ -8,8 +8,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, 'csrc')
 BUILD = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libuppe_b200.so')
-SOURCES = ['uppe3d.cu', 'uppe1d.cu', 'uppe1d_f32.cu', 'uppe1d_f64.cu', 'uppe1d_noalloc.cu']
-HEADERS = ['common.cuh', 'uppe1d_kernel.cuh']
+SOURCES = ['uppe3d.cu', 'uppe1d.cu', 'uppe1d_f32.cu', 'uppe1d_f64.cu', 'uppe1d_noalloc.cu', 'uppe1d_cl_f32.cu',
+           'uppe1d_cl_f64.cu']
+HEADERS = ['common.cuh', 'uppe1d_kernel.cuh', 'uppe1d_cluster.cuh']
 NVCC_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '-std=c++17',
               '-Xcompiler', '-fPIC', '-Xcompiler', '-O2']
 
@@ -36,6 +37,35 @@ def up_to_date():
     return all(os.path.getmtime(f) <= t for f in _deps())
 
 
+def _includes(path, seen=None):
+    """The source file and the local headers it includes, recursively."""
+    seen = set() if seen is None else seen
+    if path in seen or not os.path.exists(path):
+        return seen
+    seen.add(path)
+    with open(path) as f:
+        for line in f:
+            line = line.strip()
+            if line.startswith('#include "'):
+                name = line.split('"')[1]
+                for d in (os.path.dirname(path), os.path.join(os.path.dirname(HERE), 'include')):
+                    q = os.path.normpath(os.path.join(d, name))
+                    if os.path.exists(q):
+                        _includes(q, seen)
+                        break
+    return seen
+
+
+def _object_current(src, obj):
+    """An object is current when it is newer than its source, the headers that
+    source includes and this build script."""
+    if not os.path.exists(obj):
+        return False
+    t = os.path.getmtime(obj)
+    deps = _includes(os.path.join(CSRC, src)) | {os.path.abspath(__file__)}
+    return all(os.path.getmtime(f) <= t for f in deps)
+
+
 def build(force=False, verbose=False):
     if not force and up_to_date():
         return LIB
@@ -45,6 +75,8 @@ def build(force=False, verbose=False):
 
     def compile_one(src):
         obj = os.path.join(BUILD, src.replace('.cu', '.o'))
+        if not force and _object_current(src, obj):
+            return obj
         cmd = [nvcc] + NVCC_FLAGS + ['-c', os.path.join(CSRC, src), '-o', obj]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:

@@ -170,6 +170,23 @@ __device__ __forceinline__ void stockham(C* s, const C* tw, int tid, IDX idx, SY
   }
 }
 
+// exp(i ph) in FP32 from an FP64 phase: ph = q pi/2 + f with q = rint(2 ph / pi)
+// and |f| <= pi/4 formed in FP64, f rounded to FP32 (absolute error <= 2^-25 rad
+// there, against ~1.2e-7 for an argument near pi), sincosf of f, then the exact
+// rotation by i^q.  The mixed-precision interaction-picture factors use it.
+__device__ __forceinline__ float2 cis_quadrant(double ph) {
+  const double q = rint(ph * 0.63661977236758134308);
+  const double f = fma(-q, 1.5707963267948966192, ph);
+  float s, c;
+  sincosf((float)f, &s, &c);
+  switch ((int)((long long)q & 3)) {
+    case 0: return make_float2(c, s);
+    case 1: return make_float2(-s, c);
+    case 2: return make_float2(-c, -s);
+    default: return make_float2(s, -c);
+  }
+}
+
 // Non-negative double -> order-preserving 64-bit key for atomicMax (NaN > +inf).
 __device__ __forceinline__ unsigned long long dkey(double v) {
   return (unsigned long long)__double_as_longlong(v);

@@ -8,7 +8,7 @@
 #include <numeric>
 #include <vector>
 
-#include "uppe1d_kernel.cuh"
+#include "uppe1d_cluster.cuh"
 
 extern char g_uppe_err[512];
 
@@ -25,6 +25,9 @@ struct uppe1d_plan {
   int nblocks;
   int nsm;
   size_t smem;
+  bool use_cl = false;    // lines run on four-CTA clusters (uppe1d_cluster.cuh)
+  int ncl = 0;            // clusters of the persistent cluster launch
+  size_t cl_smem = 0;
   Batch1D b;
   Inst1D* d_inst;
   std::vector<Inst1D> h_inst;
@@ -71,7 +74,7 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   if (!d || d->n_inst <= 0 || !d->inst || !d->D || !d->G) return UPPE_ERR_ARG;
   if (d->precision != UPPE_C64 && d->precision != UPPE_C128) return UPPE_ERR_ARG;
   const int dbl = d->precision == UPPE_C128;
-  const int nmax_allowed = dbl ? 8192 : 16384;
+  const int nmax_allowed = 16384;   // complex128 beyond 8192 only on the cluster kernel (below)
   uppe1d_plan* p = new uppe1d_plan();
   p->dbl = dbl;
   p->csz = dbl ? 16 : 8;
@@ -115,6 +118,27 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     nmax = std::max(nmax, n);
   }
   if (any_raman && !d->H) { delete p; return UPPE_ERR_ARG; }
+  // The cluster kernel serves plans whose lines are all 2048..16384 points without
+  // Raman or history and at least one of them long (>= 8192): one line then runs
+  // on four SMs.  UPPE_1D_CLUSTER=0 keeps the single-CTA kernel where it can serve.
+  {
+    bool ok = true, longer = false;
+    for (int i = 0; i < d->n_inst; ++i) {
+      const uppe1d_inst_desc& s = d->inst[i];
+      if (s.raman || s.hist_cap > 0 || s.Nt < 2048) ok = false;
+      if (s.Nt >= 8192) longer = true;
+    }
+    const char* env = getenv("UPPE_1D_CLUSTER");
+    const bool off = env && env[0] == '0';
+    p->use_cl = ok && longer && !(off && !(dbl && nmax > 8192));
+    if (dbl && nmax > 8192 && !p->use_cl) {
+      snprintf(g_uppe_err, sizeof(g_uppe_err),
+               "complex128 lines of %d points run on the cluster kernel, which needs every line of the "
+               "plan in [2048, 16384] points without Raman or history", nmax);
+      delete p;
+      return UPPE_ERR_SIZE;
+    }
+  }
   for (int i = 0; i < d->n_inst; ++i)
     if (d->inst[i].plasma && (d->lut_n < 2 || !d->lut_log10I || !d->lut_W)) { delete p; return UPPE_ERR_ARG; }
   p->ftotal = off; p->htotal = hoff; p->zhtotal = zoff; p->nmax = nmax;
@@ -130,7 +154,8 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   std::vector<int> order(p->ninst);
   std::iota(order.begin(), order.end(), 0);
   std::stable_sort(order.begin(), order.end(), [&](int a, int b2) {
-    const double ca = (double)p->h_inst[a].Nt * p->h_inst[a].L, cb = (double)p->h_inst[b2].Nt * p->h_inst[b2].L;
+    const double ca = d->inst[a].cost > 0.0 ? d->inst[a].cost : (double)p->h_inst[a].Nt * p->h_inst[a].L;
+    const double cb = d->inst[b2].cost > 0.0 ? d->inst[b2].cost : (double)p->h_inst[b2].Nt * p->h_inst[b2].L;
     return ca > cb;
   });
   TRY1(up1(p, &ptr, order.data(), sizeof(int) * p->ninst)); p->b.order = (const int*)ptr;
@@ -196,9 +221,42 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   p->smem = p->csz * (size_t)(nmax + nmax / 32) + sizeof(double) * (64 + T1);
   p->b.inst = p->d_inst;
   p->b.ninst = p->ninst;
+  p->b.xtw = nullptr;
+  p->b.cl_scratch = nullptr;
+  p->b.cl_scratch_bytes = 0;
+  if (p->use_cl) {
+    // cross-CTA twiddles W_N^(m r) (r = 1..3, m < M = N/4) for M = 512 .. nmax/4
+    const int mmax = nmax / kCS;
+    std::vector<unsigned char> xt(p->csz * (size_t)(cl_xtw_offset(mmax) + 3LL * mmax));
+    for (int M = 512; M <= mmax; M *= 2) {
+      const long long o = cl_xtw_offset(M);
+      for (int r = 1; r < kCS; ++r)
+        for (int m = 0; m < M; ++m) {
+          const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * r) /
+                                  (long double)(kCS * M);
+          const double cr = (double)cosl(ang), ci = (double)sinl(ang);
+          const long long e = o + (long long)(r - 1) * M + m;
+          if (dbl) ((double2*)xt.data())[e] = make_double2(cr, ci);
+          else ((float2*)xt.data())[e] = make_float2((float)cr, (float)ci);
+        }
+    }
+    TRY1(up1(p, &ptr, xt.data(), xt.size())); p->b.xtw = ptr;
+    p->cl_smem = dbl ? cl_smem<double>(nmax) : cl_smem<float>(nmax);
+    const int maxcl = dbl ? uppe1d_cl_max_clusters<double>(p->cl_smem) : uppe1d_cl_max_clusters<float>(p->cl_smem);
+    p->ncl = std::min(p->ninst, maxcl > 0 ? maxcl : nsm / kCS);
+    p->b.cl_scratch_bytes = (long long)(dbl ? cl_scratch_bytes<double>(nmax) : cl_scratch_bytes<float>(nmax));
+    TRY1(up1(p, &ptr, nullptr, (size_t)p->b.cl_scratch_bytes * p->ncl)); p->b.cl_scratch = ptr;
+  }
 #undef TRY1
   *out = p;
   return 0;
+}
+
+// the propagation kernel of the plan: four-CTA clusters per line, or one CTA per line
+static cudaError_t launch_lines(const uppe1d_plan* p, const Batch1D& b, cudaStream_t s) {
+  if (p->use_cl)
+    return p->dbl ? launch_uppe1d_cl<double>(b, p->ncl, p->cl_smem, s) : launch_uppe1d_cl<float>(b, p->ncl, p->cl_smem, s);
+  return p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s) : launch_uppe1d<float>(b, p->nblocks, p->smem, s);
 }
 
 extern "C" long long uppe1d_field_elems(const uppe1d_plan* p) { return p ? p->ftotal : 0; }
@@ -217,8 +275,7 @@ extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double*
   b.hist = hist;
   b.zhist = zhist;
   UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
-  UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s)
-                   : launch_uppe1d<float>(b, p->nblocks, p->smem, s));
+  UPPE1_CK(launch_lines(p, b, s));
   if (results) {
     UPPE1_CK(cudaMemcpyAsync(p->h_res, p->b.res, sizeof(Res1D) * p->ninst, cudaMemcpyDeviceToHost, s));
     UPPE1_CK(cudaStreamSynchronize(s));
@@ -236,8 +293,7 @@ extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double*
 // ---- step log, replay and adjoint ------------------------------------------
 static int run1(uppe1d_plan* p, Batch1D& b, uppe1d_result* results, cudaStream_t s) {
   UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
-  UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s)
-                   : launch_uppe1d<float>(b, p->nblocks, p->smem, s));
+  UPPE1_CK(launch_lines(p, b, s));
   if (results) {
     UPPE1_CK(cudaMemcpyAsync(p->h_res, p->b.res, sizeof(Res1D) * p->ninst, cudaMemcpyDeviceToHost, s));
     UPPE1_CK(cudaStreamSynchronize(s));
@@ -301,6 +357,7 @@ extern "C" int uppe1d_run_programs(uppe1d_plan* p, int nprog, const long long* o
       if (u.inst >= 0) {
         const Inst1D& in = p->h_inst[u.inst];
         if (in.hist_cap > 0) return prog_fail("program instances must have hist_cap = 0");
+        if (p->dbl && in.Nt > 8192) return prog_fail("complex128 programs take lines of at most 8192 points");
         if (g.Nt == 0) { g.Nt = in.Nt; g.log2n = in.log2n; g.dt = in.dt; }
         else if (in.Nt != g.Nt || in.dt != g.dt)
           return prog_fail("the propagations of one program must share Nt and dt");
@@ -410,6 +467,10 @@ extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int 
     return UPPE_ERR_ARG;
   }
   const Inst1D& q = p->h_inst[inst];
+  if (q.Nt > 8192) {
+    snprintf(g_uppe_err, sizeof(g_uppe_err), "uppe1d_adjoint: lines of at most 8192 points");
+    return UPPE_ERR_SIZE;
+  }
   if (q.raman || (q.plasma && q.pc.ava != 0.0)) {
     snprintf(g_uppe_err, sizeof(g_uppe_err),
              "uppe1d_adjoint: the Raman response and avalanche ionisation have no adjoint here");
@@ -478,6 +539,125 @@ extern "C" int uppe_spectrum_field(const double* breaks, const double* coef, int
   const int threads = 256;
   const int blocks = (Nt + threads - 1) / threads < 1024 ? (Nt + threads - 1) / threads : 1024;
   k_spectrum_field<<<blocks, threads, 0, s>>>(breaks, coef, nb, Nt, dt, f0, gdd, tod, (double2*)out);
+  UPPE1_CK(cudaGetLastError());
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Input-pulse utilities on the device (the reference does these on the host with
+// numpy/scipy: erk43ip_method.py:383-446, 492-598, 599-764).
+//
+// uppe_fft_c128: one complex128 line of N = 2^m points, radix-2 Stockham
+// autosort passes in global memory (pass with half-length m and stride s:
+// y[q + s 2p] = a + b, y[q + s (2p+1)] = (a - b) W_n^p, a = x[q + s p],
+// b = x[q + s (p + m)]), twiddles from sincospi in FP64.  Optional input
+// rotation by N/2 (ifftshift) in the first pass and output rotation (fftshift)
+// with a scale in the last.  Input pulses are built once per run, so a simple
+// bandwidth-light formulation serves; the propagators never call it.
+// ---------------------------------------------------------------------------
+namespace uppe {
+__global__ void k_fft_pass(const double2* __restrict__ x, double2* __restrict__ y, int N, int n, int s,
+                           int dir, int shift_in) {
+  const int half = N / 2, m = n / 2;
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < half; t += gridDim.x * blockDim.x) {
+    const int p = t / s, q = t % s;
+    int ia = q + s * p, ib = q + s * (p + m);
+    if (shift_in) { ia = (ia + half) & (N - 1); ib = (ib + half) & (N - 1); }
+    const double2 a = x[ia], b = x[ib];
+    double sn, cs;
+    sincospi((double)dir * 2.0 * (double)p / (double)n, &sn, &cs);
+    const double dr = a.x - b.x, di = a.y - b.y;
+    y[q + s * (2 * p)] = make_double2(a.x + b.x, a.y + b.y);
+    y[q + s * (2 * p + 1)] = make_double2(dr * cs - di * sn, dr * sn + di * cs);
+  }
+}
+
+__global__ void k_fft_out(const double2* __restrict__ x, double2* __restrict__ out, int N, double scale,
+                          int shift_out) {
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < N; i += gridDim.x * blockDim.x) {
+    const double2 v = x[i];
+    out[shift_out ? (i + N / 2) & (N - 1) : i] = make_double2(v.x * scale, v.y * scale);
+  }
+}
+
+// field[k] *= exp(i (gdd w^2 / 2 + tod w^3 / 6)), w = 2 pi fftfreq(N, dt)[k]
+__global__ void k_spectral_phase(double2* f, int n, double dt, double gdd, double tod) {
+  const double val = 1.0 / (n * dt);
+  const double twopi = 6.283185307179586476925286766559;
+  for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < n; k += gridDim.x * blockDim.x) {
+    const double w = twopi * ((k < (n + 1) / 2 ? k : k - n) * val);
+    double sn, cs;
+    sincos(0.5 * gdd * w * w + (1.0 / 6.0) * tod * w * w * w, &sn, &cs);
+    const double2 v = f[k];
+    f[k] = make_double2(v.x * cs - v.y * sn, v.x * sn + v.y * cs);
+  }
+}
+
+// Direct (non-uniform) Fourier sum of the exact-transform path: one block per
+// output time, a fixed-order block reduction (deterministic).
+constexpr int kEftThreads = 256;
+__global__ void __launch_bounds__(kEftThreads) k_exact_ft(const double* __restrict__ t, int Nt,
+                                                          const double* __restrict__ om,
+                                                          const double2* __restrict__ a, int Nf,
+                                                          double2* __restrict__ out) {
+  __shared__ double sr[kEftThreads], si[kEftThreads];
+  for (int i = blockIdx.x; i < Nt; i += gridDim.x) {
+    const double ti = t[i];
+    double re = 0.0, im = 0.0;
+    for (int k = threadIdx.x; k < Nf; k += kEftThreads) {
+      double sn, cs;
+      sincos(-om[k] * ti, &sn, &cs);
+      const double2 v = a[k];
+      re += v.x * cs - v.y * sn;
+      im += v.x * sn + v.y * cs;
+    }
+    sr[threadIdx.x] = re;
+    si[threadIdx.x] = im;
+    __syncthreads();
+    for (int o = kEftThreads / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) { sr[threadIdx.x] += sr[threadIdx.x + o]; si[threadIdx.x] += si[threadIdx.x + o]; }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[(i + Nt / 2) % Nt] = make_double2(sr[0], si[0]);   // fftshift
+    __syncthreads();
+  }
+}
+}  // namespace uppe
+
+static int grid_for(long long n) {
+  const long long b = (n + 255) / 256;
+  return (int)(b < 1 ? 1 : (b > 4096 ? 4096 : b));
+}
+
+extern "C" int uppe_fft_c128(const void* in, void* out, void* work, int N, int dir, double scale, int shift_in,
+                             int shift_out, cudaStream_t s) {
+  if (!in || !out || !work || N < 2 || (N & (N - 1)) || N > (1 << 24) || (dir != -1 && dir != 1))
+    return UPPE_ERR_ARG;
+  double2* w[2] = {static_cast<double2*>(work), static_cast<double2*>(work) + N};
+  const double2* src = static_cast<const double2*>(in);
+  int k = 0, si = shift_in;
+  for (int n = N, st = 1; n > 1; n >>= 1, st <<= 1, k ^= 1) {
+    k_fft_pass<<<grid_for(N / 2), 256, 0, s>>>(src, w[k], N, n, st, dir, si);
+    src = w[k];
+    si = 0;
+  }
+  k_fft_out<<<grid_for(N), 256, 0, s>>>(src, static_cast<double2*>(out), N, scale, shift_out);
+  UPPE1_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe_spectral_phase(void* field, int N, double dt, double gdd, double tod, cudaStream_t s) {
+  if (!field || N < 1 || !(dt > 0.0)) return UPPE_ERR_ARG;
+  k_spectral_phase<<<grid_for(N), 256, 0, s>>>(static_cast<double2*>(field), N, dt, gdd, tod);
+  UPPE1_CK(cudaGetLastError());
+  return 0;
+}
+
+extern "C" int uppe_exact_ft(const double* t, int Nt, const double* omega, const void* amp, int Nf, void* out,
+                             cudaStream_t s) {
+  if (!t || !omega || !amp || !out || Nt < 1 || Nf < 1) return UPPE_ERR_ARG;
+  k_exact_ft<<<Nt < 8192 ? Nt : 8192, kEftThreads, 0, s>>>(t, Nt, omega, static_cast<const double2*>(amp), Nf,
+                                                           static_cast<double2*>(out));
   UPPE1_CK(cudaGetLastError());
   return 0;
 }

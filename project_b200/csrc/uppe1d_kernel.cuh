@@ -90,6 +90,9 @@ struct Batch1D {
   const Op1D* ops;
   Res1D* op_res;                 // one result per operation
   void* records;                 // recorded fields (or null)
+  const void* xtw;               // cluster kernel: cross-CTA twiddles W_N^(m r) (or null)
+  void* cl_scratch;              // cluster kernel: per-cluster scratch
+  long long cl_scratch_bytes;
 };
 
 template <int N> struct Cfg1 {
@@ -217,13 +220,9 @@ template <> struct EFac<double> {
 };
 template <> struct EFac<float> {
   __device__ __forceinline__ static float2 get(double2 D, double hh) {
-    double ph = hh * D.y;
-    const double twopi = 6.283185307179586476925286766559;
-    ph = ph - twopi * rint(ph * (1.0 / twopi));
-    float s, c;
-    sincosf((float)ph, &s, &c);
+    const float2 e = cis_quadrant(hh * D.y);
     const float m = expf((float)(hh * D.x));
-    return make_float2(m * c, m * s);
+    return make_float2(m * e.x, m * e.y);
   }
 };
 
@@ -620,8 +619,12 @@ __device__ __forceinline__ void adaptive_run(Ctx1<Rl>& c, const Batch1D& b, int 
     ion_cand = 0.0;
     err = attempt1<Rl, N>(c, h, cand(), &ion_cand);
     attempts += 1;
-    if (!isfinite(err) || !isfinite(h)) { status |= UPPE_STATUS_NONFINITE; break; }
-    if (err < tol) {
+    if (!isfinite(h) || (!isfinite(err) && h <= min_step)) { status |= UPPE_STATUS_NONFINITE; break; }
+    if (!isfinite(err)) {
+      // the attempt overflowed (the state is untouched): retry with a tenth of the step
+      status |= UPPE_STATUS_RETRIED;
+      h = fmax(h * 0.1, min_step);
+    } else if (err < tol) {
       accept(h);
       double factor = 0.95 * pow(tol / (err + 1e-30), 0.25);
       if (err_prev >= 0.0 && err_prev > 1e-30) factor *= pow(err_prev / (err + 1e-30), 0.1);
@@ -689,6 +692,13 @@ __device__ void run_instance(const Batch1D& b, int i, unsigned char* smem) {
   c.H = b.H ? b.H + in.off : nullptr;
   c.in = &in;
   c.lut = b.lut;
+  if (c.lut.n > 1 && c.lut.inv_dx == 0.0) {
+    // a table passed without its grid constants (the allocation-free entry
+    // point): the first-index guess comes from the table's ends, as plans set it
+    const Rl* xp = reinterpret_cast<const Rl*>(c.lut.x);
+    c.lut.x0 = (double)xp[0];
+    c.lut.inv_dx = (c.lut.n - 1) / ((double)xp[c.lut.n - 1] - c.lut.x0);
+  }
   C* field = reinterpret_cast<C*>(b.field) + in.off;
   C* hist = in.hist_cap > 0 ? reinterpret_cast<C*>(b.hist) + in.hist_off : nullptr;
   double* zh = in.hist_cap > 0 ? b.zhist + in.zh_off : nullptr;

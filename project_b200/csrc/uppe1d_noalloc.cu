@@ -63,6 +63,16 @@ __global__ void k_noalloc_twiddles(size_t byte_off, int nmax) {
   }
 }
 
+// Instance record into its slot; the work order (instance 0) and the work-queue
+// counter start at zero on every call.
+__global__ void k_noalloc_header(Inst1D q) {
+  if (blockIdx.x != 0 || threadIdx.x != 0) return;
+  *reinterpret_cast<Inst1D*>(g_noalloc_scratch + kInstOff) = q;
+  int* oc = reinterpret_cast<int*>(g_noalloc_scratch + kOrderOff);
+  oc[0] = 0;
+  oc[1] = 0;
+}
+
 int fail(int code, const char* msg) {
   snprintf(g_uppe_err, sizeof(g_uppe_err), "uppe1d_propagate_noalloc: %s", msg);
   return code;
@@ -140,7 +150,6 @@ extern "C" int uppe1d_propagate_noalloc(const uppe1d_inst_desc* s, int precision
   q.pc.rr = (double)(float)s->rate_rec; q.pc.dt = (double)(float)s->dt;
   q.pc.rho_nt = (double)(float)s->rho_nt; q.pc.ava = s->ava_coef;
   q.omega0 = s->omega0;
-  const int order_counter[2] = {0, 0};   // the work-queue counter must start at zero
 
   Batch1D b;
   memset(&b, 0, sizeof(b));
@@ -162,33 +171,19 @@ extern "C" int uppe1d_propagate_noalloc(const uppe1d_inst_desc* s, int precision
   b.lut.x = b.lut.w = nullptr;
   b.lut.zero_x = -INFINITY;   // no zero-run shortcut: identical results, no host scan
   if (s->plasma) {
-    // only the grid ends are read back, for the kernel's first index guess
-    double x0, x1;
-    if (dbl) {
-      NA_CK(cudaMemcpyAsync(&x0, lut_log10I, 8, cudaMemcpyDeviceToHost, stream));
-      NA_CK(cudaMemcpyAsync(&x1, static_cast<const double*>(lut_log10I) + lut_n - 1, 8,
-                            cudaMemcpyDeviceToHost, stream));
-    } else {
-      float f0, f1;
-      NA_CK(cudaMemcpyAsync(&f0, lut_log10I, 4, cudaMemcpyDeviceToHost, stream));
-      NA_CK(cudaMemcpyAsync(&f1, static_cast<const float*>(lut_log10I) + lut_n - 1, 4,
-                            cudaMemcpyDeviceToHost, stream));
-      NA_CK(cudaStreamSynchronize(stream));
-      x0 = f0;
-      x1 = f1;
-    }
-    NA_CK(cudaStreamSynchronize(stream));
-    if (!(x1 > x0)) return fail(UPPE_ERR_ARG, "the ionisation grid must increase");
+    // inv_dx = 0 tells the kernel to take the grid constants from the table's
+    // ends on the device, so nothing is read back to the host
     b.lut.x = lut_log10I;
     b.lut.w = lut_W;
     b.lut.n = lut_n;
-    b.lut.x0 = x0;
-    b.lut.inv_dx = (lut_n - 1) / (x1 - x0);
+    b.lut.x0 = 0.0;
+    b.lut.inv_dx = 0.0;
   }
 
-  NA_CK(cudaMemcpyAsync(base + kInstOff, &q, sizeof(q), cudaMemcpyHostToDevice, stream));
-  NA_CK(cudaMemcpyAsync(base + kOrderOff, order_counter, sizeof(order_counter),
-                        cudaMemcpyHostToDevice, stream));
+  // the instance record goes in as a kernel argument (by value): no copy from
+  // host memory is left pending when this call returns
+  k_noalloc_header<<<1, 32, 0, stream>>>(q);
+  NA_CK(cudaGetLastError());
   if (dbl) k_noalloc_twiddles<double2><<<8, 256, 0, stream>>>(kHeader, n);
   else k_noalloc_twiddles<float2><<<8, 256, 0, stream>>>(kHeader, n);
   NA_CK(cudaGetLastError());

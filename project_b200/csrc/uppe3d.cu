@@ -31,6 +31,9 @@
 #include <stdlib.h>
 #include <string.h>
 
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <vector>
 
 #include "common.cuh"
@@ -150,7 +153,10 @@ template <> struct IPFactor<float> {
   // loses ~1e-16 * k ~ 1e-9 rad/m, far below FP32 resolution of the field, and
   // needs no division.  k_z comes from an FP32 square root refined by one FP64
   // Newton step (error ~1e-8 1/m).  The phase h/2*Im(D) is formed in FP64 and
-  // reduced mod 2 pi before it is rounded to FP32; __sincosf then works on [-pi, pi].
+  // reduced mod 2 pi before it is rounded to FP32; __sincosf then works on
+  // [-pi, pi] (absolute error ~4e-7).  The accurate sincosf cut the error of one
+  // attempt at 256x256x512 only from 4.0e-7 to 2.9e-7 (the FP32 transforms
+  // dominate) for 13 % more y-pass time, so the fast form is kept here.
   __device__ __forceinline__ static float2 get(const Tables3D&, const OmegaCol& oc, int,
                                                double q, double h2) {
     if (!oc.valid) return make_float2(1.f, 0.f);
@@ -755,6 +761,9 @@ struct YMaps {
   CUtensorMap in;     // (omega, ky, kx) view of the pass input (tmp[1])
   CUtensorMap acur;   // the same view of A = fft2(Z) (YMID1R transforms no input)
   CUtensorMap z2;     // the same view of tmp[2] = fft_x(Z) (YMID1's second field)
+  CUtensorMap tsum;   // the stage operands, prefetched into L2 one tile ahead
+  CUtensorMap k1;
+  CUtensorMap a4p;
 };
 
 __device__ __forceinline__ unsigned smem_u32(const void* p) {
@@ -775,8 +784,12 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
   return false;
 }
 
-template <int N, int MODE>
-__global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
+// LATE = 0: the stage operands of a tile are loaded into registers before its
+// wait (two CTAs per SM); LATE = 1: they are loaded where they are used (from L2,
+// where the previous tile prefetched them), which leaves room for three CTAs per
+// SM.  Same arithmetic either way.
+template <int N, int MODE, int LATE>
+__global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
   using C = float2;
   using Rl = float;
   constexpr int NTHR = 256;
@@ -811,6 +824,18 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
         :: "r"(smem_u32(buf[b])), "l"(reinterpret_cast<unsigned long long>(map)), "r"(w0), "r"(0), "r"(o),
            "r"(bar)
         : "memory");
+  };
+  // the next tile's stage operands into L2 (their loads below then hit L2)
+  auto prefetch_ops = [&](int tile) {
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    auto pf = [&](const CUtensorMap* m) {
+      asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
+                   :: "l"(reinterpret_cast<unsigned long long>(m)), "r"(w0), "r"(0), "r"(o) : "memory");
+    };
+    if constexpr (MODE == YMID2 || MODE == YMID3) { pf(&maps.acur); pf(&maps.tsum); }
+    else if constexpr (MODE == YMID4) pf(&maps.tsum);
+    else if constexpr (MODE == YMID1R) pf(&maps.k1);
+    else if constexpr (MODE == YFWD5) pf(&maps.a4p);
   };
   auto issueA = [&](int tile) {
     const int o = tile / ntw, w0 = (tile % ntw) * kW;
@@ -855,26 +880,41 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
   int k = 0;
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
     const int b = k & 1;
-    if (tid == 0 && tile + (int)gridDim.x < total) issue(tile + gridDim.x, b ^ 1);
+    const bool next = tile + (int)gridDim.x < total;
+    if (tid == 0 && next) {
+      issue(tile + gridDim.x, b ^ 1);
+      prefetch_ops(tile + gridDim.x);
+    }
     const int o = tile / ntw, w0 = (tile % ntw) * kW;
     const long long base = (long long)o * Ny * Nt + w0;
     // operands of this thread's elements (e = tid + i*NTHR), in flight during the wait and FFT
-    C opA[E], opB[E];
-    const double qn = (tid < N && MODE != YMID4 && MODE != YFWD5) ? __ldg(a.tb.q + (long long)o * Ny + tid) : 0.0;
-#pragma unroll
-    for (int i = 0; i < E; ++i) {
+    C opA[LATE ? 1 : E], opB[LATE ? 1 : E];
+    auto load_ops = [&](int i, C& A_, C& B_) {
       const int e = tid + i * NTHR;
       const long long gi = base + (long long)(e / kW) * Nt + (e % kW);
-      if constexpr (MODE == YMID2 || MODE == YMID3) { opA[i] = __ldg(acur + gi); opB[i] = __ldg(tsum + gi); }
-      else if constexpr (MODE == YMID4) opB[i] = __ldg(tsum + gi);
-      else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
-      else if constexpr (MODE == YFWD5) opA[i] = __ldg(a4p + gi);
+      if constexpr (MODE == YMID2 || MODE == YMID3) { A_ = __ldg(acur + gi); B_ = __ldg(tsum + gi); }
+      else if constexpr (MODE == YMID4) B_ = __ldg(tsum + gi);
+      else if constexpr (MODE == YMID1R) B_ = __ldg(k1b + gi);
+      else if constexpr (MODE == YFWD5) A_ = __ldg(a4p + gi);
+    };
+    const double qn = (tid < N && MODE != YMID4 && MODE != YFWD5) ? __ldg(a.tb.q + (long long)o * Ny + tid) : 0.0;
+    if constexpr (!LATE) {
+#pragma unroll
+      for (int i = 0; i < E; ++i) load_ops(i, opA[i], opB[i]);
     }
     if (tid < N) qrow[tid] = qn;   // read after the barrier below
     bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
     if (TWO) ok = ok && mbar_wait(smem_u32(&mbar[2]), (unsigned)(k & 1));
     if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
-      if (tid == 0) { atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT); st->done = 1; }
+      if (tid == 0) {
+        atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT);
+        st->done = 1;
+        // every copy this CTA started must have landed before it exits: wait again,
+        // bounded, on each barrier with a copy in flight
+        mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+        if (next) mbar_wait(smem_u32(&mbar[b ^ 1]), (unsigned)(((k + 1) >> 1) & 1));
+        if (TWO) mbar_wait(smem_u32(&mbar[2]), (unsigned)(k & 1));
+      }
       return;
     }
     C* s = buf[b];
@@ -886,8 +926,11 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
       const int e = tid + i * NTHR;
       const int n = e / kW, w = e % kW;     // n = ky, o = kx; s[e] = s[idx(w, n)]
       const long long gi = base + (long long)n * Nt + w;
+      C oA = C{0, 0}, oB = C{0, 0};
+      if constexpr (LATE) load_ops(i, oA, oB);
+      else { oA = opA[i]; oB = opB[i]; }
       if constexpr (MODE == YFWD5) {
-        const C a5 = s[e], a4 = opA[i];
+        const C a5 = s[e], a4 = oA;
         const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
         const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
         red = (d > red || d != d) ? d : red;
@@ -895,7 +938,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
       }
       if constexpr (MODE == YMID4) {
         const C a4 = s[e];
-        const C A4 = cadd(opB[i], cscale(a4, h6R));
+        const C A4 = cadd(oB, cscale(a4, h6R));
         a4p[gi] = a4;
         const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
         red = (m > red || m != m) ? m : red;
@@ -906,7 +949,7 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
       C u;
       if constexpr (MODE == YMID1R) {   // s = A tile, opB = k1
         const C v = cmul(s[e], Ef);
-        const C a1 = cmul(opB[i], Ef);
+        const C a1 = cmul(oB, Ef);
         tsum[gi] = a1;
         u = cadd(v, cscale(a1, h2R));
       } else if constexpr (MODE == YMID1) {   // s = k1 = N(A), bufA = A
@@ -919,13 +962,13 @@ __global__ void __launch_bounds__(256, 2) k_ypass_tma(SpaceArgs a, const __grid_
         u = cadd(v, cscale(a1, h2R));
       } else if constexpr (MODE == YMID2) {
         const C a2 = s[e];
-        const C v = cmul(opA[i], Ef);
-        tsum[gi] = cadd(opB[i], cscale(a2, (Rl)2));
+        const C v = cmul(oA, Ef);
+        tsum[gi] = cadd(oB, cscale(a2, (Rl)2));
         u = cadd(v, cscale(a2, h2R));
       } else {   // YMID3
         const C a3 = s[e];
-        const C v = cmul(opA[i], Ef);
-        const C ts = cadd(opB[i], cscale(a3, (Rl)2));
+        const C v = cmul(oA, Ef);
+        const C ts = cadd(oB, cscale(a3, (Rl)2));
         tsum[gi] = cmul(cadd(v, cscale(ts, h6R)), Ef);
         u = cmul(cadd(v, cscale(a3, hR)), Ef);
       }
@@ -1275,14 +1318,21 @@ __global__ void k_controller(State3D* st) {
   double err = st->err;
   double h = st->h;
   st->attempts += 1;
-  if (!isfinite(err) || !isfinite(h)) {
+  const double tol = st->tol, min_step = st->min_step, max_step = st->max_step;
+  if (!isfinite(h) || (!isfinite(err) && h <= min_step * 1.01)) {
     st->status |= UPPE_STATUS_NONFINITE;
     st->done = 1;
     st->last_accept = 0;
     return;
   }
-  const double tol = st->tol, min_step = st->min_step, max_step = st->max_step;
-  if (err < tol || h <= min_step * 1.01) {
+  if (!isfinite(err)) {
+    // the attempt overflowed (the accepted state is untouched): reject it and
+    // retry with a tenth of the step; at min_step the run stops (above)
+    st->status |= UPPE_STATUS_RETRIED;
+    st->fresh = 0;
+    st->last_accept = 0;
+    h = fmax(h * 0.1, min_step);
+  } else if (err < tol || h <= min_step * 1.01) {
     if (st->hlog && st->accepted < st->hlog_cap) st->hlog[st->accepted] = h;
     st->fail_count = (h <= min_step * 1.01 && err > tol) ? st->fail_count + 1 : 0;
     if (st->fail_count > 0) st->status |= UPPE_STATUS_MIN_STEP;
@@ -1316,6 +1366,16 @@ __global__ void k_controller(State3D* st) {
     st->done = 1;
   }
   st->h = h;
+}
+
+// the tuner's state: zeroed fields at unit scale, fresh (every pass of an attempt runs)
+__global__ void k_set_scale_one(State3D* st) {
+  st->A_scale = 1.0;
+  st->inv_A_scale = 1.0;
+  st->ion_bits = 0ull;
+  st->zidx = 0;
+  st->fresh = 1;
+  st->done = 0;
 }
 
 __global__ void k_set_h(State3D* st, double h) {
@@ -1431,9 +1491,17 @@ struct uppe3d_plan {
   double pass_scale = 1.0;                          // plain y passes
   double* diag_buf = nullptr;     // per-block partial sums + 3 results
   cudaStream_t cap_stream = nullptr;
-  bool ytma = false;              // TMA-fed y passes (complex64, 64 <= Ny <= 256)
+  bool ytma = false;              // TMA-fed y passes possible (complex64, 64 <= Ny <= 256)
   YMaps ymaps;
   int nsm = 148;
+  // launch configuration picked per shape by the tuner (uppe3d_tuning): every
+  // candidate computes the same bits, only the time differs
+  int y_tma = 1;                  // y passes on k_ypass_tma (1) or k_space (0)
+  int y_ctas = 2;                 // k_ypass_tma CTAs per SM (1, 2 or 3)
+  int y_late = 0;                 // k_ypass_tma loads the stage operands where used (1)
+  int t_wpb = 8;                  // warps (t-lines) per block of k_tpass_w (4 or 8)
+  float tune_ms[8] = {0};         // measured per-attempt pass times of the candidates
+  int tuned = 0;                  // 1 timed here, 2 from the process cache, 0 defaults
 };
 
 #define UPPE_CK(x)                                                                 \
@@ -1493,35 +1561,49 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
 
 // the y passes of the attempt that k_ypass_tma serves (its `in` map is tmp[1])
 static bool use_ytma(const uppe3d_plan* p, int mode, const void* in) {
-  return p->ytma && (mode == YMID1R || ((mode == YMID1 || mode == YMID2 || mode == YMID3 || mode == YMID4 ||
+  return p->ytma && p->y_tma && (mode == YMID1R || ((mode == YMID1 || mode == YMID2 || mode == YMID3 || mode == YMID4 ||
                                          mode == YFWD5) && in == p->b.tmp[1]));
 }
 
-template <int N>
-static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
-  const dim3 g((unsigned)(2 * p->nsm));
+template <int N, int LATE>
+static void launch_ytma_nl(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
+  // persistent CTAs: never more per SM than the shared memory lets be resident
+  const int per_sm = ytma_smem<N>(a.mode) * p->y_ctas <= 220 * 1024 ? p->y_ctas : 2;
+  const dim3 g((unsigned)(per_sm * p->nsm));
   const size_t sm = ytma_smem<N>(a.mode);
   switch (a.mode) {
-    case YMID1: k_ypass_tma<N, YMID1><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID1R: k_ypass_tma<N, YMID1R><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID2: k_ypass_tma<N, YMID2><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID3: k_ypass_tma<N, YMID3><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID4: k_ypass_tma<N, YMID4><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    default: k_ypass_tma<N, YFWD5><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID1: k_ypass_tma<N, YMID1, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID1R: k_ypass_tma<N, YMID1R, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID2: k_ypass_tma<N, YMID2, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID3: k_ypass_tma<N, YMID3, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID4: k_ypass_tma<N, YMID4, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    default: k_ypass_tma<N, YFWD5, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
   }
 }
 
 template <int N>
-static cudaError_t set_ytma_attr() {
+static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
+  if (p->y_late) launch_ytma_nl<N, 1>(p, a, s);
+  else launch_ytma_nl<N, 0>(p, a, s);
+}
+
+template <int N, int LATE>
+static cudaError_t set_ytma_attr_l() {
   const int sm = (int)ytma_smem<N>(YMID2);
-  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)ytma_smem<N>(YMID1));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YFWD5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YFWD5, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   return e;
+}
+
+template <int N>
+static cudaError_t set_ytma_attr() {
+  const cudaError_t e = set_ytma_attr_l<N, 0>();
+  return e == cudaSuccess ? set_ytma_attr_l<N, 1>() : e;
 }
 
 template <typename Rl>
@@ -1560,21 +1642,21 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
 template <int NT, typename Rl> struct TWarp {
   static constexpr bool use = NT == 512 || (NT == 1024 && sizeof(Rl) == 4);
   static constexpr int E = NT / 32;
-  static constexpr int WPB = 8;
   static constexpr int BUF = WarpFFT<(E < 16 ? 16 : E)>::SBUF > TCfg<NT>::PAD
                                  ? WarpFFT<(E < 16 ? 16 : E)>::SBUF : TCfg<NT>::PAD;
-  static size_t smem() {
+  static size_t smem(int WPB) {
     return (size_t)(NT + WPB * BUF) * sizeof(typename CT<Rl>::T) + (size_t)WPB * 32 * sizeof(double) +
            (size_t)WPB * (NT + NT / 32) * sizeof(float) + (size_t)NT * sizeof(Rl);
   }
 };
 
 template <typename Rl, int NT, int KIND>
-static void launch_t_n(const TArgs& a, long long nlines, cudaStream_t s) {
+static void launch_t_n(const TArgs& a, long long nlines, int wpb, cudaStream_t s) {
   if constexpr (KIND == 0 && TWarp<NT, Rl>::use) {
-    constexpr int WPB = TWarp<NT, Rl>::WPB;
-    const unsigned nb = (unsigned)((nlines + WPB - 1) / WPB);
-    k_tpass_w<Rl, NT / 32, WPB><<<nb, WPB * 32, TWarp<NT, Rl>::smem(), s>>>(a);
+    const unsigned nb = (unsigned)((nlines + wpb - 1) / wpb);
+    const size_t sm = TWarp<NT, Rl>::smem(wpb);
+    if (wpb == 4) k_tpass_w<Rl, NT / 32, 4><<<nb, 4 * 32, sm, s>>>(a);
+    else k_tpass_w<Rl, NT / 32, 8><<<nb, 8 * 32, sm, s>>>(a);
     return;
   }
   constexpr int WPB = TLaunch<NT, Rl>::WPB;
@@ -1593,7 +1675,7 @@ static int launch_t(uppe3d_plan* p, int mode, const void* in, void* out, cudaStr
   a.in = in; a.out = out; a.mode = mode;
   const long long nl = (long long)p->g.Nx * p->g.Ny;
   switch (p->g.Nt) {
-#define UPPE_T(n) case n: launch_t_n<Rl, n, KIND>(a, nl, s); break;
+#define UPPE_T(n) case n: launch_t_n<Rl, n, KIND>(a, nl, p->t_wpb, s); break;
     UPPE_T(32) UPPE_T(64) UPPE_T(128) UPPE_T(256) UPPE_T(512) UPPE_T(1024) UPPE_T(2048)
 #undef UPPE_T
     default: return UPPE_ERR_SIZE;
@@ -1619,8 +1701,11 @@ static cudaError_t set_t_attr() {
   cudaError_t e = cudaFuncSetAttribute(k_tpass<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
   if (e != cudaSuccess) return e;
   if constexpr (TWarp<NT, Rl>::use) {
-    e = cudaFuncSetAttribute(k_tpass_w<Rl, NT / 32, TWarp<NT, Rl>::WPB>,
-                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)TWarp<NT, Rl>::smem());
+    e = cudaFuncSetAttribute(k_tpass_w<Rl, NT / 32, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)TWarp<NT, Rl>::smem(4));
+    if (e == cudaSuccess)
+      e = cudaFuncSetAttribute(k_tpass_w<Rl, NT / 32, 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                               (int)TWarp<NT, Rl>::smem(8));
     if (e != cudaSuccess) return e;
   }
   e = cudaFuncSetAttribute(k_tload<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
@@ -1739,9 +1824,10 @@ static int setup_ytma(uppe3d_plan* p) {
   const cuuint64_t strides[2] = {(cuuint64_t)p->g.Nt * 8, (cuuint64_t)p->g.Ny * p->g.Nt * 8};
   const cuuint32_t box[3] = {(cuuint32_t)kW, (cuuint32_t)p->g.Ny, 1};
   const cuuint32_t es[3] = {1, 1, 1};
-  void* bufs[3] = {p->b.tmp[1], p->b.acur, p->b.tmp[2]};
-  CUtensorMap* maps[3] = {&p->ymaps.in, &p->ymaps.acur, &p->ymaps.z2};
-  for (int i = 0; i < 3; ++i) {
+  void* bufs[6] = {p->b.tmp[1], p->b.acur, p->b.tmp[2], p->b.tsum, p->b.k1, p->b.a4p};
+  CUtensorMap* maps[6] = {&p->ymaps.in, &p->ymaps.acur, &p->ymaps.z2, &p->ymaps.tsum, &p->ymaps.k1,
+                          &p->ymaps.a4p};
+  for (int i = 0; i < 6; ++i) {
     if (reinterpret_cast<uintptr_t>(bufs[i]) % 16) return 0;
     if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, bufs[i], dims, strides, box, es,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
@@ -1758,6 +1844,115 @@ static int setup_ytma(uppe3d_plan* p) {
     default: return 0;
   }
   p->ytma = true;
+  return 0;
+}
+
+// ---------------------------------------------------------------------------
+// Per-shape tuner.  Candidates: the y passes on k_ypass_tma (operands loaded early
+// with one or two CTAs per SM, or late with two or three), and k_tpass_w with
+// four or eight t-lines per block (same per-line code).  Every candidate computes
+// the same bits, so the choice changes only the time.  Each candidate runs whole
+// attempts launch by launch on zeroed fields with CUDA events around each launch;
+// the y and t choices are independent (different launches), so they are timed
+// separately.  Choices are kept per (Nx, Ny, Nt, precision, SM count) for the
+// life of the process; UPPE_TUNE=0 in the environment keeps the defaults.
+// ---------------------------------------------------------------------------
+struct TuneKey {
+  int Nx, Ny, Nt, dbl, nsm;
+  bool operator<(const TuneKey& o) const {
+    return std::tie(Nx, Ny, Nt, dbl, nsm) < std::tie(o.Nx, o.Ny, o.Nt, o.dbl, o.nsm);
+  }
+};
+struct TuneVal { int y_tma, y_ctas, y_late, t_wpb; float ms[8]; };
+static std::map<TuneKey, TuneVal> g_tune_cache;
+static std::mutex g_tune_mu;
+
+template <typename Rl>
+static int time_attempts(uppe3d_plan* p, cudaStream_t s, int reps, float* y_ms, float* t_ms) {
+  *y_ms = 0.f;
+  *t_ms = 0.f;
+  for (int r = 0; r < reps; ++r) {
+    k_set_h<<<1, 1, 0, s>>>(p->st, 1e-3);
+    Recorder rec;
+    rec.s = s;
+    rec.prof = true;
+    rec.fresh = 1;
+    rec.fbytes = (double)p->csz * (double)p->g.npts;
+    int rc = enqueue_attempt<Rl>(p, rec);
+    UPPE_CK(cudaStreamSynchronize(s));
+    for (size_t i = 0; i < rec.kind.size(); ++i) {
+      float ms = 0.f;
+      cudaEventElapsedTime(&ms, rec.ev[2 * i], rec.ev[2 * i + 1]);
+      if (rec.kind[i] == KIND_Y || rec.kind[i] == KIND_YT) *y_ms += ms;
+      if (rec.kind[i] == KIND_T) *t_ms += ms;
+    }
+    for (auto e : rec.ev) cudaEventDestroy(e);
+    if (rc) return rc;
+  }
+  *y_ms /= reps;
+  *t_ms /= reps;
+  return 0;
+}
+
+static int tune(uppe3d_plan* p) {
+  const char* env = getenv("UPPE_TUNE");
+  if (env && env[0] == '0') return 0;
+  const TuneKey key{p->g.Nx, p->g.Ny, p->g.Nt, p->dbl, p->nsm};
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune_cache.find(key);
+    if (it != g_tune_cache.end()) {
+      p->y_tma = it->second.y_tma;
+      p->y_ctas = it->second.y_ctas;
+      p->y_late = it->second.y_late;
+      p->t_wpb = it->second.t_wpb;
+      memcpy(p->tune_ms, it->second.ms, sizeof(p->tune_ms));
+      p->tuned = 2;
+      return 0;
+    }
+  }
+  cudaStream_t s;
+  UPPE_CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+  const size_t fbytes = p->csz * (size_t)p->g.npts;
+  void* fields[] = {p->b.z[0], p->b.z[1], p->b.acur, p->b.k1, p->b.tsum, p->b.a4p,
+                    p->b.tmp[0], p->b.tmp[1], p->b.tmp[2]};
+  for (void* f : fields) UPPE_CK(cudaMemsetAsync(f, 0, fbytes, s));
+  k_begin<<<1, 1, 0, s>>>(p->st, 1.0, 1e-5, 1e-2, 1e-9, 0);
+  k_set_scale_one<<<1, 1, 0, s>>>(p->st);
+  // the plain tile kernel rounds differently from the TMA-fed one, so it is a
+  // candidate only where the TMA path is unavailable
+  struct YC { int tma, ctas, late; } yc[4] = {{1, 2, 0}, {1, 1, 0}, {1, 3, 1}, {1, 2, 1}};
+  const int ny = p->ytma ? 4 : 1;
+  if (!p->ytma) yc[0] = YC{0, 2, 0};
+  const int tw_n = (p->g.Nt == 512 || (p->g.Nt == 1024 && !p->dbl)) ? 2 : 1;
+  const int tw[2] = {8, 4};
+  float best_y = 1e30f, best_t = 1e30f;
+  int by = 0, bt = 0;
+  int rc = 0;
+  float y_ms, t_ms;
+  p->y_tma = yc[0].tma; p->y_ctas = yc[0].ctas; p->y_late = yc[0].late; p->t_wpb = tw[0];
+  rc = p->dbl ? time_attempts<double>(p, s, 1, &y_ms, &t_ms) : time_attempts<float>(p, s, 1, &y_ms, &t_ms);
+  for (int i = 0; i < ny && !rc; ++i) {        // y candidates with the default t-pass
+    p->y_tma = yc[i].tma; p->y_ctas = yc[i].ctas; p->y_late = yc[i].late;
+    rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
+    p->tune_ms[i] = y_ms;
+    if (y_ms < best_y) { best_y = y_ms; by = i; }
+  }
+  p->y_tma = yc[by].tma; p->y_ctas = yc[by].ctas; p->y_late = yc[by].late;
+  for (int i = 0; i < tw_n && !rc; ++i) {      // t candidates with the chosen y passes
+    p->t_wpb = tw[i];
+    rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
+    p->tune_ms[5 + i] = t_ms;
+    if (t_ms < best_t) { best_t = t_ms; bt = i; }
+  }
+  p->t_wpb = tw[bt];
+  cudaStreamDestroy(s);
+  if (rc) return rc;
+  p->tuned = 1;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  TuneVal v{p->y_tma, p->y_ctas, p->y_late, p->t_wpb, {0}};
+  memcpy(v.ms, p->tune_ms, sizeof(v.ms));
+  g_tune_cache[key] = v;
   return 0;
 }
 
@@ -1891,7 +2086,13 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
     p->allocs.push_back(*f);
   }
   UPPE_TRY(p->dbl ? set_attrs<double>(p->g) : set_attrs<float>(p->g));
+  {
+    int dev = 0;
+    UPPE_CK(cudaGetDevice(&dev));
+    UPPE_CK(cudaDeviceGetAttribute(&p->nsm, cudaDevAttrMultiProcessorCount, dev));
+  }
   if (!p->dbl && p->g.Ny >= 64 && p->g.Ny <= 256) UPPE_TRY(setup_ytma(p));
+  UPPE_TRY(tune(p));
   UPPE_TRY(build_graphs(p));
 #undef UPPE_TRY
   *out = p;
@@ -2014,6 +2215,28 @@ extern "C" int uppe3d_get_field(uppe3d_plan* p, void* out, cudaStream_t s) {
 
 extern "C" long long uppe3d_field_bytes(const uppe3d_plan* p) {
   return p ? (long long)(p->csz * p->g.npts) : 0;
+}
+
+extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg5, float* ms8) {
+  if (!p || !cfg5) return UPPE_ERR_ARG;
+  cfg5[0] = p->ytma && p->y_tma;
+  cfg5[1] = p->y_ctas;
+  cfg5[2] = p->y_late;
+  cfg5[3] = p->t_wpb;
+  cfg5[4] = p->tuned;
+  if (ms8) memcpy(ms8, p->tune_ms, sizeof(p->tune_ms));
+  return 0;
+}
+
+extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_late, int t_wpb) {
+  if (!p || y_ctas < 1 || y_ctas > 3 || (t_wpb != 4 && t_wpb != 8)) return UPPE_ERR_ARG;
+  p->y_tma = y_tma ? 1 : 0;
+  p->y_ctas = y_ctas;
+  p->y_late = y_late ? 1 : 0;
+  p->t_wpb = t_wpb;
+  if (p->g_attempt) { cudaGraphExecDestroy(p->g_attempt); p->g_attempt = nullptr; }
+  if (p->g_step) { cudaGraphExecDestroy(p->g_step); p->g_step = nullptr; }
+  return build_graphs(p);
 }
 
 extern "C" int uppe3d_launches_per_step(const uppe3d_plan* p) {
@@ -2587,9 +2810,12 @@ static int adj_tlaunch_n(uppe3d_plan* p, const void* in, const void* xin, void* 
     const unsigned vnb = (unsigned)((nl + VW - 1) / VW);
     e = cudaFuncSetAttribute(k_tvjp<Rl, NT, VW>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)vsm);
     if (e == cudaSuccess) k_tvjp<Rl, NT, VW><<<vnb, VW * 32, vsm, s>>>(a, xin);
-  } else {
+  } else if (KIND == 1) {
     e = cudaFuncSetAttribute(k_tline<Rl, NT, WPB, +1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e == cudaSuccess) k_tline<Rl, NT, WPB, +1><<<nb, WPB * 32, smem, s>>>(a, scale);
+  } else {
+    e = cudaFuncSetAttribute(k_tline<Rl, NT, WPB, -1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e == cudaSuccess) k_tline<Rl, NT, WPB, -1><<<nb, WPB * 32, smem, s>>>(a, scale);
   }
   if (e != cudaSuccess) return UPPE_ERR_CUDA;
   return cudaGetLastError() == cudaSuccess ? 0 : UPPE_ERR_CUDA;
@@ -2714,6 +2940,15 @@ static int adjoint_impl(uppe3d_plan* p, const double* hl, int nsteps, int K, con
   rc |= adj_tlaunch<Rl, 1>(p, ZB, nullptr, A0bar, 1.0 / p->st_host->A_scale, s);
   UPPE_CK(cudaGetLastError());
   return rc;
+}
+
+extern "C" int uppe3d_transform_t(uppe3d_plan* p, const void* in, void* out, int dir, double scale,
+                                  cudaStream_t s) {
+  if (!p || !in || !out || (dir != -1 && dir != 1)) return UPPE_ERR_ARG;
+  if (dir < 0) return p->dbl ? adj_tlaunch<double, 2>(p, in, nullptr, out, scale, s)
+                             : adj_tlaunch<float, 2>(p, in, nullptr, out, scale, s);
+  return p->dbl ? adj_tlaunch<double, 1>(p, in, nullptr, out, scale, s)
+                : adj_tlaunch<float, 1>(p, in, nullptr, out, scale, s);
 }
 
 extern "C" long long uppe3d_adjoint_work_bytes(const uppe3d_plan* p, int nsteps, int K) {

@@ -149,6 +149,144 @@ def spectrum_spline(wavelengths_nm, intensities, use_jacobian=True, interp_kind=
     return brk, coef
 
 
+def _line_transform(x, direction, scale, shift_in=False, shift_out=False):
+    """One complex128 device line through uppe_fft_c128 (N a power of two)."""
+    import ctypes
+    import torch
+    from . import _lib
+    lib = _lib.load()
+    N = x.numel()
+    if N < 2 or N & (N - 1):
+        raise ValueError(f'the device line transform needs a power-of-two length, got {N}')
+    x = x.to(torch.complex128).contiguous()
+    out = torch.empty_like(x)
+    work = torch.empty(2 * N, dtype=torch.complex128, device=x.device)
+    _lib.check(lib.uppe_fft_c128(ctypes.c_void_p(x.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                 ctypes.c_void_p(work.data_ptr()), N, int(direction), float(scale),
+                                 1 if shift_in else 0, 1 if shift_out else 0, _lib.stream_ptr()), 'uppe_fft_c128')
+    return out
+
+
+def dispersed_pulse_device(t, pulse_energy, pulse_fwhm, GDD=0.0, TOD=0.0, device=None):
+    """generate_dispersed_pulse (erk43ip_method.py:383-446) on the device: the
+    transform-limited Gaussian, ifftshift, fft, the phase GDD w^2/2 + TOD w^3/6,
+    ifft and fftshift, all in the library's kernels (uppe_fft_c128,
+    uppe_spectral_phase).  Returns a complex128 torch tensor on the device."""
+    import ctypes
+    import torch
+    from . import _lib
+    lib = _lib.load()
+    dev = torch.device(device if device is not None else 'cuda')
+    t = np.asarray(t, dtype=np.float64)
+    P0 = pulse_energy / (pulse_fwhm * np.sqrt(np.pi / (4 * np.log(2))))
+    T0 = pulse_fwhm / (2 * np.sqrt(np.log(2)))
+    A = torch.from_numpy(np.sqrt(P0) * np.exp(-(t / T0) ** 2 / 2)).to(dev).to(torch.complex128)
+    if GDD == 0 and TOD == 0:
+        return A
+    N = len(t)
+    spec = _line_transform(A, -1, 1.0, shift_in=True)                         # fft(ifftshift(A))
+    _lib.check(lib.uppe_spectral_phase(ctypes.c_void_p(spec.data_ptr()), N, float(t[1] - t[0]), float(GDD),
+                                       float(TOD), _lib.stream_ptr()), 'uppe_spectral_phase')
+    return _line_transform(spec, +1, 1.0 / N, shift_out=True)                 # fftshift(ifft(.))
+
+
+def exact_fourier_pulse(t, wavelengths_nm, intensities, pulse_energy, GDD=0.0, TOD=0.0, use_jacobian=True,
+                        interp_kind='cubic', center_wavelength=800e-9, device=None):
+    """generate_pulse_from_spectrum(exact_fourier=True) (erk43ip_method.py:492-598,
+    664-672, 734-741): the spectrum interpolated with interp1d onto a dense uniform
+    frequency grid (min(4096, 4 n) points), its precise FWHM centre, the Simpson
+    weights of scipy.integrate.simpson for that grid (the irregular-spacing form it
+    applies when x is given, with the last-interval correction for an even count),
+    then the direct sum over the dense grid for every t on the device
+    (uppe_exact_ft) and the trapezoidal energy normalisation.  Returns
+    (A, center_freq, delta_nu) with A a complex128 torch tensor on the device."""
+    import ctypes
+    import torch
+    from scipy.interpolate import interp1d
+    from . import _lib
+    from .analysis import fwhm_precise
+    lib = _lib.load()
+    dev = torch.device(device if device is not None else 'cuda')
+    t = np.asarray(t, dtype=np.float64)
+    idx = np.argsort(wavelengths_nm)
+    wl = np.asarray(wavelengths_nm, dtype=np.float64)[idx]
+    I = np.asarray(intensities, dtype=np.float64)[idx]
+    if np.max(I) > 0:
+        I = I / np.max(I)
+    f = C0 / (wl * 1e-9)
+    if use_jacobian:
+        I = I * (wl * 1e-9) ** 2 / C0
+        if np.max(I) > 0:
+            I = I / np.max(I)
+    uf, ui = np.unique(f, return_index=True)
+    if len(uf) < len(f):
+        f, I = uf, I[ui]
+    if f[0] < f[-1]:
+        f, I = f[::-1], I[::-1]
+    kind = 'linear' if interp_kind in ('cubic', 'quadratic') and len(f) < 4 else interp_kind
+    fi = interp1d(f, I, kind=kind, bounds_error=False, fill_value=0.0)
+    nd = min(4096, len(f) * 4)
+    fd = np.linspace(f.min(), f.max(), nd)
+    sd = fi(fd)
+    sd[sd < 0] = 0
+    fl, fr, dnu = fwhm_precise(fd, sd)
+    if dnu:
+        fc = (fl + fr) / 2
+    else:
+        fc = np.sum(fd * sd) / np.sum(sd) if np.sum(sd) > 0 else C0 / center_wavelength
+    x = fd - fc
+    om = 2 * np.pi * x
+    phase = 0.5 * GDD * om ** 2 + (1.0 / 6.0) * TOD * om ** 3
+    w = simpson_weights(x)
+    amp = w * np.sqrt(sd) * np.exp(1j * phase)
+    td = torch.from_numpy(t).to(dev)
+    omd = torch.from_numpy(np.ascontiguousarray(om)).to(dev)
+    ad = torch.from_numpy(np.ascontiguousarray(amp.astype(np.complex128))).to(dev)
+    A = torch.empty(len(t), dtype=torch.complex128, device=dev)
+    _lib.check(lib.uppe_exact_ft(ctypes.c_void_p(td.data_ptr()), len(t), ctypes.c_void_p(omd.data_ptr()),
+                                 ctypes.c_void_p(ad.data_ptr()), nd, ctypes.c_void_p(A.data_ptr()),
+                                 _lib.stream_ptr()), 'uppe_exact_ft')
+    P = A.real ** 2 + A.imag ** 2
+    E = float(torch.trapezoid(P, td))
+    if E > 0:
+        A = A * np.sqrt(pulse_energy / E)
+    return A, fc, dnu
+
+
+def simpson_weights(x):
+    """Weights w with sum w_k y_k = scipy.integrate.simpson(y, x=x) for 1-D x (the
+    composite rule for irregular spacing over pairs of intervals; for an even
+    number of samples the rule covers the first n - 2 intervals and the last one
+    gets the three-point correction of Cartwright's formula)."""
+    x = np.asarray(x, dtype=np.float64)
+    n = len(x)
+    w = np.zeros(n)
+    if n == 1:
+        return w
+    if n == 2:
+        h = x[1] - x[0]
+        w[:] = 0.5 * h
+        return w
+    h = np.diff(x)
+    stop = n - 2 if n % 2 == 1 else n - 3
+    for j in range(0, stop, 2):
+        h0, h1 = h[j], h[j + 1]
+        hs, hp = h0 + h1, h0 * h1
+        r = h0 / h1 if h1 != 0 else 0.0
+        w[j] += hs / 6.0 * (2.0 - (1.0 / r if r != 0 else 0.0))
+        w[j + 1] += hs / 6.0 * (hs * (hs / hp if hp != 0 else 0.0))
+        w[j + 2] += hs / 6.0 * (2.0 - r)
+    if n % 2 == 0:
+        h0, h1 = h[-2], h[-1]
+        alpha = (2 * h1 ** 2 + 3 * h0 * h1) / (6 * (h1 + h0)) if (h1 + h0) != 0 else 0.0
+        beta = (h1 ** 2 + 3.0 * h0 * h1) / (6 * h0) if h0 != 0 else 0.0
+        eta = h1 ** 3 / (6 * h0 * (h0 + h1)) if h0 * (h0 + h1) != 0 else 0.0
+        w[-1] += alpha
+        w[-2] += beta
+        w[-3] -= eta
+    return w
+
+
 def pulse_from_spectrum(t, wavelengths_nm, intensities, pulse_energy, GDD=0.0, TOD=0.0,
                         use_jacobian=True, interp_kind='cubic', center_wavelength=800e-9,
                         device=None):
@@ -171,7 +309,7 @@ def pulse_from_spectrum(t, wavelengths_nm, intensities, pulse_energy, GDD=0.0, T
     _lib.check(lib.uppe_spectrum_field(ctypes.c_void_p(b.data_ptr()), ctypes.c_void_p(c.data_ptr()), len(brk), N,
                                        dt, C0 / center_wavelength, float(GDD), float(TOD),
                                        ctypes.c_void_p(Aw.data_ptr()), _lib.stream_ptr()), 'uppe_spectrum_field')
-    A = torch.fft.fftshift(torch.fft.ifft(Aw))
+    A = _line_transform(Aw, +1, 1.0 / N, shift_out=True)                      # fftshift(ifft(A_w))
     P = (A.real ** 2 + A.imag ** 2)
     E = float(torch.trapezoid(P, torch.from_numpy(t).to(dev)))
     if E > 0:

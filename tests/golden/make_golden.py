@@ -33,7 +33,7 @@ import scipy.fft
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REF = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+REF = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('UPPE_REFERENCE', '/root/reference')
 REF_1D = os.path.join(REF, 'src', '1D-ERK4(3)IP UPPE gas')
 REF_3D = os.path.join(REF, 'src', '3+1D-UPPE-ERK4(3)IP-envelope')
 REF_THZ = os.path.join(REF, 'src', 'THz', '2+1D-all field UPPE Argon.py')
@@ -301,6 +301,83 @@ def make_spectrum():
     sys.path.remove(REF_1D)
 
 
+def make_pulses():
+    """generate_dispersed_pulse (erk43ip_method.py:383-446) for three GDD/TOD sets
+    and generate_pulse_from_spectrum with exact_fourier=True (:492-598, 664-672)
+    for two option sets on the seeded spectrum (1204 dense frequencies: an even
+    count, so scipy's last-interval correction is exercised)."""
+    sys.path.insert(0, REF_1D)
+    erk = load(os.path.join(REF_1D, 'erk43ip_method.py'), 'erk43ip_method')
+    s = erk.ERK43IP_UPPE(material='argon_gas', n2=1.0e-23, beam_radius=0.65 * 125e-6,
+                         center_wavelength=800e-9)
+    t = np.linspace(-1.0e-12, 1.0e-12, 2048)
+    disp = [(0.0, 0.0), (500e-30, 0.0), (-300e-30, 4000e-45)]
+    out = {f'D{k}': s.generate_dispersed_pulse(t, 40e-6, 30e-15, GDD=g, TOD=d) for k, (g, d) in enumerate(disp)}
+    wl, I = spectrum_case()
+    te = np.linspace(-0.5e-12, 0.5e-12, 1024)
+    exact = [('cubic', True, 0.0, 0.0), ('linear', False, 200e-30, -1500e-45)]
+    for k, (kind, jac, gdd, tod) in enumerate(exact):
+        out[f'X{k}'] = s.generate_pulse_from_spectrum(te, wl, I, 50e-6, GDD=gdd, TOD=tod, use_jacobian=jac,
+                                                      interp_kind=kind, exact_fourier=True)
+    save('ref1d_pulses', t=t, E=40e-6, fwhm=30e-15, gdd=np.array([d[0] for d in disp]),
+         tod=np.array([d[1] for d in disp]), te=te, wl=wl, I=I, Ex=50e-6,
+         x_kinds=np.array([e[0] for e in exact]), x_jac=np.array([e[1] for e in exact]),
+         x_gdd=np.array([e[2] for e in exact]), x_tod=np.array([e[3] for e in exact]), **out)
+    sys.path.remove(REF_1D)
+
+
+class _Dev(np.ndarray):
+    """ndarray with cupy's .get() (returns itself) for the driver's host copies."""
+    def get(self):
+        return np.asarray(self)
+
+
+def make_beam_diag():
+    """MPC_Final_Runner.save_snapshot (src/3+1D-ERK4(3)IP UPPE/sim.py:187-249) run on a
+    seeded 16 x 16 x 64 field through the numpy stand-in; its DIAG record (written
+    before the plotting, which the matplotlib stub stops) is the fixture."""
+    import tempfile
+    ref_mpc = os.path.join(REF, 'src', '3+1D-ERK4(3)IP UPPE')
+    sys.path.insert(0, ref_mpc)
+    cp = sys.modules['cupy']
+    saved = cp.argmax
+    cp.argmax = lambda a, *k, **kw: np.asarray(np.argmax(a, *k, **kw)).view(_Dev)
+    sys.modules['matplotlib'].use = lambda *a, **k: None      # backend choice only
+    sim = load(os.path.join(ref_mpc, 'sim.py'), 'ref_sim')
+    rng = np.random.Generator(np.random.PCG64(31))
+    N, Nt = 16, 64
+    x = np.linspace(-1e-3, 1e-3, N)
+    t = np.linspace(-2e-12, 2e-12, Nt)
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    env = np.exp(-((X - 0.1e-3) ** 2 + (Y + 0.05e-3) ** 2) / (0.35e-3) ** 2)[:, :, None] \
+        * np.exp(-(t / 0.6e-12) ** 2)[None, None, :]
+    field = (env * (1 + 0.1 * rng.standard_normal((N, N, Nt)))
+             * np.exp(1j * (0.3 * rng.standard_normal((N, N, Nt)) + 2e24 * t ** 2))).astype(np.complex64)
+    r = object.__new__(sim.MPC_Final_Runner)
+    fs = types.SimpleNamespace(x=x.view(_Dev), y=x.copy().view(_Dev), t=t.view(_Dev), dx=x[1] - x[0],
+                               dy=x[1] - x[0], dt=t[1] - t[0], float_dtype=np.float32,
+                               freq_axis_hz=np.fft.fftshift(np.fft.fftfreq(Nt, t[1] - t[0])))
+    r.solver_fs = fs
+    r.A_scale = 3.7e7
+    r.Nxy = N
+    r.w0_waist = 0.4e-3
+    r.wavelength = 1064e-9
+    r.window_width = 2e-3
+    r.viz_wl_min_nm, r.viz_wl_max_nm, r.viz_time_ps_min, r.viz_time_ps_max = 1050.0, 1080.0, -30.0, 30.0
+    with tempfile.TemporaryDirectory() as d:
+        r.output_dir = d
+        try:
+            r.save_snapshot(3, field, 'fs')
+        except AttributeError:          # the plotting after the record (matplotlib is stubbed)
+            pass
+        rec = dict(np.load(os.path.join(d, 'cycle_03_fs_DIAG.npz')))
+    cp.argmax = saved
+    rec.pop('label', None)
+    save('ref3d_beam_diag', x=x, t=t, field_norm=field, A_scale=r.A_scale, w0=r.w0_waist, lam=r.wavelength,
+         **{f'ref_{k}': v for k, v in rec.items()})
+    sys.path.remove(ref_mpc)
+
+
 # ---------------------------------------------------------------------------
 # real-field 3+1D fixtures
 # ---------------------------------------------------------------------------
@@ -450,6 +527,8 @@ if __name__ == '__main__':
     print('1D fixtures from', REF_1D)
     make_1d()
     make_spectrum()
+    make_pulses()
+    make_beam_diag()
     print('real-field fixtures from', REF_RF)
     make_realfield()
     print('3D fixtures from', REF_3D)

@@ -1,0 +1,75 @@
+"""Per-shape launch tuner of the 3+1D plan (GPU).
+
+uppe3d_plan_create times the candidate launch configurations of the y passes
+(TMA-fed kernel with early or late operand loads and one to three CTAs per SM) and of the
+warp t-line kernel (four or eight lines per block) and keeps the fastest.  The
+candidates are chosen so that they compute the same bits: these tests force each
+one and compare the propagated fields bit for bit (the plain tile kernel, which
+rounds differently, is used only where the TMA path is unavailable).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(precision='single', n=64, nt=512):
+    from project_b200.media import Argon
+    x = np.linspace(-1.5e-3, 1.5e-3, n)
+    t = np.linspace(-100e-15, 100e-15, nt)
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    T0 = 40e-15 / (2 * np.sqrt(np.log(2)))
+    A0 = (np.sqrt(1e17) * np.exp(-(X ** 2 + Y ** 2) / 0.25e-6)[:, :, None]
+          * np.exp(-(t / T0) ** 2 / 2)[None, None, :])
+    lx = np.linspace(np.log10(1e12), np.log10(1e20), 2000)
+    W = np.minimum(3e9 * (10.0 ** lx / 5e16) ** 8, 1e20)      # ionises at this peak intensity
+    med = Argon(800e-9, 1.0, precision, True, lut=(lx, W))
+    return x, t, med, A0
+
+
+def _tuning(sol):
+    from project_b200 import _lib
+    cfg = (ctypes.c_int * 5)()
+    ms = (ctypes.c_float * 8)()
+    _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
+    return list(cfg), list(ms)
+
+
+def test_tuner_runs_and_every_candidate_gives_identical_fields():
+    import torch
+    from project_b200 import _lib
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, med, A0 = _setup()
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='single')
+    cfg, ms = _tuning(sol)
+    assert cfg[4] in (1, 2)                       # timed here or taken from the process cache
+    assert cfg[1] in (1, 2, 3) and cfg[3] in (4, 8)
+    if cfg[4] == 1:
+        assert all(v > 0 for v in ms[:4]) and ms[5] > 0 and ms[6] > 0
+    ref = None
+    ycands = [(1, 2, 0), (1, 1, 0), (1, 3, 1), (1, 2, 1)]
+    for y_tma, y_ctas, y_late in ycands:
+        for wpb in (4, 8):
+            _lib.check(sol._lib.uppe3d_set_tuning(sol._plan, y_tma, y_ctas, y_late, wpb),
+                       'uppe3d_set_tuning')
+            assert _tuning(sol)[0][:4] == [y_tma, y_ctas, y_late, wpb]
+            z, _, A = sol.propagate(A0.astype(np.complex64), 0.02, tol=1e-4, return_gpu=True)
+            assert sol.last_result.status == 0
+            if ref is None:
+                ref = (z, sol.last_result.attempts, A.clone(), sol.diagnostics()['peak_ionization'])
+                assert ref[3] > 0                    # the plasma path ran
+            else:
+                assert z == ref[0] and sol.last_result.attempts == ref[1]
+                assert torch.equal(A, ref[2]), (y_tma, y_ctas, y_late, wpb)
+
+
+def test_tuner_can_be_switched_off(monkeypatch):
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, med, _ = _setup(n=32, nt=256)
+    monkeypatch.setenv('UPPE_TUNE', '0')
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='single')
+    cfg, ms = _tuning(sol)
+    assert cfg[4] == 0 and cfg[3] == 8
+    assert all(v == 0 for v in ms)
