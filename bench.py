@@ -200,6 +200,7 @@ def batched1d_instances(n=256, seed=2, L=1.0):
     10 uJ..1 mJ, pressure U(0.2, 3) bar (n2, beta2, beta3, plasma scale with it), GDD
     U(-500, 500) fs^2; argon capillary a = 125 um, A_eff = pi (0.65 a)^2, loss 0.5 dB/m,
     beta2 15 fs^2/m, beta3 15 fs^3/m per bar, ADK plasma, one-photon-per-mode noise."""
+    from project_b200.distributed import instance_cost
     from project_b200.pulses import dispersed_pulse, photon_noise
     from project_b200.solver1d import ERK43IP_UPPE, GasPlasma1D
     rng = np.random.Generator(np.random.PCG64(seed))
@@ -215,7 +216,10 @@ def batched1d_instances(n=256, seed=2, L=1.0):
                          center_wavelength=LAM_1D, alpha=0.5 * np.log(10) / 10, use_raman=False,
                          taylor=(15e-30 * P, 15e-45 * P), plasma=GasPlasma1D(Aeff, pressure_atm=P),
                          precision='single')
-        insts.append(s.instance(t, L, tol=1e-6))
+        inst = s.instance(t, L, tol=1e-6)
+        inst['desc'].cost = instance_cost(Nt, L, energy=E, pressure=P)   # longest expected first
+        inst['energy'], inst['pressure'] = E, P
+        insts.append(inst)
         fields.append(dispersed_pulse(t, E, 30e-15, GDD=GDD) + photon_noise(t, LAM_1D, 1000 + k))
     return insts, fields
 
@@ -232,7 +236,7 @@ def run_batched1d(dev, rank=0, world=1, accuracy=False):
     n_all = len(insts)
     mine = list(range(n_all))
     if world > 1:
-        costs = [instance_cost(i['desc'].Nt, i['desc'].L) for i in insts]
+        costs = [i['desc'].cost for i in insts]
         mine = partition_instances(costs, world)[rank]
         insts, fields = [insts[i] for i in mine], [fields[i] for i in mine]
     bp = BatchedPropagator(insts, precision='single', device=dev)
@@ -248,6 +252,22 @@ def run_batched1d(dev, rank=0, world=1, accuracy=False):
     torch.cuda.synchronize()
     sec = e0.elapsed_time(e1) / 1e3
     att = [r.attempts for r in res]
+    busy, span = ctypes.c_double(), ctypes.c_double()
+    from project_b200 import _lib
+    _lib.check(bp._lib.uppe1d_last_activity(bp._plan, ctypes.byref(busy), ctypes.byref(span), _lib.stream_ptr()),
+               'uppe1d_last_activity')
+    # FLOP model of one attempt of an N-point line: 4 nonlinear evaluations (the
+    # first stage is carried over), each with 3 line FFTs (5 N log2 N) and ~80 N
+    # pointwise operations (stage algebra, Kerr, steepening, plasma scan)
+    nts = [int(i['desc'].Nt) for i in insts]
+    flops = sum(a * 4 * (3 * 5 * n * np.log2(n) + 80 * n) for a, n in zip(att, nts))
+    fp32_nominal = 148 * 128 * 2 * 1.965e9
+    occupancy = {'sm_busy': busy.value, 'span_ms': span.value,
+                 'how': 'persistent CTAs record the global timer at start and when the queue runs dry; '
+                        'sum(exit - start) / (148 SMs x span)',
+                 'flop_model': '4 evaluations x (3 x 5 N log2 N + 80 N) per attempt',
+                 'tflops': flops / sec / 1e12, 'fp32_frac_nominal': flops / sec / fp32_nominal,
+                 'fp32_peak_nominal_tflops': fp32_nominal / 1e12}
     acc = None
     if accuracy and world == 1:
         try:
@@ -263,10 +283,11 @@ def run_batched1d(dev, rank=0, world=1, accuracy=False):
         att = [merged[i]['attempts'] for i in range(n_all)]
         res = [type('R', (), merged[i]) for i in range(n_all)]
     return {'value': n_all / sec, 'unit': 'sims/s', 'n_instances': n_all, 'seconds': sec, 'ranks': world,
+            'kernel': 'four-CTA clusters per line' if bp._lib.uppe1d_uses_clusters(bp._plan) else 'one CTA per line',
             'attempts_total': int(sum(att)), 'attempts_max': int(max(att)),
             'status_nonzero': int(sum(1 for r in res if r.status)), 'dtype': 'c64',
             'workload': 'batched 1D sweep, 256 argon-capillary instances, L = 1 m, tol 1e-6, '
-                        'one persistent launch', 'accuracy': acc}
+                        'one persistent launch', 'occupancy': occupancy, 'accuracy': acc}
 
 
 def batched1d_accuracy(bp, insts, packed0, final64, dev):
@@ -294,6 +315,20 @@ def batched1d_accuracy(bp, insts, packed0, final64, dev):
     rels = np.array(rels)
     worst = [{'Nt': int(insts[sub[j]]['desc'].Nt), 'attempts_c128': int(r2[j].attempts),
               'relL2': float(rels[j])} for j in np.argsort(rels)[::-1][:3]]
+    # conditioning of those instances: complex128 runs from the same input and from
+    # the input times (1 + 1e-7 xi), xi complex unit-variance noise (seeded)
+    wk = [sub[j] for j in np.argsort(rels)[::-1][:3]]
+    bw = BatchedPropagator([insts[k] for k in wk], precision='double', device=dev)
+    fa = torch.cat([packed0[off[k]:off[k + 1]] for k in wk]).to(torch.complex128).contiguous()
+    g = torch.Generator(device='cpu').manual_seed(7)
+    xi = torch.complex(torch.randn(fa.shape, generator=g, dtype=torch.float64),
+                       torch.randn(fa.shape, generator=g, dtype=torch.float64)).to(dev) / np.sqrt(2.0)
+    fb = (fa * (1 + 1e-7 * xi)).contiguous()
+    bw.run_packed(fa)
+    bw.run_packed(fb)
+    for j in range(len(wk)):
+        worst[j]['c128_input_1e-7_perturbed_relL2'] = _rel(fb[bw.offsets[j]:bw.offsets[j + 1]],
+                                                          fa[bw.offsets[j]:bw.offsets[j + 1]])
     # the same comparison on the same steps: complex128 replays of each instance's
     # complex64 step log; a replay whose energy leaves the complex64 run's by more
     # than 1 % (a step accepted in one precision is unstable in the other) is counted
@@ -414,7 +449,7 @@ def run_gradients(dev, accuracy=False):
 
     def frozen_loss(cv, gv, solver):
         with torch.no_grad():
-            A = solver.replay(obj.input_field(cv, gv).to(solver.complex_dtype), steps)
+            A = solver.replay(obj.input_field(cv, gv).to(solver.complex_dtype), steps)   # obj, steps: current
             a = A[obj.ix, obj.iy, :].to(torch.complex128)
             return float(-(a.real ** 2 + a.imag ** 2).sum() * solver.dt)
 
@@ -449,7 +484,25 @@ def run_gradients(dev, accuracy=False):
             f3['accuracy'] = {'L_m': Lfd, 'relL2_exit_c64_vs_c128_same_steps': _rel(o64, o128), 'tolerance': 1e-4,
                               'loss_c64': frozen_loss(cd, gdd.detach(), sol),
                               'loss_c128': frozen_loss(cd, gdd.detach(), s128)}
-        del s128
+        # the same check with the complex128 plan: its adjoint against central
+        # differences of its own frozen-step map (separates the adjoint from the
+        # rounding of the mixed map)
+        obj128 = FilamentZernike(s128, w0=1e-3, energy=1.5e-3, fwhm=50e-15, aperture_radius=2e-3)
+        c2 = cd.clone().requires_grad_(True)
+        g2 = gdd.detach().clone().requires_grad_(True)
+        l128 = obj128.loss(c2, g2, Lfd, tol=1e-4, K=32)
+        gc2, gg2 = torch.autograd.grad(l128, [c2, g2])
+        steps_saved = steps
+        steps = np.array(Propagate3D.last_steps)
+        obj_saved, obj = obj, obj128
+        fd2_c = (frozen_loss(cd + e, gdd.detach(), s128) - frozen_loss(cd - e, gdd.detach(), s128)) / (2 * dc)
+        fd2_g = (frozen_loss(cd, gdd.detach() + dg, s128) - frozen_loss(cd, gdd.detach() - dg, s128)) / (2 * dg)
+        obj, steps = obj_saved, steps_saved
+        f3['central_difference_complex128'] = {
+            'zernike_index': j, 'adjoint': float(gc2[j]), 'fd': fd2_c,
+            'adjoint_gdd_per_fs2': float(gg2) * 1e-30, 'fd_gdd_per_fs2': fd2_g * 1e-30,
+            'grad_relL2_mixed_vs_c128': float(torch.linalg.vector_norm(gc - gc2) / torch.linalg.vector_norm(gc2))}
+        del s128, obj128
         torch.cuda.empty_cache()
     out['filament_3d'] = f3
     return out
@@ -542,7 +595,8 @@ def profile_kernels(sol, lib, n_attempts=3):
         for i in range(n.value):
             if byts[i] == 0:
                 continue
-            name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space', 4: 'k_ypass_tma'}.get(kind[i], 'scalar')
+            name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space', 4: 'k_ypass_tma',
+                    5: 'k_ypass_rq'}.get(kind[i], 'scalar')
             a = agg.setdefault(name, [0.0, 0.0, 0])
             a[0] += ms[i]
             a[1] += byts[i]
@@ -739,14 +793,16 @@ def plan_tuning(sol):
     """The launch configuration the plan's tuner picked, with the candidates' times."""
     import ctypes
     from project_b200 import _lib
-    cfg = (ctypes.c_int * 5)()
-    ms = (ctypes.c_float * 8)()
+    cfg = (ctypes.c_int * 6)()
+    ms = (ctypes.c_float * _lib.UPPE3D_TUNE_SLOTS)()
     _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
-    names = ['tma 2/SM', 'tma 1/SM', 'tma late 3/SM', 'tma late 2/SM']
-    return {'y_pass': ('plain' if not cfg[0] else f"tma{' late' if cfg[2] else ''} {cfg[1]}/SM"),
-            't_lines_per_block': cfg[3], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[4]],
-            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:4]) if v > 0},
-            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[5:7]) if v > 0}}
+    names = ['tma16 2/SM', 'tma16 1/SM', 'tma16 late 3/SM', 'tma16 late 2/SM', 'tma8 4/SM', 'tma8 late 6/SM',
+             'reg4step 2/SM', 'reg4step late 3/SM']
+    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step'}[cfg[0]]
+    y = kind if not cfg[0] else f"{kind}{' late' if cfg[2] else ''} {cfg[1]}/SM"
+    return {'y_pass': y, 't_lines_per_block': cfg[4], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[5]],
+            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:8]) if v > 0},
+            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[8:10]) if v > 0}}
 
 
 def run_b200(args, rank, world, local_rank):
@@ -950,26 +1006,44 @@ def run_b200(args, rank, world, local_rank):
 
 
 def run_profile_case(args):
-    """Only the propagator: set up, warm up, run the timed attempts, print timing."""
+    """Only the propagator, for profiler commands: position the 2 m run at z =
+    --profile-z (untimed), warm up, then run the timed attempts inside an NVTX
+    range named "timed" (ncu --nvtx --nvtx-include "timed/" captures only those).
+    --profile-table mpi uses the multiphoton table (ionising filament); --profile-grid
+    N runs an N x N x 512 grid over the same 6 mm (a smaller case for full captures);
+    --profile-tuning Y,C,L,K,W forces the launch configuration (uppe3d_set_tuning:
+    y kernel, CTAs per SM, late loads, omega columns, t-lines per block), since the
+    tuner's own timings shift under a profiler."""
     import torch
     from project_b200 import _lib
     from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
-    x, y, t = grids()
+    n = args.profile_grid
+    x, y, t = grids(n)
     cdt = np.complex64 if args.precision == 'single' else np.complex128
-    sol = ERK43IP_UPPE_3D_Optimized(x, y, t, argon_medium(args.precision), precision=args.precision)
+    med = mpi_argon(args.precision) if args.profile_table == 'mpi' else argon_medium(args.precision)
+    sol = ERK43IP_UPPE_3D_Optimized(x, y, t, med, precision=args.precision)
+    if args.profile_tuning:
+        cfg = [int(v) for v in args.profile_tuning.split(',')]
+        _lib.check(sol._lib.uppe3d_set_tuning(sol._plan, *cfg), 'uppe3d_set_tuning')
     sol.set_field(torch.from_numpy(make_input(x, y, t, cdt)).cuda())
     lib, s = sol._lib, _lib.stream_ptr()
     _lib.check(lib.uppe3d_begin(sol._plan, L_PROP, TOL, 1e-2, 1e-9, 0, s), 'begin')
+    if args.profile_z > 0:
+        run_chunks(sol, 10 ** 6, 4, stop=lambda r: r.z >= args.profile_z)
     _lib.check(lib.uppe3d_run_steps(sol._plan, args.warmup, s), 'warmup')
     torch.cuda.synchronize()
+    lines = line_stats(sol, med)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push('timed')
     e0.record()
     _lib.check(lib.uppe3d_run_steps(sol._plan, args.steps, s), 'run')
     e1.record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     r = sol.result()
     print(json.dumps({'ms_per_attempt': e0.elapsed_time(e1) / args.steps, 'attempts': r.attempts,
-                      'accepted': r.accepted, 'z': r.z, 'status': r.status}), flush=True)
+                      'accepted': r.accepted, 'z': r.z, 'status': r.status, 'grid': [n, n, NT],
+                      'table': args.profile_table, 'lines': lines}), flush=True)
     return 0
 
 
@@ -989,6 +1063,10 @@ def main():
     ap.add_argument('--no-ionising', action='store_true')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
+    ap.add_argument('--profile-z', type=float, default=0.0, help='profile case: start the timed attempts at z')
+    ap.add_argument('--profile-table', default='adk', choices=['adk', 'mpi'])
+    ap.add_argument('--profile-grid', type=int, default=NX)
+    ap.add_argument('--profile-tuning', default='', help='profile case: y_tma,y_ctas,y_late,y_kw,t_wpb')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))

@@ -175,6 +175,17 @@ typedef struct uppe1d_plan uppe1d_plan;
 int uppe1d_plan_create(const uppe1d_desc* desc, uppe1d_plan** plan);
 int uppe1d_plan_destroy(uppe1d_plan* plan);
 long long uppe1d_field_elems(const uppe1d_plan* plan);   /* sum Nt                   */
+/* Clusters of the plan's four-CTA line kernel (0: one CTA per line).  A plan whose
+ * lines are all 2048..16384 points without Raman or history, one of them at least
+ * 8192, runs each line on a cluster of four SMs sharing it through distributed
+ * shared memory (no reference counterpart: the reference runs one line at a time
+ * on the CPU).  UPPE_1D_CLUSTER=0 keeps one CTA per line where that can hold it. */
+int uppe1d_uses_clusters(const uppe1d_plan* plan);
+/* SM occupancy of the plan's last propagation launch (no reference counterpart):
+ * each persistent CTA records the global timer when it starts and when the work
+ * queue runs dry; sm_busy = sum over CTAs of (exit - start) / (SMs x span), span =
+ * last exit - first start.  Synchronises the stream. */
+int uppe1d_last_activity(uppe1d_plan* plan, double* sm_busy, double* span_ms, uppe_stream_t stream);
 long long uppe1d_hist_elems(const uppe1d_plan* plan);    /* sum hist_cap * Nt        */
 long long uppe1d_hist_slots(const uppe1d_plan* plan);    /* sum hist_cap             */
 /* propagate (erk43ip_method.py:288-369) for every instance.  field: device,
@@ -239,6 +250,12 @@ typedef struct {
   double aval_coef;        /* W_ava = aval_coef I_equiv (0 for the gases)              */
   double chi3e, chi5e;     /* eps0 chi3, eps0 chi5: P = chi3e E^3 + chi5e E^5 (:300-312) */
   double rate_rec, rho_nt, Ui, e_charge, m_e, tau_c;   /* density / Drude constants (:11-118) */
+  /* Raman response of fused silica (media_physics.py:303-305, 362-390): NULL for none;
+   * else H(omega_k), k = 0..Nt, of the 2 Nt-point response (interleaved re, im: 2 (Nt+1)
+   * doubles) and its fraction: E_eff^2 = (1 - f_R) E^2 + f_R (the zero-padded E^2
+   * convolved circularly over 2 Nt samples with the response), P = chi3e E E_eff^2. */
+  const double* raman_H;
+  double raman_fR;
 } uppe_rf_desc;
 
 typedef struct uppe_rf_plan uppe_rf_plan;
@@ -382,26 +399,34 @@ int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, do
 
 /* Launch configuration chosen for the plan's shape by the tuner that runs in
  * uppe3d_plan_create (no reference counterpart: the reference leaves kernel
- * choice to cuFFT).  Candidates: y passes on the TMA-fed kernel (stage operands
- * loaded before the tile's wait with 1 or 2 CTAs per SM, or where they are used
- * with 3 or 2; complex64 plans with 64 <= Ny <= 256), and 4 or 8 t-lines per
- * block of the warp t-line kernel.  All candidates compute identical bits (the
- * plain tile kernel, which rounds differently, serves the other shapes).  cfg5 =
- * {TMA y passes, CTAs per SM, late operand loads, t-lines per block, 1 timed / 2
- * from the process cache / 0 defaults (UPPE_TUNE=0)}; ms8 (may be NULL):
- * per-attempt time of the y passes for the four y candidates [0..3] and of the t
- * passes for 8 and 4 lines per block [5..6], in ms (0 when not timed). */
-int uppe3d_tuning(const uppe3d_plan* plan, int* cfg5, float* ms8);
-/* Force a launch configuration (y_tma 0 selects the plain tile kernel; y_ctas
- * 1..3, t_wpb 4 or 8) and re-capture the attempt graphs; for comparing the
+ * choice to cuFFT).  Candidates: y passes on the TMA-fed kernel with tiles of 16
+ * omega columns (stage operands loaded before the tile's wait with 2 or 1 CTAs
+ * per SM, or where they are used with 3 or 2) or of 8 columns (early with 4,
+ * late with 6 CTAs per SM) -- complex64 plans with 64 <= Ny <= 256 -- then, for
+ * Ny = 256, on the register four-step kernel (operands loaded with the tile, 2
+ * CTAs per SM, or where used, 3), and 8 or 4 t-lines per block of the warp
+ * t-line kernel.  All candidates compute identical bits (the plain tile kernel,
+ * which rounds differently, serves the other shapes).  cfg6 = {y kernel (1
+ * TMA-fed, 2 register four-step, 0 plain tile), CTAs per SM, late operand loads,
+ * omega columns per tile, t-lines per block, 1 timed / 2 from the process cache
+ * / 0 defaults (UPPE_TUNE=0)}; ms (may be NULL, UPPE3D_TUNE_SLOTS floats):
+ * per-attempt time of the y passes for the eight y candidates in that order
+ * [0..7] and of the t passes for 8 and 4 lines per block [8..9], in ms (0 when
+ * not timed). */
+#define UPPE3D_TUNE_SLOTS 10
+int uppe3d_tuning(const uppe3d_plan* plan, int* cfg6, float* ms);
+/* Force a launch configuration (y_tma 1 TMA-fed, 2 register four-step -- Ny =
+ * 256 complex64 only --, 0 the plain tile kernel; y_ctas 1..6, y_kw 16 or 8,
+ * t_wpb 4 or 8) and re-capture the attempt graphs; for comparing the
  * candidates. */
-int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int t_wpb);
+int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,
  * bracketing each launch with CUDA events on `stream`.  Writes per launch its
- * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar, 4 TMA-fed y-pass) and algorithmic
+ * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar, 4 TMA-fed y-pass, 5 register
+ * four-step y-pass) and algorithmic
  * bytes (0 for launches the device state made exit early). */
 int uppe3d_profile_attempt(uppe3d_plan* plan, int cap, float* ms, int* kind, double* bytes,
                            int* n, uppe_stream_t stream);

@@ -1,15 +1,30 @@
 """Recipe: compile the reference's CUDA-C plasma kernel source
 (src/3+1D-UPPE-ERK4(3)IP-envelope/media_physics.py:11-67) as host C++ into
 oracle/_ref/ (test infrastructure).  The source string is read out of the
-reference file; nothing is copied into this repository."""
+reference file; nothing is copied into this repository.
+
+The reference tree is the first command-line argument, else the environment
+variable UPPE_REFERENCE, else the development container's checkout."""
 import ast
 import hashlib
 import os
 import subprocess
+import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 OUT = os.path.join(HERE, '_ref')
-REF_MEDIA = os.path.join('/root/reference', 'src', '3+1D-UPPE-ERK4(3)IP-envelope', 'media_physics.py')
+MEDIA_REL = os.path.join('src', '3+1D-UPPE-ERK4(3)IP-envelope', 'media_physics.py')
+
+
+def reference_root(argv=None):
+    argv = sys.argv if argv is None else argv
+    if __name__ == '__main__' and len(argv) > 1:
+        return argv[1]
+    return os.environ.get('UPPE_REFERENCE', '/root/reference')
+
+
+def media_path(root=None):
+    return os.path.join(root or reference_root(), MEDIA_REL)
 
 PRELUDE = r'''
 #include <math.h>
@@ -34,8 +49,8 @@ extern "C" void _launch_plasma_integration_kernel(unsigned grid, unsigned block,
 '''
 
 
-def kernel_source(path=REF_MEDIA):
-    tree = ast.parse(open(path, encoding='utf-8').read())
+def kernel_source(path=None):
+    tree = ast.parse(open(path or media_path(), encoding='utf-8').read())
     for node in tree.body:
         if isinstance(node, ast.Assign) and any(getattr(t, 'id', '') == 'PLASMA_KERNEL_CODE'
                                                 for t in node.targets):

@@ -16,6 +16,8 @@ UPPE_C64, UPPE_C128 = 0, 1
 STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS, STATUS_RETRIED = 1, 2, 4, 64
 # line limits of uppe1d_propagate_noalloc (its static device array)
 UPPE_NOALLOC_MAX_NT_C64, UPPE_NOALLOC_MAX_NT_C128 = 16384, 8192
+# timing slots of uppe3d_tuning: eight y-pass candidates, then two t-pass ones
+UPPE3D_TUNE_SLOTS = 10
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -63,7 +65,7 @@ class DescRF(ctypes.Structure):
                 ('kk', _P), ('kref', _P), ('w', _P), ('filt', _P), ('kperp2', _P), ('damp', _P),
                 ('lut_n', _I), ('lut_log10I', _P), ('lut_W', _P), ('I_coef', _D), ('aval_coef', _D),
                 ('chi3e', _D), ('chi5e', _D), ('rate_rec', _D), ('rho_nt', _D), ('Ui', _D),
-                ('e_charge', _D), ('m_e', _D), ('tau_c', _D)]
+                ('e_charge', _D), ('m_e', _D), ('tau_c', _D), ('raman_H', _P), ('raman_fR', _D)]
 
 
 class Op1D(ctypes.Structure):
@@ -115,12 +117,14 @@ SIGNATURES = {
     'uppe1d_adjoint': (_I, [_P, _I, _P, _I, _I, _P, _P, _P, _P, _P, _P, _P, _P, _P]),
     'uppe1d_propagate_noalloc': (_I, [ctypes.POINTER(InstDesc1D), _I, _P, _P, _P, _I, _P, _P, _P,
                                       ctypes.POINTER(Result1D), _P]),
+    'uppe1d_last_activity': (_I, [_P, ctypes.POINTER(_D), ctypes.POINTER(_D), _P]),
+    'uppe1d_uses_clusters': (_I, [_P]),
     'uppe_fft_c128': (_I, [_P, _P, _P, _I, _I, _D, _I, _I, _P]),
     'uppe_spectral_phase': (_I, [_P, _I, _D, _D, _D, _P]),
     'uppe_exact_ft': (_I, [_P, _I, _P, _P, _I, _P, _P]),
     'uppe3d_transform_t': (_I, [_P, _P, _P, _I, _D, _P]),
     'uppe3d_tuning': (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
-    'uppe3d_set_tuning': (_I, [_P, _I, _I, _I, _I]),
+    'uppe3d_set_tuning': (_I, [_P, _I, _I, _I, _I, _I]),
     'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),
                                     ctypes.POINTER(_D), ctypes.POINTER(_I), _P]),
 }

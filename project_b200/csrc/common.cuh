@@ -33,21 +33,22 @@ template <int DIR, typename C> __device__ __forceinline__ C mul_pmi(C a) {
 }
 template <typename C> __device__ __forceinline__ C czero() { return {0, 0}; }
 
-// exp(DIR * 2 pi i k / R) as compile-time constants for R <= 16
+// exp(DIR * 2 pi i k / R) as compile-time constants for R dividing 32: the angle
+// index on the 32-grid is exact for every such R (cos and sin of 2 pi i / 32 for
+// i = 0..8; the values of the 16-grid are the even entries)
 template <int R, int K> struct Twid {
-  static constexpr int k16 = (K * 16 / R) % 16;   // angle index on the 16-grid
-  __host__ __device__ static constexpr double kc(int i) {
-    return i == 0 ? 1.0 : i == 1 ? 0.92387953251128675613 : i == 2 ? 0.70710678118654752440
-         : i == 3 ? 0.38268343236508977173 : i == 4 ? 0.0 : i == 5 ? -0.38268343236508977173
-         : i == 6 ? -0.70710678118654752440 : -0.92387953251128675613;
+  static_assert(R > 0 && 32 % R == 0, "compile-time twiddles cover R | 32");
+  static constexpr int k32 = (K * (32 / R)) % 32;   // angle index on the 32-grid
+  __host__ __device__ static constexpr double c32(int i) {   // cos(2 pi i / 32), 0 <= i <= 8
+    return i == 0 ? 1.0 : i == 1 ? 0.98078528040323044913 : i == 2 ? 0.92387953251128675613
+         : i == 3 ? 0.83146961230254523708 : i == 4 ? 0.70710678118654752440 : i == 5 ? 0.55557023301960222474
+         : i == 6 ? 0.38268343236508977173 : i == 7 ? 0.19509032201612826785 : 0.0;
   }
-  __host__ __device__ static constexpr double ks(int i) {
-    return i == 0 ? 0.0 : i == 1 ? 0.38268343236508977173 : i == 2 ? 0.70710678118654752440
-         : i == 3 ? 0.92387953251128675613 : i == 4 ? 1.0 : i == 5 ? 0.92387953251128675613
-         : i == 6 ? 0.70710678118654752440 : 0.38268343236508977173;
-  }
-  static constexpr double cv = k16 < 8 ? kc(k16) : -kc(k16 - 8);
-  static constexpr double sv = k16 < 8 ? ks(k16) : -ks(k16 - 8);
+  // first half turn: i in [0, 16); cos = c32(i) on [0, 8], -c32(16 - i) above
+  __host__ __device__ static constexpr double kc(int i) { return i <= 8 ? c32(i) : -c32(16 - i); }
+  __host__ __device__ static constexpr double ks(int i) { return i <= 8 ? c32(8 - i) : c32(i - 8); }
+  static constexpr double cv = k32 < 16 ? kc(k32) : -kc(k32 - 16);
+  static constexpr double sv = k32 < 16 ? ks(k32) : -ks(k32 - 16);
 };
 
 // x * exp(DIR * 2 pi i K / R)

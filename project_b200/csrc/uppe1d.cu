@@ -28,6 +28,7 @@ struct uppe1d_plan {
   bool use_cl = false;    // lines run on four-CTA clusters (uppe1d_cluster.cuh)
   int ncl = 0;            // clusters of the persistent cluster launch
   size_t cl_smem = 0;
+  int last_ctas = 0;      // CTAs of the last propagation launch (activity record)
   Batch1D b;
   Inst1D* d_inst;
   std::vector<Inst1D> h_inst;
@@ -247,19 +248,51 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     p->b.cl_scratch_bytes = (long long)(dbl ? cl_scratch_bytes<double>(nmax) : cl_scratch_bytes<float>(nmax));
     TRY1(up1(p, &ptr, nullptr, (size_t)p->b.cl_scratch_bytes * p->ncl)); p->b.cl_scratch = ptr;
   }
+  {
+    // activity record: two timer values per CTA of the widest launch
+    const int ctas = std::max(p->nblocks, kCS * p->ncl);
+    TRY1(up1(p, &ptr, nullptr, 2 * sizeof(unsigned long long) * (size_t)ctas));
+    p->b.busy = static_cast<unsigned long long*>(ptr);
+  }
 #undef TRY1
   *out = p;
   return 0;
 }
 
 // the propagation kernel of the plan: four-CTA clusters per line, or one CTA per line
-static cudaError_t launch_lines(const uppe1d_plan* p, const Batch1D& b, cudaStream_t s) {
+static cudaError_t launch_lines(uppe1d_plan* p, const Batch1D& b, cudaStream_t s) {
+  p->last_ctas = p->use_cl ? kCS * p->ncl : p->nblocks;
   if (p->use_cl)
     return p->dbl ? launch_uppe1d_cl<double>(b, p->ncl, p->cl_smem, s) : launch_uppe1d_cl<float>(b, p->ncl, p->cl_smem, s);
   return p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s) : launch_uppe1d<float>(b, p->nblocks, p->smem, s);
 }
 
+// SM occupancy of the last propagation launch from the CTAs' timer records: the
+// persistent CTAs (one per SM) stay busy until the work queue runs dry, so
+// sum(exit - start) / (SMs x span) is the fraction of the GPU's SM-time spent on
+// instances.  Synchronises the stream.
+extern "C" int uppe1d_last_activity(uppe1d_plan* p, double* sm_busy, double* span_ms, cudaStream_t s) {
+  if (!p || !sm_busy || !span_ms || p->last_ctas <= 0) return UPPE_ERR_ARG;
+  std::vector<unsigned long long> t(2 * (size_t)p->last_ctas);
+  UPPE1_CK(cudaMemcpyAsync(t.data(), p->b.busy, t.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
+  UPPE1_CK(cudaStreamSynchronize(s));
+  unsigned long long t0 = ~0ull, t1 = 0;
+  double sum = 0.0;
+  for (int c = 0; c < p->last_ctas; ++c) {
+    const unsigned long long a = t[2 * c], e = t[2 * c + 1];
+    if (e < a) return UPPE_ERR_ARG;   // a CTA that never recorded its exit
+    t0 = std::min(t0, a);
+    t1 = std::max(t1, e);
+    sum += (double)(e - a);
+  }
+  const double span = (double)(t1 - t0);
+  *span_ms = span * 1e-6;
+  *sm_busy = span > 0.0 ? sum / (span * (double)p->nsm) : 0.0;
+  return 0;
+}
+
 extern "C" long long uppe1d_field_elems(const uppe1d_plan* p) { return p ? p->ftotal : 0; }
+extern "C" int uppe1d_uses_clusters(const uppe1d_plan* p) { return p && p->use_cl ? p->ncl : 0; }
 extern "C" long long uppe1d_hist_elems(const uppe1d_plan* p) { return p ? p->htotal : 0; }
 extern "C" long long uppe1d_hist_slots(const uppe1d_plan* p) { return p ? p->zhtotal : 0; }
 
@@ -433,6 +466,7 @@ extern "C" int uppe1d_run_programs(uppe1d_plan* p, int nprog, const long long* o
   b.hlog = nullptr;
   b.hsched = nullptr;
   UPPE1_CK(cudaMemsetAsync(p->b.counter, 0, sizeof(int), s));
+  p->last_ctas = nb;
   UPPE1_CK(p->dbl ? launch_uppe1d<double>(b, nb, p->smem, s) : launch_uppe1d<float>(b, nb, p->smem, s));
   if (op_results) {
     std::vector<Res1D> hr(nops);

@@ -36,8 +36,17 @@ __host__ __device__ constexpr long long cl_xtw_offset(int M) { return 3LL * (M -
 
 template <typename Rl> struct ClCtx {
   using C = typename CT<Rl>::T;
-  C* line;               // shared: this CTA's block of the line
-  C* buf;                // shared: the other buffer of the cross step
+  // the two line buffers at the start of the dynamic shared memory (PAD elements
+  // each), addressed through the shared array itself so that accesses compile to
+  // shared-memory instructions; cur selects the one that holds the line
+  int cur;
+  int pad;
+  __device__ __forceinline__ C* sbase() const {
+    extern __shared__ __align__(16) unsigned char smem[];
+    return reinterpret_cast<C*>(smem);
+  }
+  __device__ __forceinline__ C* line() const { return sbase() + cur * pad; }
+  __device__ __forceinline__ C* buf() const { return sbase() + (cur ^ 1) * pad; }
   double* red;           // shared: 64 doubles (block sums)
   double* starts;        // shared: density at the start of each chunk (T1)
   double* slot;          // shared: 8 doubles exchanged across the cluster
@@ -70,33 +79,35 @@ __device__ __forceinline__ void cl_cross(ClCtx<Rl>& c, cg::cluster_group& cl) {
   cl.sync();                                   // every CTA's line is complete
   C* rem[kCS];
 #pragma unroll
-  for (int q = 0; q < kCS; ++q) rem[q] = cl.map_shared_rank(c.line, q);
+  for (int q = 0; q < kCS; ++q) rem[q] = cl.map_shared_rank(c.line(), q);
   const int r = c.r;
+  // all of a thread's remote loads in flight together (M / T1 <= 8 iterations)
+#pragma unroll
   for (int m = threadIdx.x; m < M; m += T1) {
     C acc = rem[0][pad1(m)];
 #pragma unroll
     for (int q = 1; q < kCS; ++q) acc = cadd(acc, w4<DIR>(rem[q][pad1(m)], q * r));
     if (DIR < 0 && r > 0) acc = cmul(acc, c.xtw[(r - 1) * M + m]);
-    c.buf[pad1(m)] = acc;
+    c.buf()[pad1(m)] = acc;
   }
   cl.sync();                                   // every CTA has read the lines
-  C* t = c.line; c.line = c.buf; c.buf = t;
+  c.cur ^= 1;
 }
 
 // time domain (CTA r: samples r M + m) -> omega domain (CTA r: bins r + 4 j)
 template <typename Rl, int M>
 __device__ __forceinline__ void cl_fft_fwd(ClCtx<Rl>& c, cg::cluster_group& cl) {
   cl_cross<Rl, M, -1>(c, cl);
-  line_fft<M, -1>(c.line, c.tw, threadIdx.x);
+  line_fft<M, -1>(c.line(), c.tw, threadIdx.x);
 }
 
 // omega domain -> time domain, unnormalised
 template <typename Rl, int M>
 __device__ __forceinline__ void cl_fft_inv(ClCtx<Rl>& c, cg::cluster_group& cl) {
   using C = typename CT<Rl>::T;
-  line_fft<M, +1>(c.line, c.tw, threadIdx.x);
+  line_fft<M, +1>(c.line(), c.tw, threadIdx.x);
   if (c.r > 0) {
-    for (int m = threadIdx.x; m < M; m += T1) c.line[pad1(m)] = cmul(c.line[pad1(m)], cconj(c.xtw[(c.r - 1) * M + m]));
+    for (int m = threadIdx.x; m < M; m += T1) c.line()[pad1(m)] = cmul(c.line()[pad1(m)], cconj(c.xtw[(c.r - 1) * M + m]));
   }
   cl_cross<Rl, M, +1>(c, cl);
 }
@@ -146,13 +157,13 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
   const PlasmaConst& m = c.in->pc;
   const double Aeff = c.in->A_eff;
   const AffineStep aff(m);
-  for (int t = tid; t < M; t += T1) c.line[pad1(t)] = c.GA[t];
+  for (int t = tid; t < M; t += T1) c.line()[pad1(t)] = c.GA[t];
   __syncthreads();
   bool any_w = false, ok = (m.ava == 0.0);
   double cm = 1.0, dm = 0.0;
   if (tid < NA) {
     for (int t = tid * CH; t < tid * CH + CH; ++t) {
-      const C a = c.line[pad1(t)];
+      const C a = c.line()[pad1(t)];
       const Rl I = (Rl)(((double)a.x * a.x + (double)a.y * a.y) / Aeff);
       const double w = (double)(float)lut_eval<Rl>(c.lut, I);
       any_w |= (w != 0.0);
@@ -214,7 +225,7 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
         double rho = q == 0 ? 0.0 : *cl.map_shared_rank(&c.slot[6], q - 1);
         for (int t = 0; t < M; ++t) {
           if (t % CH == 0) c.starts[t / CH] = rho;
-          const C a = c.line[pad1(t)];
+          const C a = c.line()[pad1(t)];
           const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
           const double w = (double)(float)lut_eval<Rl>(c.lut, (Rl)Id);
           const double wa = (double)(float)(m.ava * (double)(Rl)Id);
@@ -232,7 +243,7 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
   if (tid < NA) {
     double rho = rho0;
     for (int t = tid * CH; t < tid * CH + CH; ++t) {
-      const C a = c.line[pad1(t)];
+      const C a = c.line()[pad1(t)];
       const double Id = ((double)a.x * a.x + (double)a.y * a.y) / Aeff;
       const Rl I = (Rl)Id;
       const double w = (double)(float)lut_eval<Rl>(c.lut, I);
@@ -243,7 +254,7 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
       const double loss = -(gen * m.Ui) / (2.0 * (double)I + 1e-30);
       const double cr = loss - m.sigma_half * rho_t;
       const double ci = -m.sigma_half * m.w0tc * rho_t;
-      c.line[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
+      c.line()[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
     }
   }
   const double mx = cl_max(c, cl, ion / m.rho_nt);
@@ -262,13 +273,13 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
   const Rl hR = (Rl)h, h2 = (Rl)(h / 2), h6 = (Rl)(h / 6);
   double nrm = 0.0;
   if (mode == IN_A) {
-    for (int w = tid; w < M; w += T1) c.line[pad1(w)] = c.A[w];
+    for (int w = tid; w < M; w += T1) c.line()[pad1(w)] = c.A[w];
   } else if (mode == IN_5) {
     for (int w = tid; w < M; w += T1) {
       const C u = cadd(c.T[w], cscale(c.A4P[w], h6));
       c.A4[w] = u;
       nrm += (double)u.x * u.x + (double)u.y * u.y;
-      c.line[pad1(w)] = u;
+      c.line()[pad1(w)] = u;
     }
   } else {
     const C* X = mode == IN_2 ? c.K1 : c.O;
@@ -289,7 +300,7 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
         c.T[w] = cmul(cadd(v, cscale(ts, h6)), E);    // beta
         u = cmul(cadd(v, cscale(xx, hR)), E);
       }
-      c.line[pad1(w)] = u;
+      c.line()[pad1(w)] = u;
     }
   }
   __syncthreads();
@@ -297,15 +308,15 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
   const Rl invN = (Rl)(1.0 / N);
   const bool plasma = c.in->plasma;
   for (int t = tid; t < M; t += T1) {
-    const C a = cscale(c.line[pad1(t)], invN);
+    const C a = cscale(c.line()[pad1(t)], invN);
     if (plasma) c.GA[t] = a;
     const Rl I = a.x * a.x + a.y * a.y;
-    c.line[pad1(t)] = cscale(a, I);
+    c.line()[pad1(t)] = cscale(a, I);
   }
   __syncthreads();
   cl_fft_fwd<Rl, M>(c, cl);
   for (int w = tid; w < M; w += T1) {
-    const C p = c.line[pad1(w)];
+    const C p = c.line()[pad1(w)];
     const Rl gr = (Rl)c.G[w];
     out[w] = C{-gr * p.y, gr * p.x};     // i gamma U(w) P_NL(w)
   }
@@ -313,7 +324,7 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
   if (plasma && cl_plasma<Rl, M>(c, cl, ion_out)) {
     __syncthreads();
     cl_fft_fwd<Rl, M>(c, cl);
-    for (int w = tid; w < M; w += T1) out[w] = cadd(out[w], c.line[pad1(w)]);
+    for (int w = tid; w < M; w += T1) out[w] = cadd(out[w], c.line()[pad1(w)]);
     __syncthreads();
   }
   return mode == IN_5 ? cl_sum(c, cl, nrm) : 0.0;
@@ -358,9 +369,9 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   const Inst1D& in = b.inst[i];
   ClCtx<Rl> c;
   c.r = (int)cl.block_rank();
-  c.line = reinterpret_cast<C*>(smem);
-  c.buf = c.line + Cfg1<M>::PAD;
-  c.red = reinterpret_cast<double*>(c.buf + Cfg1<M>::PAD);
+  c.cur = 0;
+  c.pad = Cfg1<M>::PAD;
+  c.red = reinterpret_cast<double*>(reinterpret_cast<C*>(smem) + 2 * Cfg1<M>::PAD);
   c.starts = c.red + 64;
   c.slot = c.starts + T1;
   c.tw = reinterpret_cast<const C*>(b.tw) + (M - 1);
@@ -384,10 +395,10 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   c.in = &in;
   c.lut = b.lut;
   C* field = reinterpret_cast<C*>(b.field) + in.off + (long long)c.r * M;
-  for (int t = tid; t < M; t += T1) c.line[pad1(t)] = field[t];
+  for (int t = tid; t < M; t += T1) c.line()[pad1(t)] = field[t];
   __syncthreads();
   cl_fft_fwd<Rl, M>(c, cl);
-  for (int w = tid; w < M; w += T1) c.A[w] = c.line[pad1(w)];
+  for (int w = tid; w < M; w += T1) c.A[w] = c.line()[pad1(w)];
   __syncthreads();
   double ion_peak = 0.0, ion_cand = 0.0;
   cl_nl_eval<Rl, M>(c, cl, IN_A, 0.0, c.K1, &ion_peak);
@@ -468,11 +479,11 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
     en = cl_sum(c, cl, en) * in.dt / N;
     ph = cl_sum(c, cl, ph) * in.dt / N;
   }
-  for (int w = tid; w < M; w += T1) c.line[pad1(w)] = c.A[w];
+  for (int w = tid; w < M; w += T1) c.line()[pad1(w)] = c.A[w];
   __syncthreads();
   cl_fft_inv<Rl, M>(c, cl);
   const Rl invN = (Rl)(1.0 / N);
-  for (int t = tid; t < M; t += T1) field[t] = cscale(c.line[pad1(t)], invN);
+  for (int t = tid; t < M; t += T1) field[t] = cscale(c.line()[pad1(t)], invN);
   if (lead) {
     Res1D rr;
     rr.z = z; rr.h = h; rr.err = err; rr.attempts = attempts; rr.accepted = accepted;
@@ -490,12 +501,13 @@ __global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(T1, 1) k_uppe1d_cl
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_k;
   cg::cluster_group cl = cg::this_cluster();
+  mark_busy(b.busy, 0);
   for (;;) {
     if (cl.block_rank() == 0 && threadIdx.x == 0) s_k = atomicAdd(b.counter, 1);
     cl.sync();
     const int k = *cl.map_shared_rank(&s_k, 0);
     cl.sync();
-    if (k >= b.ninst) return;
+    if (k >= b.ninst) { mark_busy(b.busy, 1); return; }
     const int i = b.order[k];
     switch (b.inst[i].log2n) {
       case 11: cl_run_instance<Rl, 512>(b, i, smem, cl); break;

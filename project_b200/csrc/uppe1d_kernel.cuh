@@ -93,7 +93,17 @@ struct Batch1D {
   const void* xtw;               // cluster kernel: cross-CTA twiddles W_N^(m r) (or null)
   void* cl_scratch;              // cluster kernel: per-cluster scratch
   long long cl_scratch_bytes;
+  unsigned long long* busy;      // per CTA: globaltimer at start and at exit (or null)
 };
+
+// activity record of a persistent CTA (ns of the global timer)
+static __device__ __forceinline__ void mark_busy(unsigned long long* busy, int slot) {
+  if (busy && threadIdx.x == 0) {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    busy[2 * blockIdx.x + slot] = t;
+  }
+}
 
 template <int N> struct Cfg1 {
   static constexpr int FT = N / 2 < T1 ? N / 2 : T1;   // FFT team size
@@ -829,12 +839,13 @@ template <typename Rl>
 __global__ void __launch_bounds__(T1, 1) k_uppe1d(Batch1D b) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_k;
+  mark_busy(b.busy, 0);
   for (;;) {
     if (threadIdx.x == 0) s_k = atomicAdd(b.counter, 1);
     __syncthreads();
     const int k = s_k;
     __syncthreads();
-    if (k >= b.ninst) return;
+    if (k >= b.ninst) { mark_busy(b.busy, 1); return; }
     const int i = b.order[k];
     if (b.prog) {
       switch (b.prog[i].log2n) {

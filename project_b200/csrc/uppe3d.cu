@@ -207,6 +207,9 @@ struct SpaceArgs {
 template <typename C> struct TileIdx {
   __device__ __forceinline__ int operator()(int sig, int n) const { return n * kW + sig; }
 };
+template <int KW> struct TileIdxK {
+  __device__ __forceinline__ int operator()(int sig, int n) const { return n * KW + sig; }
+};
 struct BlockSync {
   __device__ __forceinline__ void operator()() const { __syncthreads(); }
 };
@@ -231,10 +234,10 @@ __device__ __forceinline__ void load_tile(C* s, const C* __restrict__ g, long lo
 #pragma unroll
   for (int k = 0; k < NV; ++k) sv[tid + k * NTHR] = r[k];
 }
-template <typename C, int N, int NTHR>
+template <typename C, int N, int NTHR, int KW = kW>
 __device__ __forceinline__ void store_tile(const C* s, C* __restrict__ g, long long base,
                                            long long stride, int tid) {
-  constexpr int VPR = kW * (int)sizeof(C) / 16;
+  constexpr int VPR = KW * (int)sizeof(C) / 16;
   float4* __restrict__ gv = reinterpret_cast<float4*>(g);
   const float4* sv = reinterpret_cast<const float4*>(s);
 #pragma unroll 4
@@ -788,13 +791,20 @@ __device__ __forceinline__ bool mbar_wait(unsigned bar, unsigned parity) {
 // wait (two CTAs per SM); LATE = 1: they are loaded where they are used (from L2,
 // where the previous tile prefetched them), which leaves room for three CTAs per
 // SM.  Same arithmetic either way.
-template <int N, int MODE, int LATE>
-__global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
+// KW omega columns per tile (16 or 8, 256 or 128 threads: the same radix plan per
+// column, so both compute the same bits); MINB resident CTAs per SM.
+template <int KW, int LATE> struct YTmaCfg {
+  static constexpr int NTHR = 16 * KW;
+  static constexpr int MINB = KW == 16 ? (LATE ? 3 : 2) : (LATE ? 6 : 4);
+};
+template <int N, int MODE, int LATE, int KW>
+__global__ void __launch_bounds__(YTmaCfg<KW, LATE>::NTHR, YTmaCfg<KW, LATE>::MINB)
+k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
   using C = float2;
   using Rl = float;
-  constexpr int NTHR = 256;
-  constexpr int E = N * kW / NTHR;
-  constexpr int TILE = N * kW;
+  constexpr int NTHR = YTmaCfg<KW, LATE>::NTHR;
+  constexpr int E = N * KW / NTHR;
+  constexpr int TILE = N * KW;
   // the dynamic window starts at offset 0 (no static shared memory here); the
   // buffers are TILE * 8 = 128 N bytes apart, so each starts 128-byte aligned
   extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -810,10 +820,10 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
   if (MODE == YMID1R && st->fresh) return;
   if (MODE == YMID1 && !st->fresh) return;
   const int Nt = a.g.Nt, Ny = a.g.Ny;
-  const int ntw = Nt / kW;
+  const int ntw = Nt / KW;
   const int total = a.g.Nx * ntw;
   auto issue = [&](int tile, int b) {
-    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const int o = tile / ntw, w0 = (tile % ntw) * KW;
     const unsigned bar = smem_u32(&mbar[b]);
     const CUtensorMap* map = MODE == YMID1R ? &maps.acur : &maps.in;
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -827,7 +837,7 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
   };
   // the next tile's stage operands into L2 (their loads below then hit L2)
   auto prefetch_ops = [&](int tile) {
-    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const int o = tile / ntw, w0 = (tile % ntw) * KW;
     auto pf = [&](const CUtensorMap* m) {
       asm volatile("cp.async.bulk.prefetch.tensor.3d.L2.global.tile [%0, {%1, %2, %3}];"
                    :: "l"(reinterpret_cast<unsigned long long>(m)), "r"(w0), "r"(0), "r"(o) : "memory");
@@ -838,7 +848,7 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
     else if constexpr (MODE == YFWD5) pf(&maps.a4p);
   };
   auto issueA = [&](int tile) {
-    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const int o = tile / ntw, w0 = (tile % ntw) * KW;
     const unsigned bar = smem_u32(&mbar[2]);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
@@ -874,7 +884,7 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
   const double h = st->h;
   const double h2 = 0.5 * h;
   const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
-  TileIdx<C> idx;
+  TileIdxK<KW> idx;
   BlockSync sync;
   double red = 0.0;
   int k = 0;
@@ -885,24 +895,32 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
       issue(tile + gridDim.x, b ^ 1);
       prefetch_ops(tile + gridDim.x);
     }
-    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const int o = tile / ntw, w0 = (tile % ntw) * KW;
     const long long base = (long long)o * Ny * Nt + w0;
     // operands of this thread's elements (e = tid + i*NTHR), in flight during the wait and FFT
     C opA[LATE ? 1 : E], opB[LATE ? 1 : E];
     auto load_ops = [&](int i, C& A_, C& B_) {
       const int e = tid + i * NTHR;
-      const long long gi = base + (long long)(e / kW) * Nt + (e % kW);
+      const long long gi = base + (long long)(e / KW) * Nt + (e % KW);
       if constexpr (MODE == YMID2 || MODE == YMID3) { A_ = __ldg(acur + gi); B_ = __ldg(tsum + gi); }
       else if constexpr (MODE == YMID4) B_ = __ldg(tsum + gi);
       else if constexpr (MODE == YMID1R) B_ = __ldg(k1b + gi);
       else if constexpr (MODE == YFWD5) A_ = __ldg(a4p + gi);
     };
-    const double qn = (tid < N && MODE != YMID4 && MODE != YFWD5) ? __ldg(a.tb.q + (long long)o * Ny + tid) : 0.0;
+    constexpr int QN = (N + NTHR - 1) / NTHR;   // k_perp^2 values of the row per thread
+    double qn[QN];
+#pragma unroll
+    for (int i = 0; i < QN; ++i) {
+      const int n = tid + i * NTHR;
+      qn[i] = (n < N && MODE != YMID4 && MODE != YFWD5) ? __ldg(a.tb.q + (long long)o * Ny + n) : 0.0;
+    }
     if constexpr (!LATE) {
 #pragma unroll
       for (int i = 0; i < E; ++i) load_ops(i, opA[i], opB[i]);
     }
-    if (tid < N) qrow[tid] = qn;   // read after the barrier below
+#pragma unroll
+    for (int i = 0; i < QN; ++i)
+      if (tid + i * NTHR < N) qrow[tid + i * NTHR] = qn[i];   // read after the barrier below
     bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
     if (TWO) ok = ok && mbar_wait(smem_u32(&mbar[2]), (unsigned)(k & 1));
     if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
@@ -918,13 +936,13 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
       return;
     }
     C* s = buf[b];
-    if constexpr (MODE != YMID1R) stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
-    if constexpr (TWO) stockham<N, kW, NTHR, -1, 1, C>(bufA, tw, tid, idx, sync);
-    const OmegaCol oc(a.tb, w0 + tid % kW);
+    if constexpr (MODE != YMID1R) stockham<N, KW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+    if constexpr (TWO) stockham<N, KW, NTHR, -1, 1, C>(bufA, tw, tid, idx, sync);
+    const OmegaCol oc(a.tb, w0 + tid % KW);
 #pragma unroll
     for (int i = 0; i < E; ++i) {
       const int e = tid + i * NTHR;
-      const int n = e / kW, w = e % kW;     // n = ky, o = kx; s[e] = s[idx(w, n)]
+      const int n = e / KW, w = e % KW;     // n = ky, o = kx; s[e] = s[idx(w, n)]
       const long long gi = base + (long long)n * Nt + w;
       C oA = C{0, 0}, oB = C{0, 0};
       if constexpr (LATE) load_ops(i, oA, oB);
@@ -979,8 +997,8 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
       __syncthreads();
       // bufA is free once every thread has read its elements: fetch the next tile's
       if (TWO && tid == 0 && tile + (int)gridDim.x < total) issueA(tile + gridDim.x);
-      stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
-      store_tile<C, N, NTHR>(s, out, base, Nt, tid);
+      stockham<N, KW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+      store_tile<C, N, NTHR, KW>(s, out, base, Nt, tid);
     }
     __syncthreads();   // buffer b is refilled at iteration k + 1
   }
@@ -990,10 +1008,157 @@ __global__ void __launch_bounds__(256, LATE ? 3 : 2) k_ypass_tma(SpaceArgs a, co
   }
 }
 
-template <int N>
+template <int N, int KW = kW>
 static size_t ytma_smem(int mode) {
-  return sizeof(float2) * (size_t)((mode == YMID1 ? 3 : 2) * N * kW + N) + 3 * sizeof(unsigned long long) +
+  return sizeof(float2) * (size_t)((mode == YMID1 ? 3 : 2) * N * KW + N) + 3 * sizeof(unsigned long long) +
          N * sizeof(double);
+}
+
+// ---------------------------------------------------------------------------
+// y passes of complex64 plans with Ny = 256 on the register four-step FFT of the
+// x passes.  Thread (w, j) of a tile (kW omega columns x 256 ky rows) holds rows
+// j + 16 i, i < 16, in registers from the load to the store: a 256-point
+// transform is a 16-point DFT in registers, a twiddle, one shared-memory
+// transpose and a second 16-point DFT, and bin X[j + 16 k] lands on the same
+// thread in register k, so the stage algebra runs on the registers and the
+// results go straight back to HBM (half a warp covers 16 consecutive omega =
+// one 128-byte row).  Per element that is two shared-memory round trips against
+// six for the tile passes of k_ypass_tma.  The DFTs, the twiddles and the order
+// they are applied in are those of k_ypass_tma's two radix-16 Stockham passes,
+// and the stage algebra is the same expression per element, so both kernels
+// give the same bits.  LATE = 0 issues the stage-operand loads with the tile's
+// (two CTAs per SM); LATE = 1 issues them element by element in the stage loop
+// (three CTAs per SM).  One instantiation per pass.
+// ---------------------------------------------------------------------------
+template <int MODE, int LATE>
+__global__ void __launch_bounds__(kW * 16, LATE ? 3 : 2)
+k_ypass_rq(SpaceArgs a) {
+  using C = float2;
+  using Rl = float;
+  constexpr int R = 16, N = R * R, NTHR = kW * R;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* T = tw + N;                                          // transpose buffer, N * kW
+  double* qrow = reinterpret_cast<double*>(T + N * kW);   // k_perp^2 of the tile's kx row
+  const int tid = threadIdx.x, w = tid % kW, j = tid / kW;
+  State3D* st = a.st;
+  if (st->done) return;
+  if (MODE == YMID1R && st->fresh) return;
+  if (MODE == YMID1 && !st->fresh) return;
+  const int Nt = a.g.Nt;
+  const int ntile = Nt / kW;
+  const int o = blockIdx.x / ntile;            // kx index
+  const int w0 = (blockIdx.x % ntile) * kW;    // omega offset
+  const long long base = (long long)o * N * Nt + w0 + w;
+  auto gidx = [&](int i) { return base + (long long)(j + R * i) * Nt; };
+  C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
+  C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
+  C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
+  C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
+  C* __restrict__ out = reinterpret_cast<C*>(a.out);
+  C* __restrict__ su = reinterpret_cast<C*>(a.save_u);
+  const C* __restrict__ in = reinterpret_cast<const C*>(MODE == YMID1R ? a.b.acur : a.in);
+  constexpr bool TWO = MODE == YMID1;          // YMID1 also transforms fft_x(Z) = tmp[2]
+  C v[R], v2[TWO ? R : 1];
+#pragma unroll
+  for (int i = 0; i < R; ++i) v[i] = __ldg(in + gidx(i));
+  if constexpr (TWO) {
+    const C* __restrict__ z2 = reinterpret_cast<const C*>(a.b.tmp[2]);
+#pragma unroll
+    for (int i = 0; i < R; ++i) v2[i] = __ldg(z2 + gidx(i));
+  }
+  C opA[LATE ? 1 : R], opB[LATE ? 1 : R];
+  auto load_ops = [&](int i, C& A_, C& B_) {
+    const long long gi = gidx(i);
+    if constexpr (MODE == YMID2 || MODE == YMID3) { A_ = __ldg(acur + gi); B_ = __ldg(tsum + gi); }
+    else if constexpr (MODE == YMID4) B_ = __ldg(tsum + gi);
+    else if constexpr (MODE == YMID1R) B_ = __ldg(k1b + gi);
+    else if constexpr (MODE == YFWD5) A_ = __ldg(a4p + gi);
+  };
+  if constexpr (!LATE) {
+#pragma unroll
+    for (int i = 0; i < R; ++i) load_ops(i, opA[i], opB[i]);
+  }
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twy);
+    for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
+    if (MODE != YMID4 && MODE != YFWD5)
+      for (int i = tid; i < N; i += NTHR) qrow[i] = __ldg(a.tb.q + (long long)o * N + i);
+  }
+  __syncthreads();
+  if constexpr (MODE != YMID1R) fft_sq<R, -1>(v, T, tw, j, w);
+  if constexpr (TWO) fft_sq<R, -1>(v2, T, tw, j, w);
+  const double h = st->h;
+  const double h2 = 0.5 * h;
+  const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
+  const OmegaCol oc(a.tb, w0 + w);
+  double red = 0.0;
+#pragma unroll
+  for (int i = 0; i < R; ++i) {
+    const int n = j + R * i;                   // ky row of register i
+    const long long gi = gidx(i);
+    C oA = C{0, 0}, oB = C{0, 0};
+    if constexpr (LATE) load_ops(i, oA, oB);
+    else { oA = opA[i]; oB = opB[i]; }
+    if constexpr (MODE == YFWD5) {
+      const C a5 = v[i], a4 = oA;
+      const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
+      const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+      red = (d > red || d != d) ? d : red;
+      continue;
+    }
+    if constexpr (MODE == YMID4) {
+      const C a4 = v[i];
+      const C A4 = cadd(oB, cscale(a4, h6R));
+      a4p[gi] = a4;
+      const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+      red = (m > red || m != m) ? m : red;
+      v[i] = A4;
+      continue;
+    }
+    const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qrow[n], h2);
+    C u;
+    if constexpr (MODE == YMID1R) {   // v = A, opB = k1
+      const C vv = cmul(v[i], Ef);
+      const C a1 = cmul(oB, Ef);
+      tsum[gi] = a1;
+      u = cadd(vv, cscale(a1, h2R));
+    } else if constexpr (MODE == YMID1) {   // v = k1 = N(A), v2 = A
+      const C A = v2[i], k1 = v[i];
+      acur[gi] = A;
+      k1b[gi] = k1;
+      const C vv = cmul(A, Ef);
+      const C a1 = cmul(k1, Ef);
+      tsum[gi] = a1;
+      u = cadd(vv, cscale(a1, h2R));
+    } else if constexpr (MODE == YMID2) {
+      const C a2 = v[i];
+      const C vv = cmul(oA, Ef);
+      tsum[gi] = cadd(oB, cscale(a2, (Rl)2));
+      u = cadd(vv, cscale(a2, h2R));
+    } else {   // YMID3
+      const C a3 = v[i];
+      const C vv = cmul(oA, Ef);
+      const C ts = cadd(oB, cscale(a3, (Rl)2));
+      tsum[gi] = cmul(cadd(vv, cscale(ts, h6R)), Ef);
+      u = cmul(cadd(vv, cscale(a3, hR)), Ef);
+    }
+    v[i] = u;
+    if (su) su[gi] = u;
+  }
+  if constexpr (MODE == YMID4 || MODE == YFWD5) {
+    red = warp_max<32>(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+  }
+  if constexpr (MODE != YFWD5) {
+    fft_sq<R, +1>(v, T, tw, j, w);
+#pragma unroll
+    for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
+  }
+}
+
+static constexpr size_t yrq_smem() {
+  return sizeof(float2) * (size_t)(256 + 256 * kW) + 256 * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -1492,15 +1657,17 @@ struct uppe3d_plan {
   double* diag_buf = nullptr;     // per-block partial sums + 3 results
   cudaStream_t cap_stream = nullptr;
   bool ytma = false;              // TMA-fed y passes possible (complex64, 64 <= Ny <= 256)
-  YMaps ymaps;
+  YMaps ymaps;                    // boxes of kW omega columns
+  YMaps ymaps8;                   // boxes of 8 omega columns
   int nsm = 148;
   // launch configuration picked per shape by the tuner (uppe3d_tuning): every
   // candidate computes the same bits, only the time differs
-  int y_tma = 1;                  // y passes on k_ypass_tma (1) or k_space (0)
-  int y_ctas = 2;                 // k_ypass_tma CTAs per SM (1, 2 or 3)
-  int y_late = 0;                 // k_ypass_tma loads the stage operands where used (1)
+  int y_tma = 1;                  // y passes on k_ypass_tma (1), k_ypass_rq (2) or k_space (0)
+  int y_ctas = 2;                 // k_ypass_tma CTAs per SM (1..6; k_ypass_rq: 2 or 3, fixed by LATE)
+  int y_late = 0;                 // the y kernel loads the stage operands where used (1)
+  int y_kw = kW;                  // k_ypass_tma omega columns per tile (16 or 8)
   int t_wpb = 8;                  // warps (t-lines) per block of k_tpass_w (4 or 8)
-  float tune_ms[8] = {0};         // measured per-attempt pass times of the candidates
+  float tune_ms[UPPE3D_TUNE_SLOTS] = {0};   // measured per-attempt pass times of the candidates
   int tuned = 0;                  // 1 timed here, 2 from the process cache, 0 defaults
 };
 
@@ -1559,51 +1726,85 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
   k_space<Rl, N><<<(unsigned)nblocks, SpaceCfg<N>::NTHR, smem, s>>>(a);
 }
 
-// the y passes of the attempt that k_ypass_tma serves (its `in` map is tmp[1])
+// the y passes of the attempt that k_ypass_tma and k_ypass_rq serve (input tmp[1])
+static bool fused_ypass(const uppe3d_plan* p, int mode, const void* in) {
+  return mode == YMID1R ||
+         ((mode == YMID1 || mode == YMID2 || mode == YMID3 || mode == YMID4 || mode == YFWD5) && in == p->b.tmp[1]);
+}
 static bool use_ytma(const uppe3d_plan* p, int mode, const void* in) {
-  return p->ytma && p->y_tma && (mode == YMID1R || ((mode == YMID1 || mode == YMID2 || mode == YMID3 || mode == YMID4 ||
-                                         mode == YFWD5) && in == p->b.tmp[1]));
+  return p->ytma && p->y_tma == 1 && fused_ypass(p, mode, in);
+}
+// k_ypass_rq: complex64, Ny = 256, and only where k_ypass_tma is available too
+// (the two give the same bits; the plain tile kernel does not)
+static bool yrq_ok(const uppe3d_plan* p) { return p->ytma && !p->dbl && p->g.Ny == 256; }
+static bool use_yrq(const uppe3d_plan* p, int mode, const void* in) {
+  return p->y_tma == 2 && yrq_ok(p) && fused_ypass(p, mode, in);
 }
 
-template <int N, int LATE>
+template <int LATE>
+static void launch_yrq_l(const SpaceArgs& a, unsigned nblocks, cudaStream_t s) {
+  constexpr unsigned T = kW * 16;
+  constexpr size_t sm = yrq_smem();
+  switch (a.mode) {
+    case YMID1: k_ypass_rq<YMID1, LATE><<<nblocks, T, sm, s>>>(a); break;
+    case YMID1R: k_ypass_rq<YMID1R, LATE><<<nblocks, T, sm, s>>>(a); break;
+    case YMID2: k_ypass_rq<YMID2, LATE><<<nblocks, T, sm, s>>>(a); break;
+    case YMID3: k_ypass_rq<YMID3, LATE><<<nblocks, T, sm, s>>>(a); break;
+    case YMID4: k_ypass_rq<YMID4, LATE><<<nblocks, T, sm, s>>>(a); break;
+    default: k_ypass_rq<YFWD5, LATE><<<nblocks, T, sm, s>>>(a); break;
+  }
+}
+
+template <int N, int LATE, int KW>
 static void launch_ytma_nl(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
   // persistent CTAs: never more per SM than the shared memory lets be resident
-  const int per_sm = ytma_smem<N>(a.mode) * p->y_ctas <= 220 * 1024 ? p->y_ctas : 2;
+  const size_t sm = ytma_smem<N, KW>(a.mode);
+  int per_sm = p->y_ctas;
+  while (per_sm > 1 && sm * per_sm > 220 * 1024) --per_sm;
   const dim3 g((unsigned)(per_sm * p->nsm));
-  const size_t sm = ytma_smem<N>(a.mode);
+  const YMaps& mp = KW == kW ? p->ymaps : p->ymaps8;
+  constexpr int T = YTmaCfg<KW, LATE>::NTHR;
   switch (a.mode) {
-    case YMID1: k_ypass_tma<N, YMID1, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID1R: k_ypass_tma<N, YMID1R, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID2: k_ypass_tma<N, YMID2, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID3: k_ypass_tma<N, YMID3, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    case YMID4: k_ypass_tma<N, YMID4, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
-    default: k_ypass_tma<N, YFWD5, LATE><<<g, 256, sm, s>>>(a, p->ymaps); break;
+    case YMID1: k_ypass_tma<N, YMID1, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
+    case YMID1R: k_ypass_tma<N, YMID1R, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
+    case YMID2: k_ypass_tma<N, YMID2, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
+    case YMID3: k_ypass_tma<N, YMID3, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
+    case YMID4: k_ypass_tma<N, YMID4, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
+    default: k_ypass_tma<N, YFWD5, LATE, KW><<<g, T, sm, s>>>(a, mp); break;
   }
 }
 
 template <int N>
 static void launch_ytma_n(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
-  if (p->y_late) launch_ytma_nl<N, 1>(p, a, s);
-  else launch_ytma_nl<N, 0>(p, a, s);
+  if (p->y_kw == 8) {
+    if (p->y_late) launch_ytma_nl<N, 1, 8>(p, a, s);
+    else launch_ytma_nl<N, 0, 8>(p, a, s);
+  } else {
+    if (p->y_late) launch_ytma_nl<N, 1, kW>(p, a, s);
+    else launch_ytma_nl<N, 0, kW>(p, a, s);
+  }
 }
 
-template <int N, int LATE>
+template <int N, int LATE, int KW>
 static cudaError_t set_ytma_attr_l() {
-  const int sm = (int)ytma_smem<N>(YMID2);
-  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                       (int)ytma_smem<N>(YMID1));
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YFWD5, LATE>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  const int sm = (int)ytma_smem<N, KW>(YMID2);
+  cudaError_t e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                       (int)ytma_smem<N, KW>(YMID1));
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID1R, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID2, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID3, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YMID4, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tma<N, YFWD5, LATE, KW>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
   return e;
 }
 
 template <int N>
 static cudaError_t set_ytma_attr() {
-  const cudaError_t e = set_ytma_attr_l<N, 0>();
-  return e == cudaSuccess ? set_ytma_attr_l<N, 1>() : e;
+  cudaError_t e = set_ytma_attr_l<N, 0, kW>();
+  if (e == cudaSuccess) e = set_ytma_attr_l<N, 1, kW>();
+  if (e == cudaSuccess) e = set_ytma_attr_l<N, 0, 8>();
+  if (e == cudaSuccess) e = set_ytma_attr_l<N, 1, 8>();
+  return e;
 }
 
 template <typename Rl>
@@ -1614,6 +1815,12 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   a.save_u = (mode == YMID1 || mode == YMID1R) ? p->save_u[0]
            : mode == YMID2 ? p->save_u[1] : mode == YMID3 ? p->save_u[2] : nullptr;
   a.scale = p->pass_scale;
+  if (sizeof(Rl) == 4 && use_yrq(p, mode, in)) {
+    const unsigned nb = (unsigned)((long long)p->g.Nx * (p->g.Nt / kW));
+    if (p->y_late) launch_yrq_l<1>(a, nb, s);
+    else launch_yrq_l<0>(a, nb, s);
+    return 0;
+  }
   if (sizeof(Rl) == 4 && use_ytma(p, mode, in)) {
     switch (p->g.Ny) {
       case 64: launch_ytma_n<64>(p, a, s); break;
@@ -1768,7 +1975,7 @@ struct Recorder {
   }
 };
 
-enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3, KIND_YT = 4 };
+enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3, KIND_YT = 4, KIND_YR = 5 };
 
 // the fixed pass sequence of one attempt (see the file header); the numbers are
 // the fields each launch reads + writes (algorithmic bytes / field bytes)
@@ -1778,7 +1985,8 @@ static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
   cudaStream_t s = r.s;
   void* const* t = p->b.tmp;
   const bool f = r.fresh != 0;
-  const int KY = p->ytma ? KIND_YT : KIND_Y;   // the y passes served by k_ypass_tma
+  // the fused y passes: k_ypass_rq, k_ypass_tma or the plain tile kernel
+  const int KY = (p->y_tma == 2 && yrq_ok(p)) ? KIND_YR : (p->ytma && p->y_tma == 1) ? KIND_YT : KIND_Y;
   // eval 1 (skipped on device unless the state is fresh)
   rc |= r(KIND_T, 2, f, [&] { return launch_t<Rl, 0>(p, T_FROM_Z, nullptr, t[0], s); });
   rc |= r(KIND_X, 4, f, [&] { return launch_space<Rl>(p, XFWD_Z, t[0], t[1], s); });
@@ -1822,17 +2030,19 @@ static int setup_ytma(uppe3d_plan* p) {
   EncodeTiledFn encode = reinterpret_cast<EncodeTiledFn>(fn);
   const cuuint64_t dims[3] = {(cuuint64_t)p->g.Nt, (cuuint64_t)p->g.Ny, (cuuint64_t)p->g.Nx};
   const cuuint64_t strides[2] = {(cuuint64_t)p->g.Nt * 8, (cuuint64_t)p->g.Ny * p->g.Nt * 8};
-  const cuuint32_t box[3] = {(cuuint32_t)kW, (cuuint32_t)p->g.Ny, 1};
   const cuuint32_t es[3] = {1, 1, 1};
   void* bufs[6] = {p->b.tmp[1], p->b.acur, p->b.tmp[2], p->b.tsum, p->b.k1, p->b.a4p};
-  CUtensorMap* maps[6] = {&p->ymaps.in, &p->ymaps.acur, &p->ymaps.z2, &p->ymaps.tsum, &p->ymaps.k1,
-                          &p->ymaps.a4p};
-  for (int i = 0; i < 6; ++i) {
-    if (reinterpret_cast<uintptr_t>(bufs[i]) % 16) return 0;
-    if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, bufs[i], dims, strides, box, es,
-               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
-               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
-      return 0;
+  for (int set = 0; set < 2; ++set) {       // boxes of kW and of 8 omega columns (64-byte rows)
+    YMaps& ym = set == 0 ? p->ymaps : p->ymaps8;
+    const cuuint32_t box[3] = {(cuuint32_t)(set == 0 ? kW : 8), (cuuint32_t)p->g.Ny, 1};
+    CUtensorMap* maps[6] = {&ym.in, &ym.acur, &ym.z2, &ym.tsum, &ym.k1, &ym.a4p};
+    for (int i = 0; i < 6; ++i) {
+      if (reinterpret_cast<uintptr_t>(bufs[i]) % 16) return 0;
+      if (encode(maps[i], CU_TENSOR_MAP_DATA_TYPE_UINT64, 3, bufs[i], dims, strides, box, es,
+                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+                 CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS)
+        return 0;
+    }
   }
   int dev = 0;
   UPPE_CK(cudaGetDevice(&dev));
@@ -1848,13 +2058,15 @@ static int setup_ytma(uppe3d_plan* p) {
 }
 
 // ---------------------------------------------------------------------------
-// Per-shape tuner.  Candidates: the y passes on k_ypass_tma (operands loaded early
-// with one or two CTAs per SM, or late with two or three), and k_tpass_w with
+// Per-shape tuner.  Candidates: the y passes on k_ypass_tma with tiles of 16 omega
+// columns (operands loaded early with one or two CTAs per SM, or late with two or
+// three) or of 8 columns (early with four, late with six), and k_tpass_w with
 // four or eight t-lines per block (same per-line code).  Every candidate computes
 // the same bits, so the choice changes only the time.  Each candidate runs whole
 // attempts launch by launch on zeroed fields with CUDA events around each launch;
 // the y and t choices are independent (different launches), so they are timed
-// separately.  Choices are kept per (Nx, Ny, Nt, precision, SM count) for the
+// separately.  The tile width changes which columns share a CTA, not the
+// arithmetic of a column.  Choices are kept per (Nx, Ny, Nt, precision, SM count) for the
 // life of the process; UPPE_TUNE=0 in the environment keeps the defaults.
 // ---------------------------------------------------------------------------
 struct TuneKey {
@@ -1863,7 +2075,7 @@ struct TuneKey {
     return std::tie(Nx, Ny, Nt, dbl, nsm) < std::tie(o.Nx, o.Ny, o.Nt, o.dbl, o.nsm);
   }
 };
-struct TuneVal { int y_tma, y_ctas, y_late, t_wpb; float ms[8]; };
+struct TuneVal { int y_tma, y_ctas, y_late, y_kw, t_wpb; float ms[UPPE3D_TUNE_SLOTS]; };
 static std::map<TuneKey, TuneVal> g_tune_cache;
 static std::mutex g_tune_mu;
 
@@ -1883,7 +2095,7 @@ static int time_attempts(uppe3d_plan* p, cudaStream_t s, int reps, float* y_ms, 
     for (size_t i = 0; i < rec.kind.size(); ++i) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, rec.ev[2 * i], rec.ev[2 * i + 1]);
-      if (rec.kind[i] == KIND_Y || rec.kind[i] == KIND_YT) *y_ms += ms;
+      if (rec.kind[i] == KIND_Y || rec.kind[i] == KIND_YT || rec.kind[i] == KIND_YR) *y_ms += ms;
       if (rec.kind[i] == KIND_T) *t_ms += ms;
     }
     for (auto e : rec.ev) cudaEventDestroy(e);
@@ -1905,6 +2117,7 @@ static int tune(uppe3d_plan* p) {
       p->y_tma = it->second.y_tma;
       p->y_ctas = it->second.y_ctas;
       p->y_late = it->second.y_late;
+      p->y_kw = it->second.y_kw;
       p->t_wpb = it->second.t_wpb;
       memcpy(p->tune_ms, it->second.ms, sizeof(p->tune_ms));
       p->tuned = 2;
@@ -1920,29 +2133,31 @@ static int tune(uppe3d_plan* p) {
   k_begin<<<1, 1, 0, s>>>(p->st, 1.0, 1e-5, 1e-2, 1e-9, 0);
   k_set_scale_one<<<1, 1, 0, s>>>(p->st);
   // the plain tile kernel rounds differently from the TMA-fed one, so it is a
-  // candidate only where the TMA path is unavailable
-  struct YC { int tma, ctas, late; } yc[4] = {{1, 2, 0}, {1, 1, 0}, {1, 3, 1}, {1, 2, 1}};
-  const int ny = p->ytma ? 4 : 1;
-  if (!p->ytma) yc[0] = YC{0, 2, 0};
+  // candidate only where the TMA path is unavailable; the register four-step
+  // kernel gives the TMA-fed kernel's bits and serves Ny = 256
+  struct YC { int tma, ctas, late, kw; } yc[8] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
+                                                {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW}};
+  const int ny = p->ytma ? (yrq_ok(p) ? 8 : 6) : 1;
+  if (!p->ytma) yc[0] = YC{0, 2, 0, kW};
   const int tw_n = (p->g.Nt == 512 || (p->g.Nt == 1024 && !p->dbl)) ? 2 : 1;
   const int tw[2] = {8, 4};
   float best_y = 1e30f, best_t = 1e30f;
   int by = 0, bt = 0;
   int rc = 0;
   float y_ms, t_ms;
-  p->y_tma = yc[0].tma; p->y_ctas = yc[0].ctas; p->y_late = yc[0].late; p->t_wpb = tw[0];
+  p->y_tma = yc[0].tma; p->y_ctas = yc[0].ctas; p->y_late = yc[0].late; p->y_kw = yc[0].kw; p->t_wpb = tw[0];
   rc = p->dbl ? time_attempts<double>(p, s, 1, &y_ms, &t_ms) : time_attempts<float>(p, s, 1, &y_ms, &t_ms);
   for (int i = 0; i < ny && !rc; ++i) {        // y candidates with the default t-pass
-    p->y_tma = yc[i].tma; p->y_ctas = yc[i].ctas; p->y_late = yc[i].late;
+    p->y_tma = yc[i].tma; p->y_ctas = yc[i].ctas; p->y_late = yc[i].late; p->y_kw = yc[i].kw;
     rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
     p->tune_ms[i] = y_ms;
     if (y_ms < best_y) { best_y = y_ms; by = i; }
   }
-  p->y_tma = yc[by].tma; p->y_ctas = yc[by].ctas; p->y_late = yc[by].late;
+  p->y_tma = yc[by].tma; p->y_ctas = yc[by].ctas; p->y_late = yc[by].late; p->y_kw = yc[by].kw;
   for (int i = 0; i < tw_n && !rc; ++i) {      // t candidates with the chosen y passes
     p->t_wpb = tw[i];
     rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
-    p->tune_ms[5 + i] = t_ms;
+    p->tune_ms[8 + i] = t_ms;
     if (t_ms < best_t) { best_t = t_ms; bt = i; }
   }
   p->t_wpb = tw[bt];
@@ -1950,7 +2165,7 @@ static int tune(uppe3d_plan* p) {
   if (rc) return rc;
   p->tuned = 1;
   std::lock_guard<std::mutex> lk(g_tune_mu);
-  TuneVal v{p->y_tma, p->y_ctas, p->y_late, p->t_wpb, {0}};
+  TuneVal v{p->y_tma, p->y_ctas, p->y_late, p->y_kw, p->t_wpb, {0}};
   memcpy(v.ms, p->tune_ms, sizeof(v.ms));
   g_tune_cache[key] = v;
   return 0;
@@ -2217,22 +2432,26 @@ extern "C" long long uppe3d_field_bytes(const uppe3d_plan* p) {
   return p ? (long long)(p->csz * p->g.npts) : 0;
 }
 
-extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg5, float* ms8) {
-  if (!p || !cfg5) return UPPE_ERR_ARG;
-  cfg5[0] = p->ytma && p->y_tma;
-  cfg5[1] = p->y_ctas;
-  cfg5[2] = p->y_late;
-  cfg5[3] = p->t_wpb;
-  cfg5[4] = p->tuned;
-  if (ms8) memcpy(ms8, p->tune_ms, sizeof(p->tune_ms));
+extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg6, float* ms) {
+  if (!p || !cfg6) return UPPE_ERR_ARG;
+  cfg6[0] = p->y_tma == 2 ? 2 : (p->ytma && p->y_tma) ? 1 : 0;
+  cfg6[1] = p->y_ctas;
+  cfg6[2] = p->y_late;
+  cfg6[3] = p->y_kw;
+  cfg6[4] = p->t_wpb;
+  cfg6[5] = p->tuned;
+  if (ms) memcpy(ms, p->tune_ms, sizeof(p->tune_ms));
   return 0;
 }
 
-extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_late, int t_wpb) {
-  if (!p || y_ctas < 1 || y_ctas > 3 || (t_wpb != 4 && t_wpb != 8)) return UPPE_ERR_ARG;
-  p->y_tma = y_tma ? 1 : 0;
-  p->y_ctas = y_ctas;
+extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb) {
+  if (!p || y_ctas < 1 || y_ctas > 6 || (y_kw != 8 && y_kw != kW) || (t_wpb != 4 && t_wpb != 8) ||
+      y_tma < 0 || y_tma > 2 || (y_tma == 2 && (!yrq_ok(p) || y_kw != kW)))
+    return UPPE_ERR_ARG;
+  p->y_tma = y_tma;
   p->y_late = y_late ? 1 : 0;
+  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_ctas;   // k_ypass_rq: fixed by its launch bounds
+  p->y_kw = y_kw;
   p->t_wpb = t_wpb;
   if (p->g_attempt) { cudaGraphExecDestroy(p->g_attempt); p->g_attempt = nullptr; }
   if (p->g_step) { cudaGraphExecDestroy(p->g_step); p->g_step = nullptr; }
@@ -2993,6 +3212,7 @@ extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nstep
 namespace uppe {
 struct RfConst {
   double I_coef, aval, chi3e, chi5e;           // I = I_coef E^2; W_ava = aval I; P = chi3e E^3 + chi5e E^5
+  double fR;                                   // Raman fraction (0: none)
   double rr, dt, rho_nt, Ui, e2m, nu, exp_nu, step_J;   // density / Drude constants (float32-rounded inputs)
   double E_scale;
 };
@@ -3005,6 +3225,8 @@ struct RfTables {
   const double* kp2;     // k_perp^2 [Nx*Ny]
   const double* damp;    // [Nx*Ny]
   Lut lut;
+  const void* ramH;      // Raman: H_k, k = 0..Nt, of the 2 Nt-point response (solver precision)
+  const void* ramW;      // Raman: exp(-i pi k / Nt), k = 0..Nt/2
 };
 
 enum RfLine { RF_FROM_T = 0, RF_NL = 1, RF_OUT = 2 };
@@ -3021,29 +3243,100 @@ __device__ __forceinline__ void rf_rho_step(double& rho, double wp, const RfCons
 }
 
 // launch shape of k_rf_line: per warp a line buffer (PAD complex) and the real
-// samples (NT), up to 8 warps while two blocks fit an SM
-template <int NT, typename Rl> struct RfLaunch {
+// samples (NT; with the Raman response another NT for E_eff^2), up to 8 warps
+// while two blocks fit an SM
+template <int NT, typename Rl, bool RAMAN = false> struct RfLaunch {
   using C = typename CT<Rl>::T;
-  static constexpr size_t per_warp = (size_t)TCfg<NT>::PAD * sizeof(C) + NT * sizeof(Rl);
+  static constexpr size_t per_warp = (size_t)TCfg<NT>::PAD * sizeof(C) + (RAMAN ? 2 : 1) * NT * sizeof(Rl);
   static constexpr size_t fixed = NT * sizeof(C);
   static constexpr int WPB = (fixed + 8 * per_warp <= 113 * 1024) ? 8 : (fixed + 4 * per_warp <= 113 * 1024) ? 4
                            : (fixed + 2 * per_warp <= 200 * 1024) ? 2 : 1;
   static size_t smem() { return fixed + WPB * per_warp; }
 };
 
-// one t-line per warp; S: line buffer (PAD complex), R: real samples (NT)
-template <typename Rl, int NT, int WPB>
+// The Raman term (media_physics.py:376-390): r = real(ifft(fft(x) H))[:NT] with x
+// = E^2 zero-padded to M = 2 NT samples, i.e. the circular convolution of length
+// M.  x is real, so one NT-point complex transform of z[m] = x[2m] + i x[2m+1]
+// gives its spectrum (z = 0 for m >= NT/2): with W_k = exp(-i pi k / NT),
+//   X_k = (Z_k + conj Z_(NT-k))/2 - (i/2) W_k (Z_k - conj Z_(NT-k)),  k = 0..NT,
+// Y_k = X_k H_k is Hermitian, and the inverse packs back the same way:
+//   Z'_k = (Y_k + conj Y_(NT-k)) + i conj(W_k) (Y_k - conj Y_(NT-k)),  k < NT,
+// whose unnormalised inverse NT-point transform is M (r[2m] + i r[2m+1]).  Each
+// lane handles the bin pairs (k, NT - k) it owns, so the update is in place.
+template <typename Rl, int NT>
+__device__ __forceinline__ void rf_raman(typename CT<Rl>::T* S, const Rl* R, Rl* Q, const typename CT<Rl>::T* tw,
+                                         const RfTables& tb, const RfConst& rc, int lane) {
+  using C = typename CT<Rl>::T;
+  for (int m = lane; m < NT; m += 32) {
+    C z = C{(Rl)0, (Rl)0};
+    if (m < NT / 2) {
+      const Rl e0 = R[2 * m], e1 = R[2 * m + 1];
+      z = C{e0 * e0, e1 * e1};
+    }
+    S[tpad(m)] = z;
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());
+  const C* H = reinterpret_cast<const C*>(tb.ramH);
+  const C* Wt = reinterpret_cast<const C*>(tb.ramW);
+  const Rl half = (Rl)0.5;
+  auto spec = [&](C Zk, C Zn, C w) {          // X_k from Z_k, Z_(NT-k), W_k
+    const C ev = C{(Zk.x + Zn.x) * half, (Zk.y - Zn.y) * half};
+    const C od = C{(Zk.y + Zn.y) * half, -(Zk.x - Zn.x) * half};   // (Z_k - conj Z_n) / (2i)
+    return cadd(ev, cmul(w, od));
+  };
+  auto pack = [&](C Yk, C Yn, C w) {          // Z'_k from Y_k, Y_(NT-k), W_k
+    const C s = C{Yk.x + Yn.x, Yk.y - Yn.y};
+    const C d = C{Yk.x - Yn.x, Yk.y + Yn.y};
+    const C wd = cmul(C{w.x, -w.y}, d);
+    return C{s.x - wd.y, s.y + wd.x};
+  };
+  for (int k = lane; k <= NT / 2; k += 32) {
+    if (k == 0) {
+      const C Z0 = S[tpad(0)];
+      const C Y0 = cscale(H[0], Z0.x + Z0.y);          // X_0 = Re Z_0 + Im Z_0
+      const C YN = cscale(H[NT], Z0.x - Z0.y);         // X_NT = Re Z_0 - Im Z_0
+      S[tpad(0)] = pack(Y0, YN, C{(Rl)1, (Rl)0});
+      continue;
+    }
+    const int n = NT - k;
+    const C Zk = S[tpad(k)], Zn = S[tpad(n)];
+    const C wk = Wt[k];
+    const C wn = C{-wk.x, wk.y};                       // W_(NT-k) = -conj(W_k)
+    const C Yk = cmul(spec(Zk, Zn, wk), H[k]);
+    const C Yn = cmul(spec(Zn, Zk, wn), H[n]);
+    S[tpad(k)] = pack(Yk, Yn, wk);
+    if (n != k) S[tpad(n)] = pack(Yn, Yk, wn);
+  }
+  __syncwarp();
+  stockham<NT, 1, TCfg<NT>::FT, +1, 1, C>(S, tw, lane, LineIdx(), WarpSync());
+  const Rl invM = (Rl)(1.0 / (2.0 * NT));
+  const Rl a = (Rl)(1.0 - rc.fR), b = (Rl)rc.fR;
+  for (int t = lane; t < NT; t += 32) {
+    const C zr = S[tpad(t >> 1)];
+    const Rl r = ((t & 1) ? zr.y : zr.x) * invM;
+    const Rl E = R[t];
+    Q[t] = a * (E * E) + b * r;
+  }
+  __syncwarp();
+}
+
+// one t-line per warp; S: line buffer (PAD complex), R: real samples (NT); with
+// RAMAN, Q: E_eff^2 (NT)
+template <typename Rl, int NT, int WPB, bool RAMAN>
 __global__ void __launch_bounds__(WPB * 32, (WPB * 32 * 2 <= 1024) ? 2 : 1)
 k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, void* out, const void* twt,
           double in_scale, double h) {
   using C = typename CT<Rl>::T;
+  using LS = RfLaunch<NT, Rl, RAMAN>;
   constexpr int PAD = TCfg<NT>::PAD;
   constexpr int NR = NT / 2 + 1;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  C* S = reinterpret_cast<C*>(smem_raw + RfLaunch<NT, Rl>::fixed + warp * RfLaunch<NT, Rl>::per_warp);
+  C* S = reinterpret_cast<C*>(smem_raw + LS::fixed + warp * LS::per_warp);
   Rl* R = reinterpret_cast<Rl*>(S + PAD);
+  Rl* Q = R + NT;
   for (int i = threadIdx.x; i < NT; i += WPB * 32) tw[i] = reinterpret_cast<const C*>(twt)[i];
   __syncthreads();
   const long long line = (long long)blockIdx.x * WPB + warp;
@@ -3082,6 +3375,7 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
   const Rl Es = (Rl)rc.E_scale;
   for (int t = lane; t < NT; t += 32) R[t] = (S[tpad(t)].x * invN) * Es;   // physical field
   __syncwarp();
+  if constexpr (RAMAN) rf_raman<Rl, NT>(S, R, Q, tw, tb, rc, lane);   // E_eff^2 into Q; S free again
   // density and Drude current (media_physics.py:11-118).  Without avalanche and
   // while no clamp binds the density update is affine in rho, and the free
   // current J' = J exp(-nu dt) + (e^2/m) rho E step_J always is: chunks of E
@@ -3192,7 +3486,9 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
   const Rl c3 = (Rl)rc.chi3e, c5 = (Rl)rc.chi5e;
   for (int t = lane; t < NT; t += 32) {
     const Rl E = R[t];
-    Rl P = ((c3 * E) * E) * E;
+    Rl P;
+    if constexpr (RAMAN) P = (c3 * E) * Q[t];       // chi3_coef * E_t * E_eff_sq (:303-305)
+    else P = ((c3 * E) * E) * E;
     if (rc.chi5e != 0.0) {
       const Rl E2 = E * E;
       P = P + ((c5 * E) * E2) * E2;
@@ -3349,6 +3645,7 @@ struct uppe_rf_plan {
   std::vector<void*> allocs;
   int cur = 0;
   double h_last = 0.0;
+  bool raman = false;
 };
 
 static int rf_alloc(uppe_rf_plan* p, void** dst, size_t bytes, const void* src = nullptr) {
@@ -3479,6 +3776,27 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
   c.exp_nu = exp(-ndt);
   c.step_J = (fabs(ndt) < 1e-5) ? c.dt * (1.0 - 0.5 * ndt) : (1.0 - c.exp_nu) / c.nu;
   c.E_scale = 1.0;
+  c.fR = 0.0;
+  p->tb.ramH = p->tb.ramW = nullptr;
+  if (d->raman_H) {
+    // H_k as given; W_k = exp(-i pi k / Nt) in extended precision, rounded once
+    const int Nt = d->Nt;
+    std::vector<unsigned char> hb((Nt + 1) * p->csz), wb((Nt / 2 + 1) * p->csz);
+    for (int k = 0; k <= Nt; ++k) {
+      if (p->dbl) { ((double*)hb.data())[2 * k] = d->raman_H[2 * k]; ((double*)hb.data())[2 * k + 1] = d->raman_H[2 * k + 1]; }
+      else { ((float*)hb.data())[2 * k] = (float)d->raman_H[2 * k]; ((float*)hb.data())[2 * k + 1] = (float)d->raman_H[2 * k + 1]; }
+    }
+    for (int k = 0; k <= Nt / 2; ++k) {
+      const long double ang = -3.141592653589793238462643383279502884L * (long double)k / (long double)Nt;
+      const double cr = (double)cosl(ang), ci = (double)sinl(ang);
+      if (p->dbl) { ((double*)wb.data())[2 * k] = cr; ((double*)wb.data())[2 * k + 1] = ci; }
+      else { ((float*)wb.data())[2 * k] = (float)cr; ((float*)wb.data())[2 * k + 1] = (float)ci; }
+    }
+    RF_TRY(rf_alloc(p, &ptr, hb.size(), hb.data())); p->tb.ramH = ptr;
+    RF_TRY(rf_alloc(p, &ptr, wb.size(), wb.data())); p->tb.ramW = ptr;
+    c.fR = d->raman_fR;
+    p->raman = true;
+  }
   void** spec[8] = {&p->b.ekw, &p->b.v, &p->b.a1, &p->b.u, &p->b.ts, &p->b.el, &p->b.na, &p->b.e4};
   for (int i = 0; i < 8; ++i) RF_TRY(rf_alloc(p, spec[i], p->csz * p->nspec));
   RF_TRY(rf_alloc(p, &p->tmp[0], p->csz * p->nspec));
@@ -3492,18 +3810,26 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
   return 0;
 }
 
-template <typename Rl, int NT>
-static int rf_line_n(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
-  constexpr int WPB = RfLaunch<NT, Rl>::WPB;
-  const size_t smem = RfLaunch<NT, Rl>::smem();
-  UPPE_CK(cudaFuncSetAttribute(k_rf_line<Rl, NT, WPB>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+template <typename Rl, int NT, bool RAMAN>
+static int rf_line_nr(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
+  using LS = RfLaunch<NT, Rl, RAMAN>;
+  constexpr int WPB = LS::WPB;
+  const size_t smem = LS::smem();
+  UPPE_CK(cudaFuncSetAttribute(k_rf_line<Rl, NT, WPB, RAMAN>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   Geom g;
   g.Nx = p->d.Nx; g.Ny = p->d.Ny; g.Nt = p->d.Nt; g.npts = p->nreal;
   const long long nl = (long long)g.Nx * g.Ny;
-  k_rf_line<Rl, NT, WPB><<<(unsigned)((nl + WPB - 1) / WPB), WPB * 32, smem, s>>>(mode, p->tb, p->rc, g, p->Nw, in, out,
-                                                                                  p->twt, in_scale, h);
+  k_rf_line<Rl, NT, WPB, RAMAN><<<(unsigned)((nl + WPB - 1) / WPB), WPB * 32, smem, s>>>(
+      mode, p->tb, p->rc, g, p->Nw, in, out, p->twt, in_scale, h);
   UPPE_CK(cudaGetLastError());
   return 0;
+}
+
+template <typename Rl, int NT>
+static int rf_line_n(uppe_rf_plan* p, int mode, const void* in, void* out, double in_scale, double h, cudaStream_t s) {
+  // only the nonlinear response uses the Raman term
+  if (p->raman && mode == RF_NL) return rf_line_nr<Rl, NT, true>(p, mode, in, out, in_scale, h, s);
+  return rf_line_nr<Rl, NT, false>(p, mode, in, out, in_scale, h, s);
 }
 
 template <typename Rl>

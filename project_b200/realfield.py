@@ -126,16 +126,32 @@ class Air(RealFieldMedium):
 
 
 class FusedSilica(RealFieldMedium):
-    """:321-360: Sellmeier index (clipped to 0.2-6 um), avalanche on.  The Raman
-    convolution of the reference (use_raman=True) is not built here."""
+    """:321-390: Sellmeier index (clipped to 0.2-6 um), avalanche on, and with
+    use_raman the delayed response f_R = 0.18, tau1 = 12.2 fs, tau2 = 32 fs: the
+    solver convolves E^2 with it on the device (k_rf_line)."""
 
     def __init__(self, center_wavelength, use_raman=False):
-        if use_raman:
-            raise NotImplementedError('the Raman response of the real-field medium is not built')
         super().__init__(center_wavelength, n0=1.45, n2=3.0e-20, Ui_eV=9.0, rho_nt=2.1e28, tau_rec=150e-15,
                          tau_c=3.0e-15, avalanche=True)
         self.B = (0.6961663, 0.4079426, 0.8974794)
         self.C = (0.0684043 ** 2, 0.1162414 ** 2, 9.896161 ** 2)
+        self.use_raman = bool(use_raman)
+        self.f_R, self.tau1, self.tau2 = 0.18, 12.2e-15, 32.0e-15
+
+    def raman_response(self, Nt, dt, float_dtype):
+        """init_raman (:362-374): h(t) = (t1^2 + t2^2)/(t1 t2^2) exp(-t/t2) sin(t/t1)
+        on 2 Nt samples of the solver precision with h(0) = 0, H = fft(h) dt / |H(0)|;
+        returns H_k for k = 0..Nt (the rest is the conjugate mirror)."""
+        t = np.arange(2 * Nt, dtype=float_dtype) * dt
+        a = (self.tau1 ** 2 + self.tau2 ** 2) / (self.tau1 * self.tau2 ** 2)
+        h = a * np.exp(-t / self.tau2) * np.sin(t / self.tau1)
+        h[0] = 0.0
+        H = np.fft.fft(h) * dt
+        norm = float(np.abs(H[0]))
+        if norm > 1e-20:
+            H = H / norm
+        cd = np.complex64 if float_dtype == np.float32 else np.complex128
+        return H.astype(cd)[:Nt + 1]
 
     def refractive_index(self, w):
         w = np.asarray(w, dtype=np.float64)
@@ -210,6 +226,10 @@ class ERK43_RealField_UPPE_3D:
         d.chi3e, d.chi5e = EPS0 * m.chi3, EPS0 * m.chi5
         d.rate_rec, d.rho_nt, d.Ui = 1.0 / m.tau_rec, m.rho_nt, m.Ui
         d.e_charge, d.m_e, d.tau_c = E_CH, M_E, m.tau_c
+        if getattr(m, 'use_raman', False):
+            H = m.raman_response(self.Nt, self.dt, fd).astype(np.complex128)
+            self._keep['ramH'] = np.ascontiguousarray(H.view(np.float64))
+            d.raman_H, d.raman_fR = P('ramH'), m.f_R
         plan = ctypes.c_void_p()
         with torch.cuda.device(self.device):
             _lib.check(self._lib.uppe_rf_plan_create(ctypes.byref(d), ctypes.byref(plan)), 'uppe_rf_plan_create')

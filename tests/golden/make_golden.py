@@ -404,6 +404,7 @@ def make_realfield():
     # in float32 and the step size collapses
     cases = [('argon', lambda: med.Argon(lam, 1.0, 'single'), 4e10, 3e-4, 1e-3),
              ('silica', lambda: med.FusedSilica(lam, 'single'), 8e9, 2e-5, 1e-3),
+             ('silica_raman', lambda: med.FusedSilica(lam, 'single', use_raman=True), 8e9, 2e-5, 1e-3),
              ('xenon', lambda: med.Xenon(lam, 2.0, 'single'), 2e10, 2e-4, 1e-3)]
     for name, mk, Ep, L, tol in cases:
         m = mk()

@@ -151,6 +151,39 @@ def test_long_lines_vs_oracle(Nt, precision, W0):
     assert rel_l2(sol.spectrum().cpu().numpy(), Ao) < tol
 
 
+@pytest.mark.parametrize('Nt,precision', [(512, 'single'), (1024, 'single'), (1024, 'double')])
+def test_kerr_dominated_steps_vs_oracle(Nt, precision):
+    """Steps whose change is mostly the Kerr term (1.8e16 W/m^2, 1.5 bar, w0 1 mm,
+    h up to 2 mm): the nonlinear evaluation itself, including the 32-point register
+    DFTs of the 1024-sample complex64 t-lines, must keep the per-step rounding
+    level (complex64: rel-L2 ~3e-7 per step, a wrong transform shows as ~2e-5)."""
+    from oracle import uppe3d
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x = np.linspace(-2e-3, 2e-3, 32)
+    t = np.linspace(-125e-15 * Nt / 512, 125e-15 * Nt / 512, Nt)
+    lam = 800e-9
+    om = uppe3d.argon(lam, 1.5, 'double', True)
+    W = np.zeros_like(om.log10_I_cpu)
+    om.W_gpu = W
+    osol = uppe3d.Solver3D(x, x, t, om, 'double')
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    T0 = 50e-15 / (2 * np.sqrt(np.log(2)))
+    A0 = (np.sqrt(1.8e16) * np.exp(-(X ** 2 + Y ** 2) / 1e-6)[:, :, None]
+          * np.exp(-(t / T0) ** 2 / 2)[None, None, :]).astype(np.complex128)
+    osol.A_scale = float(np.max(np.abs(A0)))
+    An = A0 / osol.A_scale
+    sol = ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(lam, 1.5, precision, True, lut=(om.log10_I_cpu, W)),
+                                    precision=precision)
+    sol.set_field(A0)
+    for k, h in enumerate([2.5e-4, 5e-4, 1e-3, 2e-3]):
+        An, err_o, _, _ = osol.erk43_step(An, h)
+        sol.attempt(h)
+        sol.commit(True)
+        rel = rel_l2(sol.field().cpu().numpy() / osol.A_scale, An)
+        assert rel < (1e-13 if precision == 'double' else 5e-7 * (k + 1)), (k, rel)
+
+
 def test_diagnostics_vs_oracle():
     """Energy, photon number and peak ionisation fraction of a propagation with
     significant ionisation (MPI-like table), complex128, against the oracle."""

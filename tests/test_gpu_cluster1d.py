@@ -128,3 +128,28 @@ def test_cluster_logged_steps_replay_to_the_same_field():
     _lib.check(lib.uppe1d_propagate_schedule(bp._plan, ctypes.c_void_p(rep.data_ptr()),
                                              ctypes.c_void_p(sched.data_ptr()), n, r2, _lib.stream_ptr()), 'sched')
     assert torch.equal(rep, work)
+
+
+@pytest.mark.parametrize('cluster', ['1', '0'])
+def test_activity_record_of_the_persistent_launch(monkeypatch, cluster):
+    """uppe1d_last_activity: every persistent CTA records its start and exit, so the
+    SM-busy fraction lies in (0, 1] and the span covers the launch."""
+    import ctypes
+    from project_b200 import _lib
+    from project_b200.solver1d import BatchedPropagator
+    monkeypatch.setenv('UPPE_1D_CLUSTER', cluster)
+    s = _argon()
+    insts, fields = [], []
+    for Nt in (8192, 4096, 2048, 2048):
+        t = np.linspace(-1e-12, 1e-12, Nt)
+        insts.append(s.instance(t, 0.02, tol=1e-6))
+        fields.append(_pulse(t))
+    bp = BatchedPropagator(insts, precision='single')
+    assert bool(bp._lib.uppe1d_uses_clusters(bp._plan)) == (cluster == '1')
+    bp.run(fields)
+    busy, span = ctypes.c_double(), ctypes.c_double()
+    _lib.check(bp._lib.uppe1d_last_activity(bp._plan, ctypes.byref(busy), ctypes.byref(span), _lib.stream_ptr()),
+               'uppe1d_last_activity')
+    assert 0.0 < busy.value <= 1.0 and span.value > 0.0
+    # four instances on a 148-SM GPU: at most 16 of the SMs can be busy
+    assert busy.value <= 16 / 148 + 1e-9

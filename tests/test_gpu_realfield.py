@@ -10,10 +10,11 @@ pytestmark = pytest.mark.gpu
 def _media(name):
     from project_b200 import realfield as rf
     return {'argon': lambda: rf.Argon(800e-9, 1.0), 'silica': lambda: rf.FusedSilica(800e-9),
-            'xenon': lambda: rf.Xenon(800e-9, 2.0)}[name]()
+            'xenon': lambda: rf.Xenon(800e-9, 2.0),
+            'silica_raman': lambda: rf.FusedSilica(800e-9, use_raman=True)}[name]()
 
 
-@pytest.mark.parametrize('name', ['argon', 'silica', 'xenon'])
+@pytest.mark.parametrize('name', ['argon', 'silica', 'xenon', 'silica_raman'])
 def test_realfield_step_and_replay_match_reference(name):
     """One step from the input (fixed h) and the reference's own attempt sequence
     replayed: errors and the final spectrum (single precision, the reference's)."""
@@ -37,7 +38,7 @@ def test_realfield_step_and_replay_match_reference(name):
     assert rel_l2(Ew, g['Ew']) < 1e-4
 
 
-@pytest.mark.parametrize('name', ['argon', 'silica'])
+@pytest.mark.parametrize('name', ['argon', 'silica', 'silica_raman'])
 def test_realfield_free_running_and_double_vs_oracle(name):
     """Free-running propagate (single) against the reference, and complex128 plans
     against the FP64 oracle attempt by attempt."""
@@ -51,7 +52,8 @@ def test_realfield_free_running_and_double_vs_oracle(name):
     assert rel_l2(Ew, g['Ew']) < 1e-4
     # the gases' n4 (chi5) underflows to zero in float32 but is active in FP64, where
     # the reference's values make the field diverge: off for the FP64 comparison
-    om = {'argon': lambda: orf.argon(800e-9, 1.0, 'double'), 'silica': lambda: orf.fused_silica(800e-9, 'double')}[name]()
+    om = {'argon': lambda: orf.argon(800e-9, 1.0, 'double'), 'silica': lambda: orf.fused_silica(800e-9, 'double'),
+          'silica_raman': lambda: orf.fused_silica(800e-9, 'double', use_raman=True)}[name]()
     om.chi5 = 0.0
     osol = orf.Solver(g['x'], g['x'], g['t'], om, 'double')
     E0 = g['E0'].astype(np.float64)

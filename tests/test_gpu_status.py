@@ -129,7 +129,7 @@ def test_1d_attempt_budget_and_forced_steps_in_one_batch():
     Each gets its own status; the normal one matches its solo run."""
     from project_b200.solver1d import BatchedPropagator
     s = _argon1d('double')
-    sk = _argon1d('double', n2=1e-20)          # ~8 rad of Kerr phase per millimetre
+    sk = _argon1d('double', n2=1e-21)          # ~0.8 rad of Kerr phase per millimetre
     t, A0 = _pulse1d()
     insts = [s.instance(t, 0.05, tol=1e-6),
              s.instance(t, 0.05, tol=1e-6, max_attempts=3),

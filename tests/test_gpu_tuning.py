@@ -1,8 +1,9 @@
 """Per-shape launch tuner of the 3+1D plan (GPU).
 
 uppe3d_plan_create times the candidate launch configurations of the y passes
-(TMA-fed kernel with early or late operand loads and one to three CTAs per SM) and of the
-warp t-line kernel (four or eight lines per block) and keeps the fastest.  The
+(TMA-fed kernel with tiles of 16 or 8 omega columns, early or late operand loads
+and one to six CTAs per SM; for Ny = 256 also the register four-step kernel) and
+of the warp t-line kernel (four or eight lines per block) and keeps the fastest.  The
 candidates are chosen so that they compute the same bits: these tests force each
 one and compare the propagated fields bit for bit (the plain tile kernel, which
 rounds differently, is used only where the TMA path is unavailable).
@@ -31,30 +32,38 @@ def _setup(precision='single', n=64, nt=512):
 
 def _tuning(sol):
     from project_b200 import _lib
-    cfg = (ctypes.c_int * 5)()
-    ms = (ctypes.c_float * 8)()
+    cfg = (ctypes.c_int * 6)()
+    ms = (ctypes.c_float * _lib.UPPE3D_TUNE_SLOTS)()
     _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
     return list(cfg), list(ms)
 
 
-def test_tuner_runs_and_every_candidate_gives_identical_fields():
+YCANDS = [(1, 2, 0, 16), (1, 1, 0, 16), (1, 3, 1, 16), (1, 2, 1, 16), (1, 4, 0, 8), (1, 6, 1, 8)]
+YCANDS_256 = YCANDS + [(2, 2, 0, 16), (2, 3, 1, 16)]     # + the register four-step kernel
+
+
+@pytest.mark.parametrize('n,nt', [(64, 512), (256, 128)])
+def test_tuner_runs_and_every_candidate_gives_identical_fields(n, nt):
     import torch
     from project_b200 import _lib
     from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
-    x, t, med, A0 = _setup()
+    x, t, med, A0 = _setup(n=n, nt=nt)
     sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='single')
     cfg, ms = _tuning(sol)
-    assert cfg[4] in (1, 2)                       # timed here or taken from the process cache
-    assert cfg[1] in (1, 2, 3) and cfg[3] in (4, 8)
-    if cfg[4] == 1:
-        assert all(v > 0 for v in ms[:4]) and ms[5] > 0 and ms[6] > 0
+    assert cfg[5] in (1, 2)                       # timed here or taken from the process cache
+    assert cfg[0] in (1, 2) and 1 <= cfg[1] <= 6 and cfg[3] in (8, 16) and cfg[4] in (4, 8)
+    ycands = YCANDS_256 if n == 256 else YCANDS
+    if cfg[5] == 1:
+        assert all(v > 0 for v in ms[:len(ycands)]) and ms[8] > 0
+    if n != 256:
+        assert cfg[0] == 1 and ms[6] == 0 and ms[7] == 0
+        assert sol._lib.uppe3d_set_tuning(sol._plan, 2, 2, 0, 16, 8) == -1   # Ny = 256 only
     ref = None
-    ycands = [(1, 2, 0), (1, 1, 0), (1, 3, 1), (1, 2, 1)]
-    for y_tma, y_ctas, y_late in ycands:
-        for wpb in (4, 8):
-            _lib.check(sol._lib.uppe3d_set_tuning(sol._plan, y_tma, y_ctas, y_late, wpb),
+    for y_tma, y_ctas, y_late, y_kw in ycands:
+        for wpb in ((4, 8) if nt == 512 else (8,)):
+            _lib.check(sol._lib.uppe3d_set_tuning(sol._plan, y_tma, y_ctas, y_late, y_kw, wpb),
                        'uppe3d_set_tuning')
-            assert _tuning(sol)[0][:4] == [y_tma, y_ctas, y_late, wpb]
+            assert _tuning(sol)[0][:5] == [y_tma, y_ctas, y_late, y_kw, wpb]
             z, _, A = sol.propagate(A0.astype(np.complex64), 0.02, tol=1e-4, return_gpu=True)
             assert sol.last_result.status == 0
             if ref is None:
@@ -62,7 +71,7 @@ def test_tuner_runs_and_every_candidate_gives_identical_fields():
                 assert ref[3] > 0                    # the plasma path ran
             else:
                 assert z == ref[0] and sol.last_result.attempts == ref[1]
-                assert torch.equal(A, ref[2]), (y_tma, y_ctas, y_late, wpb)
+                assert torch.equal(A, ref[2]), (y_tma, y_ctas, y_late, y_kw, wpb)
 
 
 def test_tuner_can_be_switched_off(monkeypatch):
@@ -71,5 +80,5 @@ def test_tuner_can_be_switched_off(monkeypatch):
     monkeypatch.setenv('UPPE_TUNE', '0')
     sol = ERK43IP_UPPE_3D_Optimized(x, x, t, med, precision='single')
     cfg, ms = _tuning(sol)
-    assert cfg[4] == 0 and cfg[3] == 8
+    assert cfg[5] == 0 and cfg[4] == 8
     assert all(v == 0 for v in ms)

@@ -100,6 +100,18 @@ def test_partition_instances_is_balanced_cover():
     assert max(loads) / (sum(loads) / 8) < 1.05
 
 
+def test_instance_cost_grows_with_energy_and_pressure():
+    """The sweep's cost model: per-attempt cost Nt log2 Nt times attempts that grow
+    with pulse energy and pressure (the nonlinear phase sets the step size)."""
+    from project_b200.distributed import instance_cost
+    base = instance_cost(4096, 1.0, energy=100e-6, pressure=1.0)
+    assert instance_cost(4096, 1.0, energy=400e-6, pressure=1.0) > base
+    assert instance_cost(4096, 1.0, energy=100e-6, pressure=2.5) > base
+    assert instance_cost(8192, 1.0, energy=100e-6, pressure=1.0) > 2 * base
+    assert instance_cost(4096, 2.0, energy=100e-6, pressure=1.0) == 2 * base
+    assert instance_cost(4096, 1.0) == instance_cost(4096, 1.0, energy=None, pressure=None)
+
+
 def _worker(rank, world, port, q):
     import torch.distributed as dist
     from project_b200.distributed import gather_results, partition_instances

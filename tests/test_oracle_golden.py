@@ -131,16 +131,20 @@ def test_pulse_from_spectrum_oracle_matches_reference():
         assert rel_l2(A, g[f'A{k}']) < 1e-13
 
 
-@pytest.mark.parametrize('name', ['argon', 'silica', 'xenon'])
+@pytest.mark.parametrize('name', ['argon', 'silica', 'xenon', 'silica_raman'])
 def test_realfield_oracle_matches_reference(name):
     """Real-field solver (src/3+1D-UPPE-ERK4(3)IP-real-field) run here: PPT table,
-    density + Drude current response, one step, and the adaptive run."""
+    density + Drude current response (with the fused-silica Raman convolution for
+    silica_raman), one step, and the adaptive run."""
     from oracle import realfield as rf
     g = golden(f'refrf_{name}')
     m = {'argon': lambda: rf.argon(800e-9, 1.0), 'silica': lambda: rf.fused_silica(800e-9),
-         'xenon': lambda: rf.xenon(800e-9, 2.0)}[name]()
+         'xenon': lambda: rf.xenon(800e-9, 2.0),
+         'silica_raman': lambda: rf.fused_silica(800e-9, use_raman=True)}[name]()
     assert np.array_equal(m.W_gpu, g['lut_W'])
-    P, J = m.response(g['E0'], float(g['t'][1] - g['t'][0]))
+    dt = float(g['t'][1] - g['t'][0])
+    m.init_raman(len(g['t']), dt)          # the reference's solver does this on construction
+    P, J = m.response(g['E0'], dt)
     assert np.array_equal(P, g['P']) and np.array_equal(J, g['J'])
     s = rf.Solver(g['x'], g['x'], g['t'], m)
     z, f, Ew, log = s.propagate(g['E0'], float(g['L']), tol=float(g['tol']), max_step=float(g['L']) / 4,

@@ -109,11 +109,13 @@ def _pulse(t):
     return gaussian_pulse(t, 2e9 * fw * np.sqrt(np.pi / (4 * np.log(2))), fw)
 
 
-def test_noalloc_complex64_at_its_limit_with_plasma_vs_plan_and_oracle():
+def test_noalloc_complex64_at_its_limit_with_plasma_vs_plan_and_oracle(monkeypatch):
     """Complex64 at Nt = UPPE_NOALLOC_MAX_NT_C64 (the whole static array in use)
     with the plasma term on: the same attempts and field as the plan entry point
-    on two calls in a row, and the FP64 oracle within the mixed-precision
-    tolerance 1e-4."""
+    running the same one-CTA kernel (a plan of one 16384-point line would
+    otherwise take the cluster kernel) on two calls in a row, and the FP64
+    oracle within the mixed-precision tolerance 1e-4."""
+    monkeypatch.setenv('UPPE_1D_CLUSTER', '0')
     from project_b200 import _lib
     from project_b200.solver1d import BatchedPropagator
     osol, psol = _boosted_plasma_pair()
