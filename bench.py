@@ -512,9 +512,13 @@ def run_realfield(dev, cpu=True):
     """Real-field 3+1D solver (src/3+1D-UPPE-ERK4(3)IP-real-field): argon 1 atm,
     128 x 128 x 1024 real samples over 0.8 mm x 200 fs, 800 nm 20 fs pulse at
     4e10 V/m, single precision (the reference's); time per ERK attempt over CUDA
-    events, bytes per attempt from the pass list (74 spectral fields of
-    Nx Ny (Nt/2 + 16) complex64 plus 3 real-field passes), and the oracle's step
-    on a 32 x 32 x 1024 sample on the host."""
+    events, bytes per attempt from the pass list, and the oracle's step on a
+    32 x 32 x 1024 sample on the host.  Bytes: spectral fields F of Nx Ny (Nt/2 + 16)
+    complex64 and real fields R of Nx Ny Nt float32: rfft (R + F), x and y forward
+    transforms (4 F), inverse y of E_kw (2 F), per stage inverse x (2 F), the
+    nonlinear t-line pass (2 F) and forward x (2 F), then the fused y pass with the
+    stage algebra (5, 6, 5, 5 F), and the output (inverse x 2 F, irfft F + R):
+    55 F + 2 R."""
     import torch
     from project_b200.realfield import Argon, ERK43_RealField_UPPE_3D
     N, Nt = 128, 1024
@@ -541,11 +545,11 @@ def run_realfield(dev, cpu=True):
     Nw = Nt // 2 + 16
     Fs = N * N * Nw * 8
     Fr = N * N * Nt * 4
-    byts = 74 * Fs + 3 * Fr
+    byts = 55 * Fs + 2 * Fr
     out = {'workload': 'real-field 3+1D ERK4(3)-IP attempt, argon 1 atm, 128x128x1024, 0.8 mm x 200 fs, '
                        '20 fs 800 nm at 4e10 V/m, PPT + Drude current, single precision',
            'ms_per_attempt': ms, 'value': N * N * Nt / (ms / 1e3), 'unit': 'pt-steps/s',
-           'achieved_gbs': byts / (ms / 1e3) / 1e9, 'bytes_model': '74 spectral + 3 real field passes per attempt'}
+           'achieved_gbs': byts / (ms / 1e3) / 1e9, 'bytes_model': '55 spectral + 2 real field passes per attempt'}
     if cpu:
         from oracle import realfield as orf
         xs = np.linspace(-0.4e-3, 0.4e-3, 32)
@@ -596,7 +600,7 @@ def profile_kernels(sol, lib, n_attempts=3):
             if byts[i] == 0:
                 continue
             name = {0: 'k_tpass_w', 1: 'k_xpass_sq', 2: 'k_space', 4: 'k_ypass_tma',
-                    5: 'k_ypass_rq'}.get(kind[i], 'scalar')
+                    5: 'k_ypass_rq', 6: 'k_ypass_tq'}.get(kind[i], 'scalar')
             a = agg.setdefault(name, [0.0, 0.0, 0])
             a[0] += ms[i]
             a[1] += byts[i]
@@ -797,12 +801,12 @@ def plan_tuning(sol):
     ms = (ctypes.c_float * _lib.UPPE3D_TUNE_SLOTS)()
     _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
     names = ['tma16 2/SM', 'tma16 1/SM', 'tma16 late 3/SM', 'tma16 late 2/SM', 'tma8 4/SM', 'tma8 late 6/SM',
-             'reg4step 2/SM', 'reg4step late 3/SM']
-    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step'}[cfg[0]]
+             'reg4step 2/SM', 'reg4step late 3/SM', 'reg4step tma 2/SM']
+    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step', 3: 'reg4step tma'}[cfg[0]]
     y = kind if not cfg[0] else f"{kind}{' late' if cfg[2] else ''} {cfg[1]}/SM"
     return {'y_pass': y, 't_lines_per_block': cfg[4], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[5]],
-            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:8]) if v > 0},
-            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[8:10]) if v > 0}}
+            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:9]) if v > 0},
+            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[9:11]) if v > 0}}
 
 
 def run_b200(args, rank, world, local_rank):
@@ -1047,6 +1051,36 @@ def run_profile_case(args):
     return 0
 
 
+def run_profile_realfield(args):
+    """Only the real-field propagator (the realfield_3d workload), for profiler
+    commands: --warmup untimed attempts, then --steps attempts inside an NVTX range
+    named "timed"."""
+    import torch
+    from project_b200.realfield import Argon, ERK43_RealField_UPPE_3D
+    N, Nt = 128, 1024
+    x = np.linspace(-0.4e-3, 0.4e-3, N)
+    t = np.linspace(-100e-15, 100e-15, Nt)
+    X, Y = np.meshgrid(x, x, indexing='ij')
+    w = 2 * np.pi * 299792458.0 / 800e-9
+    env = np.exp(-2 * np.log(2) * t ** 2 / (20e-15) ** 2) * np.cos(w * t)
+    E0 = (4e10 * np.exp(-(X ** 2 + Y ** 2) / (0.2e-3) ** 2)[:, :, None] * env[None, None, :]).astype(np.float32)
+    sol = ERK43_RealField_UPPE_3D(x, x, t, Argon(800e-9, 1.0), precision='single')
+    sol.set_field(torch.from_numpy(E0).cuda())
+    for _ in range(args.warmup):
+        sol.attempt(1e-6)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push('timed')
+    e0.record()
+    for _ in range(args.steps):
+        sol.attempt(1e-6)
+    e1.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    print(json.dumps({'ms_per_attempt': e0.elapsed_time(e1) / max(args.steps, 1), 'grid': [N, N, Nt]}), flush=True)
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -1061,6 +1095,8 @@ def main():
     ap.add_argument('--no-realfield', action='store_true')
     ap.add_argument('--no-accuracy', action='store_true')
     ap.add_argument('--no-ionising', action='store_true')
+    ap.add_argument('--profile-realfield', action='store_true',
+                    help='only the real-field attempts (for profilers): --warmup untimed, --steps in an NVTX range')
     ap.add_argument('--profile-case', action='store_true',
                     help='only the solver: warm-up + timed attempts (a short command for ncu)')
     ap.add_argument('--profile-z', type=float, default=0.0, help='profile case: start the timed attempts at z')
@@ -1075,6 +1111,8 @@ def main():
         args.warmup = 3
     if args.impl == 'reference':
         return run_reference(args, rank)
+    if args.profile_realfield:
+        return run_profile_realfield(args)
     if args.profile_case:
         return run_profile_case(args)
     import datetime

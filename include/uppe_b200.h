@@ -118,6 +118,27 @@ int uppe3d_begin(uppe3d_plan* plan, double L, double tol, double max_step, doubl
 int uppe3d_run_steps(uppe3d_plan* plan, int nsteps, uppe_stream_t stream);
 int uppe3d_get_result(uppe3d_plan* plan, uppe3d_result* result, uppe_stream_t stream);
 
+/* Continuation of an adaptive run (no reference counterpart; the reference's drivers
+ * restart propagate from the last field, which resets the step size): the state
+ * between two attempts.  uppe3d_save_state copies it out (field_out: device buffer
+ * of uppe3d_field_bytes, the accepted state in the plan's layout, normalised by
+ * A_scale); uppe3d_load_state puts it into a plan of the same grid, precision and
+ * medium, after which uppe3d_resume (or uppe3d_run_steps) continues the run with the
+ * same attempts, step sizes and fields as the uninterrupted run, bit for bit. */
+typedef struct {
+  double z, h, L, tol, max_step, min_step;
+  double err;              /* error of the last attempt                            */
+  double A_scale;
+  double peak_ion;         /* running max of rho / rho_nt                           */
+  long long attempts, accepted, max_attempts;
+  int fail_count, status, done;
+} uppe3d_state;
+int uppe3d_save_state(uppe3d_plan* plan, void* field_out, uppe3d_state* state, uppe_stream_t stream);
+int uppe3d_load_state(uppe3d_plan* plan, const void* field_in, const uppe3d_state* state, uppe_stream_t stream);
+/* The adaptive loop of uppe3d_propagate from the plan's current state (after
+ * uppe3d_load_state or uppe3d_begin + uppe3d_run_steps). */
+int uppe3d_resume(uppe3d_plan* plan, uppe3d_result* result, uppe_stream_t stream);
+
 /* End of propagate (solver_3d.py:215-222): out = fftshift_t(fft_t(A * A_scale)). */
 int uppe3d_get_spectrum(uppe3d_plan* plan, void* out, uppe_stream_t stream);
 /* Time-domain field A(x, y, t) of the current state (physical units), for
@@ -404,21 +425,22 @@ int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, do
  * per SM, or where they are used with 3 or 2) or of 8 columns (early with 4,
  * late with 6 CTAs per SM) -- complex64 plans with 64 <= Ny <= 256 -- then, for
  * Ny = 256, on the register four-step kernel (operands loaded with the tile, 2
- * CTAs per SM, or where used, 3), and 8 or 4 t-lines per block of the warp
- * t-line kernel.  All candidates compute identical bits (the plain tile kernel,
- * which rounds differently, serves the other shapes).  cfg6 = {y kernel (1
- * TMA-fed, 2 register four-step, 0 plain tile), CTAs per SM, late operand loads,
- * omega columns per tile, t-lines per block, 1 timed / 2 from the process cache
- * / 0 defaults (UPPE_TUNE=0)}; ms (may be NULL, UPPE3D_TUNE_SLOTS floats):
- * per-attempt time of the y passes for the eight y candidates in that order
- * [0..7] and of the t passes for 8 and 4 lines per block [8..9], in ms (0 when
- * not timed). */
-#define UPPE3D_TUNE_SLOTS 10
+ * CTAs per SM, or where used, 3) and on the register four-step kernel fed by
+ * TMA tiles (persistent, 2 CTAs per SM), and 8 or 4 t-lines per block of the
+ * warp t-line kernel.  All candidates compute identical bits (the plain tile
+ * kernel, which rounds differently, serves the other shapes).  cfg6 = {y kernel
+ * (1 TMA-fed, 2 register four-step, 3 register four-step on TMA tiles, 0 plain
+ * tile), CTAs per SM, late operand loads, omega columns per tile, t-lines per
+ * block, 1 timed / 2 from the process cache / 0 defaults (UPPE_TUNE=0)}; ms (may
+ * be NULL, UPPE3D_TUNE_SLOTS floats): per-attempt time of the y passes for the
+ * nine y candidates in that order [0..8] and of the t passes for 8 and 4 lines
+ * per block [9..10], in ms (0 when not timed). */
+#define UPPE3D_TUNE_SLOTS 11
 int uppe3d_tuning(const uppe3d_plan* plan, int* cfg6, float* ms);
-/* Force a launch configuration (y_tma 1 TMA-fed, 2 register four-step -- Ny =
- * 256 complex64 only --, 0 the plain tile kernel; y_ctas 1..6, y_kw 16 or 8,
- * t_wpb 4 or 8) and re-capture the attempt graphs; for comparing the
- * candidates. */
+/* Force a launch configuration (y_tma 1 TMA-fed, 2 register four-step, 3
+ * register four-step on TMA tiles -- 2 and 3: Ny = 256 complex64 only, 3 without
+ * late loads --, 0 the plain tile kernel; y_ctas 1..6, y_kw 16 or 8, t_wpb 4 or
+ * 8) and re-capture the attempt graphs; for comparing the candidates. */
 int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
@@ -426,7 +448,7 @@ int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,
  * bracketing each launch with CUDA events on `stream`.  Writes per launch its
  * time [ms], pass kind (0 t-line, 1 x-pass, 2 y-pass, 3 scalar, 4 TMA-fed y-pass, 5 register
- * four-step y-pass) and algorithmic
+ * four-step y-pass, 6 register four-step y-pass on TMA tiles) and algorithmic
  * bytes (0 for launches the device state made exit early). */
 int uppe3d_profile_attempt(uppe3d_plan* plan, int cap, float* ms, int* kind, double* bytes,
                            int* n, uppe_stream_t stream);

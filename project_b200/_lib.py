@@ -16,8 +16,8 @@ UPPE_C64, UPPE_C128 = 0, 1
 STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS, STATUS_RETRIED = 1, 2, 4, 64
 # line limits of uppe1d_propagate_noalloc (its static device array)
 UPPE_NOALLOC_MAX_NT_C64, UPPE_NOALLOC_MAX_NT_C128 = 16384, 8192
-# timing slots of uppe3d_tuning: eight y-pass candidates, then two t-pass ones
-UPPE3D_TUNE_SLOTS = 10
+# timing slots of uppe3d_tuning: nine y-pass candidates, then two t-pass ones
+UPPE3D_TUNE_SLOTS = 11
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double
@@ -37,6 +37,13 @@ class Desc3D(ctypes.Structure):
 class Result3D(ctypes.Structure):
     _fields_ = [('z', _D), ('h', _D), ('err', _D), ('attempts', _LL), ('accepted', _LL),
                 ('fail_count', _I), ('status', _I), ('A_scale', _D)]
+
+
+class State3D(ctypes.Structure):
+    """uppe3d_state: the adaptive loop's state between two attempts."""
+    _fields_ = [('z', _D), ('h', _D), ('L', _D), ('tol', _D), ('max_step', _D), ('min_step', _D),
+                ('err', _D), ('A_scale', _D), ('peak_ion', _D), ('attempts', _LL), ('accepted', _LL),
+                ('max_attempts', _LL), ('fail_count', _I), ('status', _I), ('done', _I)]
 
 
 class InstDesc1D(ctypes.Structure):
@@ -84,6 +91,9 @@ SIGNATURES = {
     'uppe3d_begin': (_I, [_P, _D, _D, _D, _D, _LL, _P]),
     'uppe3d_run_steps': (_I, [_P, _I, _P]),
     'uppe3d_get_result': (_I, [_P, ctypes.POINTER(Result3D), _P]),
+    'uppe3d_save_state': (_I, [_P, _P, ctypes.POINTER(State3D), _P]),
+    'uppe3d_load_state': (_I, [_P, _P, ctypes.POINTER(State3D), _P]),
+    'uppe3d_resume': (_I, [_P, ctypes.POINTER(Result3D), _P]),
     'uppe3d_get_spectrum': (_I, [_P, _P, _P]),
     'uppe3d_get_field': (_I, [_P, _P, _P]),
     'uppe3d_launches_per_step': (_I, [_P]),

@@ -12,9 +12,19 @@
 // inverse without the 1/N factor (callers fold it into a power-of-two scale).
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 #include <stdint.h>
 
 namespace uppe {
+
+// NVTX range over a library call (host side; popped on every return path), so a
+// profiler timeline shows propagate / adjoint / program calls by name
+struct NvtxRange {
+  explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+  ~NvtxRange() { nvtxRangePop(); }
+  NvtxRange(const NvtxRange&) = delete;
+  NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 template <typename R> struct CT;
 template <> struct CT<float>  { using T = float2; };
@@ -71,7 +81,7 @@ template <int R, int K, int DIR, typename C> __device__ __forceinline__ C rot(C 
   }
 }
 
-// In-register DFT of size R (R in {1,2,4,8,16}); DIR=-1 forward, +1 inverse.
+// In-register DFT of size R (R in {1,2,4,8,16,32}); DIR=-1 forward, +1 inverse.
 template <int R, int DIR, typename C> struct DFT {
   __device__ __forceinline__ static void run(C* v) {
     C e[R / 2], o[R / 2];
@@ -216,6 +226,8 @@ template <int WIDTH = 32, typename R> __device__ __forceinline__ R warp_max(R v)
 struct Lut {
   const void* x;    // grid, field precision
   const void* w;    // rates, field precision
+  const double* slope;   // (w[j+1] - w[j]) / (x[j+1] - x[j]) in FP64 from the field-precision
+                         // values, j < n - 1 (or null: computed per evaluation)
   int n;
   double x0, inv_dx;
   double zero_x;    // W is exactly 0 for clipped log10(I) <= zero_x (-inf if none)
@@ -249,9 +261,18 @@ __device__ __forceinline__ Rl lut_eval(const Lut& L, Rl I) {
   if (j >= n - 1) return __ldg(fp + n - 1);
   const Rl xj = __ldg(xp + j);
   if (xj == x) return __ldg(fp + j);
-  const double slope = ((double)__ldg(fp + j + 1) - (double)__ldg(fp + j)) /
-                       ((double)__ldg(xp + j + 1) - (double)xj);
+  const double slope = L.slope ? __ldg(L.slope + j)
+                               : ((double)__ldg(fp + j + 1) - (double)__ldg(fp + j)) /
+                                     ((double)__ldg(xp + j + 1) - (double)xj);
   return (Rl)(slope * ((double)x - (double)xj) + (double)__ldg(fp + j));
+}
+
+// the slope table of lut_eval: the same FP64 quotients, formed once on the host
+// (IEEE division rounds identically there), from the table in the field precision
+template <typename Rl>
+static inline void lut_slopes(const double* x, const double* w, int n, double* out) {
+  for (int j = 0; j + 1 < n; ++j)
+    out[j] = ((double)(Rl)w[j + 1] - (double)(Rl)w[j]) / ((double)(Rl)x[j + 1] - (double)(Rl)x[j]);
 }
 
 // Plasma constants shared by the 1D and 3D nonlinear kernels.

@@ -70,6 +70,7 @@ extern "C" int uppe1d_plan_destroy(uppe1d_plan* p) {
 }
 
 extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
+  NvtxRange nvtx_range("uppe1d_plan_create");
   *out = nullptr;
   g_uppe_err[0] = 0;
   if (!d || d->n_inst <= 0 || !d->inst || !d->D || !d->G) return UPPE_ERR_ARG;
@@ -190,6 +191,13 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     }
     TRY1(up1(p, &ptr, lx.data(), lx.size())); p->b.lut.x = ptr;
     TRY1(up1(p, &ptr, lw.data(), lw.size())); p->b.lut.w = ptr;
+    {
+      std::vector<double> sl(n - 1);
+      if (dbl) lut_slopes<double>(d->lut_log10I, d->lut_W, n, sl.data());
+      else lut_slopes<float>(d->lut_log10I, d->lut_W, n, sl.data());
+      TRY1(up1(p, &ptr, sl.data(), sl.size() * sizeof(double)));
+      p->b.lut.slope = static_cast<const double*>(ptr);
+    }
     p->b.lut.n = n;
     p->b.lut.x0 = d->lut_log10I[0];
     p->b.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
@@ -208,6 +216,7 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
     }
   } else {
     p->b.lut.x = p->b.lut.w = nullptr;
+    p->b.lut.slope = nullptr;
     p->b.lut.n = 0;
     p->b.lut.zero_x = INFINITY;
     p->b.lut.I_zero = INFINITY;
@@ -298,6 +307,7 @@ extern "C" long long uppe1d_hist_slots(const uppe1d_plan* p) { return p ? p->zht
 
 extern "C" int uppe1d_propagate(uppe1d_plan* p, void* field, void* hist, double* zhist,
                                 uppe1d_result* results, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe1d_propagate");
   if (!p || !field) return UPPE_ERR_ARG;
   if (p->htotal > 0 && (!hist || !zhist)) {
     snprintf(g_uppe_err, sizeof(g_uppe_err), "plan has history slots: hist and zhist are required");
@@ -343,6 +353,7 @@ static int run1(uppe1d_plan* p, Batch1D& b, uppe1d_result* results, cudaStream_t
 
 extern "C" int uppe1d_propagate_logged(uppe1d_plan* p, void* field, double* hlog, int hlog_cap,
                                        uppe1d_result* results, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe1d_propagate_logged");
   if (!p || !field || !hlog || hlog_cap <= 0 || p->htotal > 0) return UPPE_ERR_ARG;
   Batch1D b = p->b;
   b.field = field;
@@ -353,6 +364,7 @@ extern "C" int uppe1d_propagate_logged(uppe1d_plan* p, void* field, double* hlog
 
 extern "C" int uppe1d_propagate_schedule(uppe1d_plan* p, void* field, const double* hsched,
                                          int nsched, uppe1d_result* results, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe1d_propagate_schedule");
   if (!p || !field || !hsched || nsched < 0 || p->htotal > 0) return UPPE_ERR_ARG;
   Batch1D b = p->b;
   b.field = field;
@@ -369,6 +381,7 @@ static int prog_fail(const char* msg) {
 extern "C" int uppe1d_run_programs(uppe1d_plan* p, int nprog, const long long* op_begin,
                                    const uppe1d_op* ops, void* fields, void* records,
                                    uppe1d_result* op_results, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe1d_run_programs");
   g_uppe_err[0] = 0;
   if (!p || nprog <= 0 || !op_begin || !ops || !fields) return prog_fail("null argument or nprog <= 0");
   if (op_begin[0] != 0) return prog_fail("op_begin[0] must be 0");
@@ -492,6 +505,7 @@ extern "C" long long uppe1d_adjoint_work_elems(int Nt, int nsteps, int K) {
 extern "C" int uppe1d_adjoint(uppe1d_plan* p, int inst, const double* hlog, int nsteps, int K,
                               const void* A0, const void* Abar, void* A0bar, void* gD, double* gG,
                               void* rhs, double* gPlasma, void* work, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe1d_adjoint");
   g_uppe_err[0] = 0;
   if (!p || inst < 0 || inst >= p->ninst || !hlog || nsteps < 0 || K <= 0 || !A0 || !Abar ||
       !A0bar || !gD || !gG || !rhs || !work)

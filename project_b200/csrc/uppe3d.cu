@@ -1162,6 +1162,180 @@ static constexpr size_t yrq_smem() {
 }
 
 // ---------------------------------------------------------------------------
+// The same y passes (complex64, Ny = 256) on persistent CTAs, two per SM: the
+// tile arrives one tile ahead by cp.async.bulk.tensor into one of two shared
+// buffers, as in k_ypass_tma, so the tile's HBM stream costs no registers and
+// overlaps the transforms; each thread then takes rows j + 16 i of column w into
+// registers and runs the register four-step FFT of k_ypass_rq, with the landed
+// buffer doubling as the transpose buffer.  Stage operands are loaded into
+// registers at the start of each tile, before its wait.  Same arithmetic element
+// by element as k_ypass_rq (hence as k_ypass_tma).
+// ---------------------------------------------------------------------------
+template <int MODE>
+__global__ void __launch_bounds__(kW * 16, 2)
+k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
+  using C = float2;
+  using Rl = float;
+  constexpr int R = 16, N = R * R, NTHR = kW * R, TILE = N * kW;
+  constexpr bool TWO = MODE == YMID1;          // YMID1 also transforms fft_x(Z) = tmp[2]
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* buf[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + TILE};
+  C* tw = buf[1] + TILE;
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);   // [2]
+  double* qrow = reinterpret_cast<double*>(mbar + 2);   // k_perp^2 of the tile's kx row
+  State3D* st = a.st;
+  if (st->done) return;
+  if (MODE == YMID1R && st->fresh) return;
+  if (MODE == YMID1 && !st->fresh) return;
+  const int tid = threadIdx.x, w = tid % kW, j = tid / kW;
+  const int Nt = a.g.Nt;
+  const int ntw = Nt / kW;
+  const int total = a.g.Nx * ntw;
+  const CUtensorMap* map = MODE == YMID1R ? &maps.acur : &maps.in;
+  auto issue = [&](int tile, int b) {
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const unsigned bar = smem_u32(&mbar[b]);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(bar), "r"((unsigned)(TILE * sizeof(C))) : "memory");
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+        :: "r"(smem_u32(buf[b])), "l"(reinterpret_cast<unsigned long long>(map)), "r"(w0), "r"(0), "r"(o),
+           "r"(bar)
+        : "memory");
+  };
+  if (tid == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  {
+    const C* gtw = reinterpret_cast<const C*>(a.tb.twy);
+    for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
+  }
+  __syncthreads();
+  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
+  C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
+  C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
+  C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
+  C* __restrict__ out = reinterpret_cast<C*>(a.out);
+  C* __restrict__ su = reinterpret_cast<C*>(a.save_u);
+  const C* __restrict__ z2 = reinterpret_cast<const C*>(a.b.tmp[2]);
+  const double h = st->h;
+  const double h2 = 0.5 * h;
+  const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
+  double red = 0.0;
+  int k = 0;
+  for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
+    const int b = k & 1;
+    const bool next = tile + (int)gridDim.x < total;
+    if (tid == 0 && next) issue(tile + gridDim.x, b ^ 1);
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const long long base = (long long)o * N * Nt + w0 + w;
+    auto gidx = [&](int i) { return base + (long long)(j + R * i) * Nt; };
+    C opA[R], opB[R], v2[TWO ? R : 1];
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const long long gi = gidx(i);
+      if constexpr (MODE == YMID2 || MODE == YMID3) { opA[i] = __ldg(acur + gi); opB[i] = __ldg(tsum + gi); }
+      else if constexpr (MODE == YMID4) opB[i] = __ldg(tsum + gi);
+      else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
+      else if constexpr (MODE == YFWD5) opA[i] = __ldg(a4p + gi);
+      if constexpr (TWO) v2[i] = __ldg(z2 + gi);
+    }
+    if (MODE != YMID4 && MODE != YFWD5) qrow[tid] = __ldg(a.tb.q + (long long)o * N + tid);   // NTHR == N
+    const bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+    if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
+      if (tid == 0) {
+        atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT);
+        st->done = 1;
+        // every copy this CTA started must have landed before it exits: wait again,
+        // bounded, on each barrier with a copy in flight
+        mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+        if (next) mbar_wait(smem_u32(&mbar[b ^ 1]), (unsigned)(((k + 1) >> 1) & 1));
+      }
+      return;
+    }
+    C* s = buf[b];
+    C v[R];
+#pragma unroll
+    for (int i = 0; i < R; ++i) v[i] = s[(j + R * i) * kW + w];
+    __syncthreads();                  // the tile is in registers: its buffer is the transpose buffer
+    if constexpr (MODE != YMID1R) fft_sq<R, -1>(v, s, tw, j, w);
+    if constexpr (TWO) fft_sq<R, -1>(v2, s, tw, j, w);
+    const OmegaCol oc(a.tb, w0 + w);
+#pragma unroll
+    for (int i = 0; i < R; ++i) {
+      const int n = j + R * i;
+      const long long gi = gidx(i);
+      if constexpr (MODE == YFWD5) {
+        const C a5 = v[i], a4 = opA[i];
+        const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
+        const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+        red = (d > red || d != d) ? d : red;
+        continue;
+      }
+      if constexpr (MODE == YMID4) {
+        const C a4 = v[i];
+        const C A4 = cadd(opB[i], cscale(a4, h6R));
+        a4p[gi] = a4;
+        const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+        red = (m > red || m != m) ? m : red;
+        v[i] = A4;
+        continue;
+      }
+      const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qrow[n], h2);
+      C u;
+      if constexpr (MODE == YMID1R) {   // v = A, opB = k1
+        const C vv = cmul(v[i], Ef);
+        const C a1 = cmul(opB[i], Ef);
+        tsum[gi] = a1;
+        u = cadd(vv, cscale(a1, h2R));
+      } else if constexpr (MODE == YMID1) {   // v = k1 = N(A), v2 = A
+        const C A = v2[i], k1 = v[i];
+        acur[gi] = A;
+        k1b[gi] = k1;
+        const C vv = cmul(A, Ef);
+        const C a1 = cmul(k1, Ef);
+        tsum[gi] = a1;
+        u = cadd(vv, cscale(a1, h2R));
+      } else if constexpr (MODE == YMID2) {
+        const C a2 = v[i];
+        const C vv = cmul(opA[i], Ef);
+        tsum[gi] = cadd(opB[i], cscale(a2, (Rl)2));
+        u = cadd(vv, cscale(a2, h2R));
+      } else {   // YMID3
+        const C a3 = v[i];
+        const C vv = cmul(opA[i], Ef);
+        const C ts = cadd(opB[i], cscale(a3, (Rl)2));
+        tsum[gi] = cmul(cadd(vv, cscale(ts, h6R)), Ef);
+        u = cmul(cadd(vv, cscale(a3, hR)), Ef);
+      }
+      v[i] = u;
+      if (su) su[gi] = u;
+    }
+    if constexpr (MODE != YFWD5) {
+      fft_sq<R, +1>(v, s, tw, j, w);
+#pragma unroll
+      for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
+    }
+    // buffer b is refilled by the copy issued at iteration k + 1: order this
+    // iteration's shared-memory accesses before that async-proxy write
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();
+  }
+  if constexpr (MODE == YMID4 || MODE == YFWD5) {
+    red = warp_max<32>(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+  }
+}
+
+static constexpr size_t ytq_smem() {
+  return sizeof(float2) * (size_t)(2 * 256 * kW + 256) + 2 * sizeof(unsigned long long) + 256 * sizeof(double);
+}
+
+// ---------------------------------------------------------------------------
 // Warp FFT of a t-line of NT = 32*E points held in registers (E = 16 or 32).
 // Natural layout: lane l holds x[l + 32 m], m < E.  Four-step layout: lane L
 // holds X[out_index(L, k)], k < E.  fwd_like: DFT_E in registers, twiddle
@@ -1662,7 +1836,7 @@ struct uppe3d_plan {
   int nsm = 148;
   // launch configuration picked per shape by the tuner (uppe3d_tuning): every
   // candidate computes the same bits, only the time differs
-  int y_tma = 1;                  // y passes on k_ypass_tma (1), k_ypass_rq (2) or k_space (0)
+  int y_tma = 1;                  // y passes on k_ypass_tma (1), k_ypass_rq (2), k_ypass_tq (3) or k_space (0)
   int y_ctas = 2;                 // k_ypass_tma CTAs per SM (1..6; k_ypass_rq: 2 or 3, fixed by LATE)
   int y_late = 0;                 // the y kernel loads the stage operands where used (1)
   int y_kw = kW;                  // k_ypass_tma omega columns per tile (16 or 8)
@@ -1740,6 +1914,35 @@ static bool yrq_ok(const uppe3d_plan* p) { return p->ytma && !p->dbl && p->g.Ny 
 static bool use_yrq(const uppe3d_plan* p, int mode, const void* in) {
   return p->y_tma == 2 && yrq_ok(p) && fused_ypass(p, mode, in);
 }
+static bool use_ytq(const uppe3d_plan* p, int mode, const void* in) {
+  return p->y_tma == 3 && yrq_ok(p) && fused_ypass(p, mode, in);
+}
+
+static void launch_ytq(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
+  const dim3 g((unsigned)(2 * p->nsm));
+  constexpr unsigned T = kW * 16;
+  constexpr size_t sm = ytq_smem();
+  const YMaps& mp = p->ymaps;
+  switch (a.mode) {
+    case YMID1: k_ypass_tq<YMID1><<<g, T, sm, s>>>(a, mp); break;
+    case YMID1R: k_ypass_tq<YMID1R><<<g, T, sm, s>>>(a, mp); break;
+    case YMID2: k_ypass_tq<YMID2><<<g, T, sm, s>>>(a, mp); break;
+    case YMID3: k_ypass_tq<YMID3><<<g, T, sm, s>>>(a, mp); break;
+    case YMID4: k_ypass_tq<YMID4><<<g, T, sm, s>>>(a, mp); break;
+    default: k_ypass_tq<YFWD5><<<g, T, sm, s>>>(a, mp); break;
+  }
+}
+
+static cudaError_t set_ytq_attr() {
+  const int sm = (int)ytq_smem();
+  cudaError_t e = cudaFuncSetAttribute(k_ypass_tq<YMID1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YFWD5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  return e;
+}
 
 template <int LATE>
 static void launch_yrq_l(const SpaceArgs& a, unsigned nblocks, cudaStream_t s) {
@@ -1815,6 +2018,10 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
   a.save_u = (mode == YMID1 || mode == YMID1R) ? p->save_u[0]
            : mode == YMID2 ? p->save_u[1] : mode == YMID3 ? p->save_u[2] : nullptr;
   a.scale = p->pass_scale;
+  if (sizeof(Rl) == 4 && use_ytq(p, mode, in)) {
+    launch_ytq(p, a, s);
+    return 0;
+  }
   if (sizeof(Rl) == 4 && use_yrq(p, mode, in)) {
     const unsigned nb = (unsigned)((long long)p->g.Nx * (p->g.Nt / kW));
     if (p->y_late) launch_yrq_l<1>(a, nb, s);
@@ -1975,7 +2182,7 @@ struct Recorder {
   }
 };
 
-enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3, KIND_YT = 4, KIND_YR = 5 };
+enum { KIND_T = 0, KIND_X = 1, KIND_Y = 2, KIND_SMALL = 3, KIND_YT = 4, KIND_YR = 5, KIND_YQ = 6 };
 
 // the fixed pass sequence of one attempt (see the file header); the numbers are
 // the fields each launch reads + writes (algorithmic bytes / field bytes)
@@ -1986,7 +2193,8 @@ static int enqueue_attempt(uppe3d_plan* p, Recorder& r) {
   void* const* t = p->b.tmp;
   const bool f = r.fresh != 0;
   // the fused y passes: k_ypass_rq, k_ypass_tma or the plain tile kernel
-  const int KY = (p->y_tma == 2 && yrq_ok(p)) ? KIND_YR : (p->ytma && p->y_tma == 1) ? KIND_YT : KIND_Y;
+  const int KY = (p->y_tma == 3 && yrq_ok(p)) ? KIND_YQ : (p->y_tma == 2 && yrq_ok(p)) ? KIND_YR
+               : (p->ytma && p->y_tma == 1) ? KIND_YT : KIND_Y;
   // eval 1 (skipped on device unless the state is fresh)
   rc |= r(KIND_T, 2, f, [&] { return launch_t<Rl, 0>(p, T_FROM_Z, nullptr, t[0], s); });
   rc |= r(KIND_X, 4, f, [&] { return launch_space<Rl>(p, XFWD_Z, t[0], t[1], s); });
@@ -2050,7 +2258,7 @@ static int setup_ytma(uppe3d_plan* p) {
   switch (p->g.Ny) {
     case 64: UPPE_CK(set_ytma_attr<64>()); break;
     case 128: UPPE_CK(set_ytma_attr<128>()); break;
-    case 256: UPPE_CK(set_ytma_attr<256>()); break;
+    case 256: UPPE_CK(set_ytma_attr<256>()); UPPE_CK(set_ytq_attr()); break;
     default: return 0;
   }
   p->ytma = true;
@@ -2095,7 +2303,8 @@ static int time_attempts(uppe3d_plan* p, cudaStream_t s, int reps, float* y_ms, 
     for (size_t i = 0; i < rec.kind.size(); ++i) {
       float ms = 0.f;
       cudaEventElapsedTime(&ms, rec.ev[2 * i], rec.ev[2 * i + 1]);
-      if (rec.kind[i] == KIND_Y || rec.kind[i] == KIND_YT || rec.kind[i] == KIND_YR) *y_ms += ms;
+      if (rec.kind[i] == KIND_Y || rec.kind[i] == KIND_YT || rec.kind[i] == KIND_YR || rec.kind[i] == KIND_YQ)
+        *y_ms += ms;
       if (rec.kind[i] == KIND_T) *t_ms += ms;
     }
     for (auto e : rec.ev) cudaEventDestroy(e);
@@ -2134,10 +2343,12 @@ static int tune(uppe3d_plan* p) {
   k_set_scale_one<<<1, 1, 0, s>>>(p->st);
   // the plain tile kernel rounds differently from the TMA-fed one, so it is a
   // candidate only where the TMA path is unavailable; the register four-step
-  // kernel gives the TMA-fed kernel's bits and serves Ny = 256
-  struct YC { int tma, ctas, late, kw; } yc[8] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
-                                                {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW}};
-  const int ny = p->ytma ? (yrq_ok(p) ? 8 : 6) : 1;
+  // kernels (plain loads or TMA-fed tiles) give the TMA-fed kernel's bits and
+  // serve Ny = 256
+  struct YC { int tma, ctas, late, kw; } yc[9] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
+                                                {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW},
+                                                {3, 2, 0, kW}};
+  const int ny = p->ytma ? (yrq_ok(p) ? 9 : 6) : 1;
   if (!p->ytma) yc[0] = YC{0, 2, 0, kW};
   const int tw_n = (p->g.Nt == 512 || (p->g.Nt == 1024 && !p->dbl)) ? 2 : 1;
   const int tw[2] = {8, 4};
@@ -2157,7 +2368,7 @@ static int tune(uppe3d_plan* p) {
   for (int i = 0; i < tw_n && !rc; ++i) {      // t candidates with the chosen y passes
     p->t_wpb = tw[i];
     rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
-    p->tune_ms[8 + i] = t_ms;
+    p->tune_ms[9 + i] = t_ms;
     if (t_ms < best_t) { best_t = t_ms; bt = i; }
   }
   p->t_wpb = tw[bt];
@@ -2191,6 +2402,7 @@ static int build_graphs(uppe3d_plan* p) {
 }
 
 extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
+  NvtxRange nvtx_range("uppe3d_plan_create");
   *out = nullptr;
   g_uppe_err[0] = 0;
   if (!d) return UPPE_ERR_ARG;
@@ -2261,6 +2473,13 @@ extern "C" int uppe3d_plan_create(const uppe3d_desc* d, uppe3d_plan** out) {
     }
     UPPE_TRY(dev_upload(p, &ptr, lx.data(), lx.size())); p->tb.lut.x = ptr;
     UPPE_TRY(dev_upload(p, &ptr, lw.data(), lw.size())); p->tb.lut.w = ptr;
+    {
+      std::vector<double> sl(n - 1);
+      if (dbl) lut_slopes<double>(d->lut_log10I, d->lut_W, n, sl.data());
+      else lut_slopes<float>(d->lut_log10I, d->lut_W, n, sl.data());
+      UPPE_TRY(dev_upload(p, &ptr, sl.data(), sl.size() * sizeof(double)));
+      p->tb.lut.slope = static_cast<const double*>(ptr);
+    }
     p->tb.lut.n = n;
     p->tb.lut.x0 = d->lut_log10I[0];
     p->tb.lut.inv_dx = (n - 1) / (d->lut_log10I[n - 1] - d->lut_log10I[0]);
@@ -2367,6 +2586,7 @@ static void fill_result(const State3D* h, uppe3d_result* r) {
 extern "C" int uppe3d_propagate(uppe3d_plan* p, double L, double tol, double max_step,
                                 double min_step, long long max_attempts, uppe3d_result* res,
                                 cudaStream_t s) {
+  NvtxRange nvtx_range("uppe3d_propagate");
   if (!p || !(tol > 0.0) || !(max_step > 0.0) || !(min_step > 0.0) || !(L >= 0.0)) return UPPE_ERR_ARG;
   if (max_attempts <= 0) max_attempts = UPPE_DEFAULT_MAX_ATTEMPTS;
   k_begin<<<1, 1, 0, s>>>(p->st, L, tol, max_step, min_step, max_attempts);
@@ -2406,6 +2626,60 @@ extern "C" int uppe3d_get_result(uppe3d_plan* p, uppe3d_result* res, cudaStream_
   return 0;
 }
 
+extern "C" int uppe3d_save_state(uppe3d_plan* p, void* field_out, uppe3d_state* out, cudaStream_t s) {
+  if (!p || !field_out || !out) return UPPE_ERR_ARG;
+  UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+  UPPE_CK(cudaStreamSynchronize(s));
+  const State3D& h = *p->st_host;
+  UPPE_CK(cudaMemcpyAsync(field_out, p->b.z[h.zidx], p->csz * (size_t)p->g.npts, cudaMemcpyDeviceToDevice, s));
+  out->z = h.z; out->h = h.h; out->L = h.L; out->tol = h.tol;
+  out->max_step = h.max_step; out->min_step = h.min_step;
+  out->err = h.err; out->A_scale = h.A_scale;
+  memcpy(&out->peak_ion, &h.ion_bits, sizeof(double));
+  out->attempts = h.attempts; out->accepted = h.accepted; out->max_attempts = h.max_attempts;
+  out->fail_count = h.fail_count; out->status = h.status; out->done = h.done;
+  return 0;
+}
+
+extern "C" int uppe3d_load_state(uppe3d_plan* p, const void* field_in, const uppe3d_state* in, cudaStream_t s) {
+  if (!p || !field_in || !in || !(in->A_scale > 0.0) || !(in->tol > 0.0) || !(in->min_step > 0.0) ||
+      !(in->max_step > 0.0))
+    return UPPE_ERR_ARG;
+  // the first stage of the next attempt is recomputed from the accepted state
+  // (fresh), which gives the same bits as the stored one of the interrupted run
+  State3D h;
+  memset(&h, 0, sizeof(h));
+  h.z = in->z; h.h = in->h; h.L = in->L; h.tol = in->tol;
+  h.max_step = in->max_step; h.min_step = in->min_step;
+  h.err = in->err; h.A_scale = in->A_scale; h.inv_A_scale = 1.0 / in->A_scale;
+  memcpy(&h.ion_bits, &in->peak_ion, sizeof(double));
+  h.attempts = in->attempts; h.accepted = in->accepted; h.max_attempts = in->max_attempts;
+  h.fail_count = in->fail_count; h.status = in->status; h.done = in->done;
+  h.zidx = 0;
+  h.fresh = 1;
+  h.hlog = nullptr;
+  UPPE_CK(cudaMemcpyAsync(p->b.z[0], field_in, p->csz * (size_t)p->g.npts, cudaMemcpyDeviceToDevice, s));
+  *p->st_host = h;
+  UPPE_CK(cudaMemcpyAsync(p->st, p->st_host, sizeof(State3D), cudaMemcpyHostToDevice, s));
+  UPPE_CK(cudaStreamSynchronize(s));   // st_host is reused by the next host read-back
+  return 0;
+}
+
+extern "C" int uppe3d_resume(uppe3d_plan* p, uppe3d_result* res, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe3d_resume");
+  if (!p) return UPPE_ERR_ARG;
+  int batch = 1;
+  for (;;) {
+    UPPE_CK(cudaMemcpyAsync(p->st_host, p->st, sizeof(State3D), cudaMemcpyDeviceToHost, s));
+    UPPE_CK(cudaStreamSynchronize(s));
+    if (p->st_host->done) break;
+    for (int i = 0; i < batch; ++i) UPPE_CK(cudaGraphLaunch(p->g_step, s));
+    if (batch < 16) batch *= 2;
+  }
+  if (res) fill_result(p->st_host, res);
+  return 0;
+}
+
 extern "C" int uppe3d_get_spectrum(uppe3d_plan* p, void* out, cudaStream_t s) {
   if (!p || !out) return UPPE_ERR_ARG;
   const long long nl = (long long)p->g.Nx * p->g.Ny;
@@ -2434,7 +2708,7 @@ extern "C" long long uppe3d_field_bytes(const uppe3d_plan* p) {
 
 extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg6, float* ms) {
   if (!p || !cfg6) return UPPE_ERR_ARG;
-  cfg6[0] = p->y_tma == 2 ? 2 : (p->ytma && p->y_tma) ? 1 : 0;
+  cfg6[0] = p->y_tma >= 2 ? p->y_tma : (p->ytma && p->y_tma) ? 1 : 0;
   cfg6[1] = p->y_ctas;
   cfg6[2] = p->y_late;
   cfg6[3] = p->y_kw;
@@ -2446,11 +2720,12 @@ extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg6, float* ms) {
 
 extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb) {
   if (!p || y_ctas < 1 || y_ctas > 6 || (y_kw != 8 && y_kw != kW) || (t_wpb != 4 && t_wpb != 8) ||
-      y_tma < 0 || y_tma > 2 || (y_tma == 2 && (!yrq_ok(p) || y_kw != kW)))
+      y_tma < 0 || y_tma > 3 || (y_tma >= 2 && (!yrq_ok(p) || y_kw != kW)) || (y_tma == 3 && y_late))
     return UPPE_ERR_ARG;
   p->y_tma = y_tma;
   p->y_late = y_late ? 1 : 0;
-  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_ctas;   // k_ypass_rq: fixed by its launch bounds
+  // k_ypass_rq / k_ypass_tq: CTAs per SM fixed by their launch bounds
+  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_tma == 3 ? 2 : y_ctas;
   p->y_kw = y_kw;
   p->t_wpb = t_wpb;
   if (p->g_attempt) { cudaGraphExecDestroy(p->g_attempt); p->g_attempt = nullptr; }
@@ -3185,6 +3460,7 @@ extern "C" int uppe3d_set_step_log(uppe3d_plan* p, double* hlog, long long cap, 
 
 extern "C" int uppe3d_adjoint(uppe3d_plan* p, const double* hlog_host, int nsteps, int K, const void* A0,
                               const void* Zbar, void* A0bar, void* work, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe3d_adjoint");
   if (!p || !hlog_host || nsteps < 0 || K <= 0 || !A0 || !Zbar || !A0bar || !work) return UPPE_ERR_ARG;
   if (p->md.g4 != 0.0 || (p->md.plasma && p->md.ava != 0.0)) {
     snprintf(g_uppe_err, sizeof(g_uppe_err),
@@ -3214,6 +3490,7 @@ struct RfConst {
   double I_coef, aval, chi3e, chi5e;           // I = I_coef E^2; W_ava = aval I; P = chi3e E^3 + chi5e E^5
   double fR;                                   // Raman fraction (0: none)
   double rr, dt, rho_nt, Ui, e2m, nu, exp_nu, step_J;   // density / Drude constants (float32-rounded inputs)
+  double inv_rho_nt;                           // 1 / rho_nt (the depletion factor as a product)
   double E_scale;
 };
 
@@ -3234,7 +3511,7 @@ enum RfLine { RF_FROM_T = 0, RF_NL = 1, RF_OUT = 2 };
 // the reference's density update for w_av = 0: Gamma = -rr exactly, so
 // exp(Gamma dt) and the step factor are the constants e_r and sf0
 __device__ __forceinline__ void rf_rho_step(double& rho, double wp, const RfConst& rc, double e_r, double sf0) {
-  double dep = (rc.rho_nt - rho) / rc.rho_nt;
+  double dep = (rc.rho_nt - rho) * rc.inv_rho_nt;
   if (dep < 0.0) dep = 0.0;
   double r = rho * e_r + wp * rc.rho_nt * dep * sf0;
   if (r > rc.rho_nt) r = rc.rho_nt;
@@ -3373,6 +3650,7 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
   }
   // ---- nonlinear response (media_physics.py:258-318 with the kernel :11-118) ----
   const Rl Es = (Rl)rc.E_scale;
+  const Rl inv_Es = (Rl)1 / Es;
   for (int t = lane; t < NT; t += 32) R[t] = (S[tpad(t)].x * invN) * Es;   // physical field
   __syncwarp();
   if constexpr (RAMAN) rf_raman<Rl, NT>(S, R, Q, tw, tb, rc, lane);   // E_eff^2 into Q; S free again
@@ -3440,12 +3718,12 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
           const Rl Ef = R[t];
           const double E = (double)(float)Ef;
           const double wp = (double)(float)S[tpad(t)].x;
-          double dep = (rc.rho_nt - rho) / rc.rho_nt;
+          double dep = (rc.rho_nt - rho) * rc.inv_rho_nt;
           if (dep < 0.0) dep = 0.0;
           const double gen = wp * rc.rho_nt * dep;            // w_av = 0
           const double Jl = fabs(E) > 1e-10 ? (gen * rc.Ui * E) / (E * E + 1e-20) : 0.0;
           const double nJ = Jf * rc.exp_nu + rc.e2m * rho * E * rc.step_J;
-          S[tpad(t)].y = (Rl)(Jf + Jl) / Es;
+          S[tpad(t)].y = (Rl)(Jf + Jl) * inv_Es;
           rf_rho_step(rho, wp, rc, e_r, sf0);
           Jf = nJ;
         }
@@ -3493,7 +3771,7 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
       const Rl E2 = E * E;
       P = P + ((c5 * E) * E2) * E2;
     }
-    S[tpad(t)].x = P / Es;
+    S[tpad(t)].x = P * inv_Es;
   }
   __syncwarp();
   // P and J (both real) share one complex transform, each scaled by its own line
@@ -3511,9 +3789,10 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
     mj = fmax(mj, __shfl_xor_sync(0xffffffffu, mj, off));
   }
   const Rl sP = mp > (Rl)0 ? mp : (Rl)1, sJ = mj > (Rl)0 ? mj : (Rl)1;
+  const Rl isP = (Rl)1 / sP, isJ = (Rl)1 / sJ;
   for (int t = lane; t < NT; t += 32) {
     const C pj = S[tpad(t)];
-    S[tpad(t)] = C{pj.x / sP, pj.y / sJ};
+    S[tpad(t)] = C{pj.x * isP, pj.y * isJ};
   }
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());    // F(P/sP + i J/sJ)
@@ -3543,60 +3822,98 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
 enum RfStage { RS_1 = 0, RS_2, RS_3, RS_4 };
 
 struct RfBufs {
-  void *ekw, *v, *a1, *u, *ts, *el, *na, *e4;
+  void *ekw, *v, *a1, *ts, *el;   // E_kw and the stage accumulators (kx, ky, omega)
 };
 
-// stage algebra of erk43_step (solver_3d.py:143-167) in (kx, ky, omega)
-template <typename Rl>
-__global__ void k_rf_stage(int mode, RfTables tb, RfBufs b, int Nt, int Nw, long long n, double h,
-                           unsigned long long* red) {
+// Stage algebra of erk43_step (solver_3d.py:143-167) fused with the y transforms
+// around it: the tile (Ny rows x kW omega columns at one kx) of x-transformed
+// N(u) is transformed along y (giving the stage's N in (kx, ky, omega)), the
+// stage algebra runs per element with exp((h/2) D), D = -i (kz - kref), formed in
+// FP64, and the next stage input (or, in the last stage, the candidate E4) is
+// transformed back along y and stored for the inverse x pass.  Per element:
+//   RS_1: v = L(E_kw), a1 = L(k1), u = v + h/2 a1
+//   RS_2: u = v + h/2 a2, ts = a1 + 2 a2, el = v + h/2 a1 + h/2 a2
+//   RS_3: u = L(v + h a3), ts += 2 a3
+//   RS_4: E4 = L(v + h/6 ts) + h/6 a4, E_low = L(el); max |E4 - E_low|, max |E4|
+// Omega bins at or above Nt/2 + 1 (row padding) stay zero.
+template <typename Rl, int N>
+__global__ void __launch_bounds__(SpaceCfg<N>::NTHR, 1)
+k_rf_ypass(int mode, RfTables tb, RfBufs b, int Nw, int NR, const void* in, void* out, const void* twy,
+           double h, unsigned long long* red) {
   using C = typename CT<Rl>::T;
-  const int NR = Nt / 2 + 1;
-  C *ekw = (C*)b.ekw, *v = (C*)b.v, *a1 = (C*)b.a1, *u = (C*)b.u, *ts = (C*)b.ts, *el = (C*)b.el,
-    *na = (C*)b.na, *e4 = (C*)b.e4;
+  constexpr int NTHR = SpaceCfg<N>::NTHR;
+  constexpr int E = SpaceCfg<N>::E;
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  C* tw = reinterpret_cast<C*>(smem_raw);
+  C* s = tw + N;
+  const int tid = threadIdx.x;
+  for (int i = tid; i < N; i += NTHR) tw[i] = reinterpret_cast<const C*>(twy)[i];
+  const int ntile = Nw / kW;
+  const int o = blockIdx.x / ntile;            // kx index
+  const int w0 = (blockIdx.x % ntile) * kW;    // omega offset
+  const long long stride = Nw;
+  const long long base = (long long)o * N * Nw + w0;
+  TileIdx<C> idx;
+  BlockSync sync;
+  load_tile<C, N, NTHR>(s, reinterpret_cast<const C*>(in), base, stride, tid);
+  __syncthreads();
+  stockham<N, kW, NTHR, -1, 1, C>(s, tw, tid, idx, sync);
+  C *ekw = (C*)b.ekw, *v = (C*)b.v, *a1 = (C*)b.a1, *ts = (C*)b.ts, *el = (C*)b.el;
   const Rl h2 = (Rl)(h / 2), h6 = (Rl)(h / 6), hR = (Rl)h;
   double mdiff = 0.0, mnorm = 0.0;
-  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-    const int k = (int)(i % Nw);
-    if (k >= NR) continue;
-    // exp((h/2) D), D = -i (kz - kref)
-    const double kz2 = tb.kk[k] - tb.kp2[i / Nw];
-    const double s = 0.5 * h;
+#pragma unroll
+  for (int i = 0; i < E; ++i) {
+    const int e = tid + i * NTHR;
+    const int n = e / kW, w = e % kW;            // n = ky
+    const int k = w0 + w;
+    const long long gi = base + n * stride + w;
+    if (k >= NR) { s[idx(w, n)] = C{(Rl)0, (Rl)0}; continue; }
+    const double kz2 = tb.kk[k] - tb.kp2[(long long)o * N + n];
+    const double sh = 0.5 * h;
     double mag = 1.0, ph;
-    if (kz2 >= 0.0) ph = -(sqrt(kz2) - tb.kref[k]) * s;
-    else { mag = exp(-sqrt(-kz2) * s); ph = tb.kref[k] * s; }
+    if (kz2 >= 0.0) ph = -(sqrt(kz2) - tb.kref[k]) * sh;
+    else { mag = exp(-sqrt(-kz2) * sh); ph = tb.kref[k] * sh; }
     double sn, cs;
     sincos(ph, &sn, &cs);
-    const C E = C{(Rl)(mag * cs), (Rl)(mag * sn)};
-    if (mode == RS_1) {          // v = L(E_kw), a1 = L(k1), u = v + h/2 a1
-      const C vv = cmul(ekw[i], E), aa = cmul(na[i], E);
-      v[i] = vv;
-      a1[i] = aa;
-      u[i] = cadd(vv, cscale(aa, h2));
-    } else if (mode == RS_2) {   // u = v + h/2 a2, ts = a1 + 2 a2, el = v + h/2 a1 + h/2 a2
-      const C a2 = na[i], vv = v[i], aa = a1[i];
-      u[i] = cadd(vv, cscale(a2, h2));
-      ts[i] = cadd(aa, cscale(a2, (Rl)2));
-      el[i] = cadd(cadd(vv, cscale(aa, h2)), cscale(a2, h2));
-    } else if (mode == RS_3) {   // u = L(v + h a3), ts += 2 a3
-      const C a3 = na[i];
-      u[i] = cmul(cadd(v[i], cscale(a3, hR)), E);
-      ts[i] = cadd(ts[i], cscale(a3, (Rl)2));
-    } else {                     // E4 = L(v + h/6 ts) + h/6 a4; E_low = L(el)
-      const C E4 = cadd(cmul(cadd(v[i], cscale(ts[i], h6)), E), cscale(na[i], h6));
-      const C El = cmul(el[i], E);
-      e4[i] = E4;
+    const C Ef = C{(Rl)(mag * cs), (Rl)(mag * sn)};
+    const C a = s[idx(w, n)];                    // this stage's N in (kx, ky, omega)
+    C u;
+    if (mode == RS_1) {
+      const C vv = cmul(ekw[gi], Ef), aa = cmul(a, Ef);
+      v[gi] = vv;
+      a1[gi] = aa;
+      u = cadd(vv, cscale(aa, h2));
+    } else if (mode == RS_2) {
+      const C vv = v[gi], aa = a1[gi];
+      u = cadd(vv, cscale(a, h2));
+      ts[gi] = cadd(aa, cscale(a, (Rl)2));
+      el[gi] = cadd(cadd(vv, cscale(aa, h2)), cscale(a, h2));
+    } else if (mode == RS_3) {
+      u = cmul(cadd(v[gi], cscale(a, hR)), Ef);
+      ts[gi] = cadd(ts[gi], cscale(a, (Rl)2));
+    } else {
+      const C E4 = cadd(cmul(cadd(v[gi], cscale(ts[gi], h6)), Ef), cscale(a, h6));
+      const C El = cmul(el[gi], Ef);
       const double dx = (double)E4.x - El.x, dy = (double)E4.y - El.y;
       const double d = sqrt(dx * dx + dy * dy), m = sqrt((double)E4.x * E4.x + (double)E4.y * E4.y);
       mdiff = (d > mdiff || d != d) ? d : mdiff;
       mnorm = (m > mnorm || m != m) ? m : mnorm;
+      u = E4;
     }
+    s[idx(w, n)] = u;
   }
   if (mode == RS_4) {
     mdiff = warp_max<32>(mdiff);
     mnorm = warp_max<32>(mnorm);
     if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(&red[0], mdiff); atomic_max_nonneg(&red[1], mnorm); }
   }
+  __syncthreads();
+  stockham<N, kW, NTHR, +1, 1, C>(s, tw, tid, idx, sync);
+  store_tile<C, N, NTHR>(s, reinterpret_cast<C*>(out), base, stride, tid);
+}
+
+template <typename Rl, int N> static size_t rf_ypass_smem() {
+  return sizeof(typename CT<Rl>::T) * (size_t)(N + N * kW);
 }
 
 template <typename Rl>
@@ -3665,8 +3982,23 @@ extern "C" int uppe_rf_plan_destroy(uppe_rf_plan* p) {
   return 0;
 }
 
+template <typename Rl, int N> static cudaError_t rf_ypass_attr() {
+  return cudaFuncSetAttribute(k_rf_ypass<Rl, N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)rf_ypass_smem<Rl, N>());
+}
+
 template <typename Rl> static int rf_set_attrs(int Nx, int Ny, int Nt) {
   cudaError_t e = cudaSuccess;
+  switch (Ny) {
+    case 16: e = rf_ypass_attr<Rl, 16>(); break;
+    case 32: e = rf_ypass_attr<Rl, 32>(); break;
+    case 64: e = rf_ypass_attr<Rl, 64>(); break;
+    case 128: e = rf_ypass_attr<Rl, 128>(); break;
+    case 256: e = rf_ypass_attr<Rl, 256>(); break;
+    case 512: e = rf_ypass_attr<Rl, 512>(); break;
+    default: return UPPE_ERR_SIZE;
+  }
+  UPPE_CK(e);
   for (int N : {Nx, Ny}) {
     switch (N) {
       case 16: e = set_space_attr<Rl, 16>(); break;
@@ -3750,6 +4082,13 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
     }
     RF_TRY(rf_alloc(p, &ptr, lx.size(), lx.data())); p->tb.lut.x = ptr;
     RF_TRY(rf_alloc(p, &ptr, lw.size(), lw.data())); p->tb.lut.w = ptr;
+    {
+      std::vector<double> sl(n - 1);
+      if (p->dbl) lut_slopes<double>(d->lut_log10I, d->lut_W, n, sl.data());
+      else lut_slopes<float>(d->lut_log10I, d->lut_W, n, sl.data());
+      RF_TRY(rf_alloc(p, &ptr, sl.size() * sizeof(double), sl.data()));
+      p->tb.lut.slope = static_cast<const double*>(ptr);
+    }
     p->tb.lut.n = n;
     const double x0 = p->dbl ? d->lut_log10I[0] : (double)(float)d->lut_log10I[0];
     const double x1 = p->dbl ? d->lut_log10I[n - 1] : (double)(float)d->lut_log10I[n - 1];
@@ -3768,6 +4107,7 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
   RfConst& c = p->rc;
   c.I_coef = d->I_coef; c.aval = d->aval_coef; c.chi3e = d->chi3e; c.chi5e = d->chi5e;
   c.rr = (double)(float)d->rate_rec; c.dt = (double)(float)d->dt; c.rho_nt = (double)(float)d->rho_nt;
+  c.inv_rho_nt = 1.0 / c.rho_nt;
   c.Ui = (double)(float)d->Ui;
   const double e = (double)(float)d->e_charge, me = (double)(float)d->m_e, tc = (double)(float)d->tau_c;
   c.e2m = e * e / me;
@@ -3797,8 +4137,8 @@ extern "C" int uppe_rf_plan_create(const uppe_rf_desc* d, uppe_rf_plan** out) {
     c.fR = d->raman_fR;
     p->raman = true;
   }
-  void** spec[8] = {&p->b.ekw, &p->b.v, &p->b.a1, &p->b.u, &p->b.ts, &p->b.el, &p->b.na, &p->b.e4};
-  for (int i = 0; i < 8; ++i) RF_TRY(rf_alloc(p, spec[i], p->csz * p->nspec));
+  void** spec[5] = {&p->b.ekw, &p->b.v, &p->b.a1, &p->b.ts, &p->b.el};
+  for (int i = 0; i < 5; ++i) RF_TRY(rf_alloc(p, spec[i], p->csz * p->nspec));
   RF_TRY(rf_alloc(p, &p->tmp[0], p->csz * p->nspec));
   RF_TRY(rf_alloc(p, &p->tmp[1], p->csz * p->nspec));
   RF_TRY(rf_alloc(p, &p->state[0], p->rsz * p->nreal));
@@ -3842,45 +4182,50 @@ static int rf_line(uppe_rf_plan* p, int mode, const void* in, void* out, double 
   }
 }
 
-// N(u) of solver_3d.py:120-141: u (kx, ky, omega) -> out
-template <typename Rl>
-static int rf_N(uppe_rf_plan* p, const void* u, void* out, cudaStream_t s) {
-  uppe3d_plan* q = p->xy;
-  int rc = 0;
-  rc |= adj_plain_y<Rl>(q, YPLAIN_INV, u, p->tmp[0], 1.0, s);
-  rc |= launch_space<Rl>(q, XINV, p->tmp[0], p->tmp[1], s);
-  rc |= rf_line<Rl>(p, RF_NL, p->tmp[1], p->tmp[0], 1.0 / ((double)p->d.Nx * p->d.Ny), 0.0, s);
-  rc |= launch_space<Rl>(q, XFWD, p->tmp[0], p->tmp[1], s);
-  rc |= adj_plain_y<Rl>(q, YPLAIN_FWD, p->tmp[1], out, 1.0, s);
-  return rc;
+// one stage: the stage input of this evaluation (already transformed back along y,
+// in tmp[0]) -> inverse x pass -> nonlinear response per t-line (solver_3d.py:120-141)
+// -> forward x pass -> y pass with the stage algebra, which leaves the next stage
+// input (transformed back along y) in tmp[0]
+template <typename Rl, int N>
+static int rf_ypass_n(uppe_rf_plan* p, int mode, double h, cudaStream_t s) {
+  const unsigned nb = (unsigned)((long long)p->d.Nx * (p->Nw / kW));
+  k_rf_ypass<Rl, N><<<nb, SpaceCfg<N>::NTHR, rf_ypass_smem<Rl, N>(), s>>>(
+      mode, p->tb, p->b, p->Nw, p->d.Nt / 2 + 1, p->tmp[1], p->tmp[0], p->xy->tb.twy, h, p->red);
+  UPPE_CK(cudaGetLastError());
+  return 0;
 }
 
 template <typename Rl>
 static int rf_stage(uppe_rf_plan* p, int mode, double h, cudaStream_t s) {
-  k_rf_stage<Rl><<<148 * 8, 256, 0, s>>>(mode, p->tb, p->b, p->d.Nt, p->Nw, p->nspec, h, p->red);
-  UPPE_CK(cudaGetLastError());
-  return 0;
+  uppe3d_plan* q = p->xy;
+  int rc = 0;
+  rc |= launch_space<Rl>(q, XINV, p->tmp[0], p->tmp[1], s);
+  rc |= rf_line<Rl>(p, RF_NL, p->tmp[1], p->tmp[0], 1.0 / ((double)p->d.Nx * p->d.Ny), 0.0, s);
+  rc |= launch_space<Rl>(q, XFWD, p->tmp[0], p->tmp[1], s);
+  if (rc) return rc;
+  switch (p->d.Ny) {
+#define UPPE_RY(n) case n: return rf_ypass_n<Rl, n>(p, mode, h, s);
+    UPPE_RY(16) UPPE_RY(32) UPPE_RY(64) UPPE_RY(128) UPPE_RY(256) UPPE_RY(512)
+#undef UPPE_RY
+    default: return UPPE_ERR_SIZE;
+  }
 }
 
 template <typename Rl>
 static int rf_attempt(uppe_rf_plan* p, double h, double* err, cudaStream_t s) {
   uppe3d_plan* q = p->xy;
   int rc = 0;
-  // E_kw = fft2(rfft(E_t))
+  // E_kw = fft2(rfft(E_t)); the first stage's N(E_kw) starts from its inverse y transform
   rc |= rf_line<Rl>(p, RF_FROM_T, p->state[p->cur], p->tmp[0], 1.0, 0.0, s);
   rc |= launch_space<Rl>(q, XFWD, p->tmp[0], p->tmp[1], s);
   rc |= adj_plain_y<Rl>(q, YPLAIN_FWD, p->tmp[1], p->b.ekw, 1.0, s);
-  rc |= rf_N<Rl>(p, p->b.ekw, p->b.na, s);                         // k1
-  rc |= rf_stage<Rl>(p, RS_1, h, s);
-  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha2
-  rc |= rf_stage<Rl>(p, RS_2, h, s);
-  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha3
-  rc |= rf_stage<Rl>(p, RS_3, h, s);
-  rc |= rf_N<Rl>(p, p->b.u, p->b.na, s);                           // alpha4'
+  rc |= adj_plain_y<Rl>(q, YPLAIN_INV, p->b.ekw, p->tmp[0], 1.0, s);
+  rc |= rf_stage<Rl>(p, RS_1, h, s);                    // k1 -> u2
+  rc |= rf_stage<Rl>(p, RS_2, h, s);                    // alpha2 -> u3
+  rc |= rf_stage<Rl>(p, RS_3, h, s);                    // alpha3 -> u4
   UPPE_CK(cudaMemsetAsync(p->red, 0, 2 * sizeof(unsigned long long), s));
-  rc |= rf_stage<Rl>(p, RS_4, h, s);
+  rc |= rf_stage<Rl>(p, RS_4, h, s);                    // alpha4' -> E4, error
   // candidate: irfft(ifft2(E4) * filter) * exp(-damp h)
-  rc |= adj_plain_y<Rl>(q, YPLAIN_INV, p->b.e4, p->tmp[0], 1.0, s);
   rc |= launch_space<Rl>(q, XINV, p->tmp[0], p->tmp[1], s);
   rc |= rf_line<Rl>(p, RF_OUT, p->tmp[1], p->state[p->cur ^ 1], 1.0 / ((double)p->d.Nx * p->d.Ny), h, s);
   UPPE_CK(cudaMemcpyAsync(p->red_host, p->red, 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, s));
@@ -3916,6 +4261,7 @@ extern "C" int uppe_rf_set_field(uppe_rf_plan* p, const void* E0, double* E_scal
 }
 
 extern "C" int uppe_rf_attempt(uppe_rf_plan* p, double h, double* err, cudaStream_t s) {
+  NvtxRange nvtx_range("uppe_rf_attempt");
   if (!p || !err || !(h > 0.0)) return UPPE_ERR_ARG;
   return p->dbl ? rf_attempt<double>(p, h, err, s) : rf_attempt<float>(p, h, err, s);
 }

@@ -118,6 +118,34 @@ class ERK43IP_UPPE_3D_Optimized:
                    'uppe3d_get_result')
         return r
 
+    def save_state(self, stream=None):
+        """Continuation point of the adaptive run between two attempts: a dict with
+        the loop state (z, h, counters, status, A_scale, ...) and a device copy of the
+        accepted normalised state.  load_state + resume continue the run bit for bit."""
+        st = _lib.State3D()
+        buf = torch.empty((self.Nx, self.Ny, self.Nt), dtype=self.complex_dtype, device=self.device)
+        _lib.check(self._lib.uppe3d_save_state(self._plan, ctypes.c_void_p(buf.data_ptr()), ctypes.byref(st),
+                                               _lib.stream_ptr(stream)), 'uppe3d_save_state')
+        return {'state': {k: getattr(st, k) for k, _ in _lib.State3D._fields_}, 'field': buf}
+
+    def load_state(self, saved, stream=None):
+        st = _lib.State3D(**saved['state'])
+        buf = saved['field'].to(device=self.device, dtype=self.complex_dtype).contiguous()
+        _lib.check(self._lib.uppe3d_load_state(self._plan, ctypes.c_void_p(buf.data_ptr()), ctypes.byref(st),
+                                               _lib.stream_ptr(stream)), 'uppe3d_load_state')
+        self.A_scale = st.A_scale
+
+    def resume(self, return_gpu=False, stream=None):
+        """Continue the adaptive run from the current state to its L; returns what
+        propagate returns."""
+        r = _lib.Result3D()
+        _lib.check(self._lib.uppe3d_resume(self._plan, ctypes.byref(r), _lib.stream_ptr(stream)), 'uppe3d_resume')
+        self.last_result = r
+        A_w = self.spectrum(stream=stream)
+        if return_gpu:
+            return r.z, self.freq_axis_hz, A_w
+        return r.z, self.freq_axis_hz, A_w.cpu().numpy()
+
     def spectrum(self, out=None, stream=None):
         """fftshift_t(fft_t(A * A_scale)) of the current state, on the device."""
         if out is None:

@@ -227,3 +227,35 @@ def test_beam_diagnostics_vs_oracle(precision, tol):
               'freq_abs_Hz'):
         assert rel_l2(d[k], o[k]) < tol, k
     assert d['it_peak'] == o['it_peak']
+
+
+@pytest.mark.parametrize('precision', ['single', 'double'])
+def test_state_continuation_is_bit_exact(precision):
+    """save_state after a few attempts, load_state into a new plan, resume: the same
+    attempts, step sizes, field and diagnostics as the uninterrupted run."""
+    import torch
+    from project_b200 import _lib
+    from project_b200.media import Argon
+    from project_b200.solver3d import ERK43IP_UPPE_3D_Optimized
+    x, t, lam, A0, osol, lut = _oracle_case(N=32, Nt=64, W0=3e9, I_peak=5e16)
+    mk = lambda: ERK43IP_UPPE_3D_Optimized(x, x, t, Argon(lam, 1.0, precision, True, lut=lut), precision=precision)
+    L, tol = 0.02, 1e-5
+    s1 = mk()
+    z, _, Aref = s1.propagate(A0, L, tol=tol, return_gpu=True)
+    r1 = s1.last_result
+    s2 = mk()
+    s2.set_field(A0)
+    st = _lib.stream_ptr()
+    _lib.check(s2._lib.uppe3d_begin(s2._plan, L, tol, 1e-2, 1e-9, 0, st), 'uppe3d_begin')
+    _lib.check(s2._lib.uppe3d_run_steps(s2._plan, 5, st), 'uppe3d_run_steps')
+    saved = s2.save_state()
+    assert 0.0 < saved['state']['z'] < L and saved['state']['done'] == 0
+    assert saved['state']['attempts'] == 5
+    s3 = mk()
+    s3.load_state(saved)
+    z3, _, A3 = s3.resume(return_gpu=True)
+    r3 = s3.last_result
+    assert z3 == z and r3.attempts == r1.attempts and r3.accepted == r1.accepted and r3.status == r1.status
+    assert r3.h == r1.h
+    assert torch.equal(A3, Aref)
+    assert s3.diagnostics()['peak_ionization'] == s1.diagnostics()['peak_ionization']
