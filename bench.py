@@ -801,8 +801,8 @@ def plan_tuning(sol):
     ms = (ctypes.c_float * _lib.UPPE3D_TUNE_SLOTS)()
     _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
     names = ['tma16 2/SM', 'tma16 1/SM', 'tma16 late 3/SM', 'tma16 late 2/SM', 'tma8 4/SM', 'tma8 late 6/SM',
-             'reg4step 2/SM', 'reg4step late 3/SM', 'reg4step tma 2/SM']
-    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step', 3: 'reg4step tma'}[cfg[0]]
+             'reg4step 2/SM', 'reg4step late 3/SM', 'reg4step tma ring 1/SM']
+    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step', 3: 'reg4step tma ring'}[cfg[0]]
     y = kind if not cfg[0] else f"{kind}{' late' if cfg[2] else ''} {cfg[1]}/SM"
     return {'y_pass': y, 't_lines_per_block': cfg[4], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[5]],
             'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:9]) if v > 0},

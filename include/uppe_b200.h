@@ -425,11 +425,11 @@ int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, do
  * per SM, or where they are used with 3 or 2) or of 8 columns (early with 4,
  * late with 6 CTAs per SM) -- complex64 plans with 64 <= Ny <= 256 -- then, for
  * Ny = 256, on the register four-step kernel (operands loaded with the tile, 2
- * CTAs per SM, or where used, 3) and on the register four-step kernel fed by
- * TMA tiles (persistent, 2 CTAs per SM), and 8 or 4 t-lines per block of the
+ * CTAs per SM, or where used, 3) and on the register four-step kernel with
+ * every operand tile on a TMA ring (persistent, 1 CTA per SM), and 8 or 4 t-lines per block of the
  * warp t-line kernel.  All candidates compute identical bits (the plain tile
  * kernel, which rounds differently, serves the other shapes).  cfg6 = {y kernel
- * (1 TMA-fed, 2 register four-step, 3 register four-step on TMA tiles, 0 plain
+ * (1 TMA-fed, 2 register four-step, 3 register four-step on a TMA ring, 0 plain
  * tile), CTAs per SM, late operand loads, omega columns per tile, t-lines per
  * block, 1 timed / 2 from the process cache / 0 defaults (UPPE_TUNE=0)}; ms (may
  * be NULL, UPPE3D_TUNE_SLOTS floats): per-attempt time of the y passes for the
@@ -438,7 +438,7 @@ int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, do
 #define UPPE3D_TUNE_SLOTS 11
 int uppe3d_tuning(const uppe3d_plan* plan, int* cfg6, float* ms);
 /* Force a launch configuration (y_tma 1 TMA-fed, 2 register four-step, 3
- * register four-step on TMA tiles -- 2 and 3: Ny = 256 complex64 only, 3 without
+ * register four-step on a TMA ring -- 2 and 3: Ny = 256 complex64 only, 3 without
  * late loads --, 0 the plain tile kernel; y_ctas 1..6, y_kw 16 or 8, t_wpb 4 or
  * 8) and re-capture the attempt graphs; for comparing the candidates. */
 int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb);

@@ -1162,27 +1162,43 @@ static constexpr size_t yrq_smem() {
 }
 
 // ---------------------------------------------------------------------------
-// The same y passes (complex64, Ny = 256) on persistent CTAs, two per SM: the
-// tile arrives one tile ahead by cp.async.bulk.tensor into one of two shared
-// buffers, as in k_ypass_tma, so the tile's HBM stream costs no registers and
-// overlaps the transforms; each thread then takes rows j + 16 i of column w into
-// registers and runs the register four-step FFT of k_ypass_rq, with the landed
-// buffer doubling as the transpose buffer.  Stage operands are loaded into
-// registers at the start of each tile, before its wait.  Same arithmetic element
-// by element as k_ypass_rq (hence as k_ypass_tma).
+// The same y passes (complex64, Ny = 256) on persistent CTAs, one per SM, with
+// every HBM operand of a tile on a TMA ring: the pass input tile and the stage
+// operand tiles (A, k1, term sum, alpha4', fft_x(Z): the ones the MODE reads,
+// 256 ky rows x kW omega columns each, by cp.async.bulk.tensor) and the FP64
+// k_perp^2 row of the tile's kx (by cp.async.bulk) land on one mbarrier per ring
+// slot, STAGES - 1 tiles ahead of the tile being transformed.  The SM therefore
+// always has the next tiles' loads in flight while it runs the register
+// four-step FFTs and the stage algebra of the current one, and holds no
+// operand in registers across a wait.  Ring: two slots of three tiles (YMID2,
+// YMID3: 2 x 96 KB) or three slots of two tiles (the other passes).  The input
+// slot doubles as the transpose buffer once its tile is in registers.  Element
+// by element the same arithmetic as k_ypass_rq, hence the same bits.
 // ---------------------------------------------------------------------------
+template <int MODE> struct YRing {
+  static constexpr int NOP = (MODE == YMID2 || MODE == YMID3) ? 3 : 2;   // tiles per slot
+  static constexpr int STAGES = NOP == 3 ? 2 : 3;
+  static constexpr bool Q = MODE != YMID4 && MODE != YFWD5;               // needs k_perp^2
+  static constexpr int TILE = 256 * kW;                                   // float2 per tile
+  static constexpr size_t bytes() {
+    return sizeof(float2) * (size_t)(STAGES * NOP * TILE + 256) + sizeof(double) * 256 * STAGES +
+           sizeof(unsigned long long) * STAGES;
+  }
+};
+
 template <int MODE>
-__global__ void __launch_bounds__(kW * 16, 2)
-k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
+__global__ void __launch_bounds__(kW * 16, 1)
+k_ypass_ring(SpaceArgs a, const __grid_constant__ YMaps maps) {
   using C = float2;
   using Rl = float;
-  constexpr int R = 16, N = R * R, NTHR = kW * R, TILE = N * kW;
+  using RG = YRing<MODE>;
+  constexpr int R = 16, N = R * R, NTHR = kW * R, TILE = RG::TILE, NOP = RG::NOP, STAGES = RG::STAGES;
   constexpr bool TWO = MODE == YMID1;          // YMID1 also transforms fft_x(Z) = tmp[2]
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  C* buf[2] = {reinterpret_cast<C*>(smem_raw), reinterpret_cast<C*>(smem_raw) + TILE};
-  C* tw = buf[1] + TILE;
-  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(tw + N);   // [2]
-  double* qrow = reinterpret_cast<double*>(mbar + 2);   // k_perp^2 of the tile's kx row
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  C* ring = reinterpret_cast<C*>(smem_raw);                     // [STAGES][NOP][TILE]
+  C* tw = ring + STAGES * NOP * TILE;
+  double* qbuf = reinterpret_cast<double*>(tw + N);             // [STAGES][256]
+  unsigned long long* mbar = reinterpret_cast<unsigned long long*>(qbuf + STAGES * 256);
   State3D* st = a.st;
   if (st->done) return;
   if (MODE == YMID1R && st->fresh) return;
@@ -1191,22 +1207,39 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
   const int Nt = a.g.Nt;
   const int ntw = Nt / kW;
   const int total = a.g.Nx * ntw;
-  const CUtensorMap* map = MODE == YMID1R ? &maps.acur : &maps.in;
+  // slot order per MODE: YMID1 {in, z2}, YMID1R {A, k1}, YMID2/3 {in, A, tsum},
+  // YMID4 {in, tsum}, YFWD5 {in, a4p}
+  const CUtensorMap* m0 = MODE == YMID1R ? &maps.acur : &maps.in;
+  const CUtensorMap* m1 = MODE == YMID1 ? &maps.z2 : MODE == YMID1R ? &maps.k1
+                        : (MODE == YMID2 || MODE == YMID3) ? &maps.acur : MODE == YMID4 ? &maps.tsum : &maps.a4p;
+  const CUtensorMap* m2 = &maps.tsum;
+  auto slot = [&](int b, int op) { return ring + (b * NOP + op) * TILE; };
   auto issue = [&](int tile, int b) {
     const int o = tile / ntw, w0 = (tile % ntw) * kW;
     const unsigned bar = smem_u32(&mbar[b]);
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
-                 :: "r"(bar), "r"((unsigned)(TILE * sizeof(C))) : "memory");
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
-        :: "r"(smem_u32(buf[b])), "l"(reinterpret_cast<unsigned long long>(map)), "r"(w0), "r"(0), "r"(o),
-           "r"(bar)
-        : "memory");
+    const unsigned bytes = (unsigned)(NOP * TILE * sizeof(C)) + (RG::Q ? 256u * 8u : 0u);
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" :: "r"(bar), "r"(bytes) : "memory");
+#pragma unroll
+    for (int op = 0; op < NOP; ++op) {
+      const CUtensorMap* m = op == 0 ? m0 : op == 1 ? m1 : m2;
+      asm volatile(
+          "cp.async.bulk.tensor.3d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4}], [%5];"
+          :: "r"(smem_u32(slot(b, op))), "l"(reinterpret_cast<unsigned long long>(m)), "r"(w0), "r"(0), "r"(o),
+             "r"(bar)
+          : "memory");
+    }
+    if constexpr (RG::Q) {
+      // the 2 KB k_perp^2 row of this kx (16-byte aligned: row starts at o * 2048 bytes)
+      asm volatile(
+          "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+          :: "r"(smem_u32(qbuf + b * 256)),
+             "l"((unsigned long long)__cvta_generic_to_global(a.tb.q + (long long)o * N)), "r"(256u * 8u), "r"(bar)
+          : "memory");
+    }
   };
   if (tid == 0) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[0])) : "memory");
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[1])) : "memory");
+    for (int b = 0; b < STAGES; ++b)
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&mbar[b])) : "memory");
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
   {
@@ -1214,63 +1247,68 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
     for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
   }
   __syncthreads();
-  if (tid == 0 && (int)blockIdx.x < total) issue(blockIdx.x, 0);
+  if (tid == 0) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    for (int s = 0; s < STAGES - 1; ++s) {
+      const int t = (int)blockIdx.x + s * (int)gridDim.x;
+      if (t < total) issue(t, s);
+    }
+  }
   C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
   C* __restrict__ k1b = reinterpret_cast<C*>(a.b.k1);
   C* __restrict__ tsum = reinterpret_cast<C*>(a.b.tsum);
   C* __restrict__ a4p = reinterpret_cast<C*>(a.b.a4p);
   C* __restrict__ out = reinterpret_cast<C*>(a.out);
   C* __restrict__ su = reinterpret_cast<C*>(a.save_u);
-  const C* __restrict__ z2 = reinterpret_cast<const C*>(a.b.tmp[2]);
   const double h = st->h;
   const double h2 = 0.5 * h;
   const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
   double red = 0.0;
   int k = 0;
   for (int tile = blockIdx.x; tile < total; tile += gridDim.x, ++k) {
-    const int b = k & 1;
-    const bool next = tile + (int)gridDim.x < total;
-    if (tid == 0 && next) issue(tile + gridDim.x, b ^ 1);
-    const int o = tile / ntw, w0 = (tile % ntw) * kW;
-    const long long base = (long long)o * N * Nt + w0 + w;
-    auto gidx = [&](int i) { return base + (long long)(j + R * i) * Nt; };
-    C opA[R], opB[R], v2[TWO ? R : 1];
-#pragma unroll
-    for (int i = 0; i < R; ++i) {
-      const long long gi = gidx(i);
-      if constexpr (MODE == YMID2 || MODE == YMID3) { opA[i] = __ldg(acur + gi); opB[i] = __ldg(tsum + gi); }
-      else if constexpr (MODE == YMID4) opB[i] = __ldg(tsum + gi);
-      else if constexpr (MODE == YMID1R) opB[i] = __ldg(k1b + gi);
-      else if constexpr (MODE == YFWD5) opA[i] = __ldg(a4p + gi);
-      if constexpr (TWO) v2[i] = __ldg(z2 + gi);
+    const int b = k % STAGES;
+    if (tid == 0) {   // refill the slot that the previous tile released
+      const int t = tile + (STAGES - 1) * (int)gridDim.x;
+      if (t < total) issue(t, (k + STAGES - 1) % STAGES);
     }
-    if (MODE != YMID4 && MODE != YFWD5) qrow[tid] = __ldg(a.tb.q + (long long)o * N + tid);   // NTHR == N
-    const bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
+    const bool ok = mbar_wait(smem_u32(&mbar[b]), (unsigned)((k / STAGES) & 1));
     if (!__syncthreads_and(ok)) {     // a tile never arrived: stop the run with a status
       if (tid == 0) {
         atomicOr(&st->status, UPPE_STATUS_DEVICE_WAIT);
         st->done = 1;
-        // every copy this CTA started must have landed before it exits: wait again,
-        // bounded, on each barrier with a copy in flight
-        mbar_wait(smem_u32(&mbar[b]), (unsigned)((k >> 1) & 1));
-        if (next) mbar_wait(smem_u32(&mbar[b ^ 1]), (unsigned)(((k + 1) >> 1) & 1));
+        // every copy this CTA started must have landed before it exits: wait
+        // again, bounded, on each slot with a copy in flight
+        for (int s = 0; s < STAGES; ++s)
+          if (tile + s * (int)gridDim.x < total)
+            mbar_wait(smem_u32(&mbar[(k + s) % STAGES]), (unsigned)(((k + s) / STAGES) & 1));
       }
       return;
     }
-    C* s = buf[b];
-    C v[R];
+    const int o = tile / ntw, w0 = (tile % ntw) * kW;
+    const long long base = (long long)o * N * Nt + w0 + w;
+    auto gidx = [&](int i) { return base + (long long)(j + R * i) * Nt; };
+    auto sidx = [&](int i) { return (j + R * i) * kW + w; };
+    C* s0 = slot(b, 0);
+    const C* s1 = slot(b, 1);
+    const C* s2 = slot(b, NOP - 1);
+    const double* qrow = qbuf + b * 256;
+    C v[R], v2[TWO ? R : 1];
 #pragma unroll
-    for (int i = 0; i < R; ++i) v[i] = s[(j + R * i) * kW + w];
-    __syncthreads();                  // the tile is in registers: its buffer is the transpose buffer
-    if constexpr (MODE != YMID1R) fft_sq<R, -1>(v, s, tw, j, w);
-    if constexpr (TWO) fft_sq<R, -1>(v2, s, tw, j, w);
+    for (int i = 0; i < R; ++i) v[i] = s0[sidx(i)];
+    if constexpr (TWO) {
+#pragma unroll
+      for (int i = 0; i < R; ++i) v2[i] = s1[sidx(i)];
+    }
+    __syncthreads();                  // the input tile is in registers: slot 0 is the transpose buffer
+    if constexpr (MODE != YMID1R) fft_sq<R, -1>(v, s0, tw, j, w);
+    if constexpr (TWO) fft_sq<R, -1>(v2, s0, tw, j, w);
     const OmegaCol oc(a.tb, w0 + w);
 #pragma unroll
     for (int i = 0; i < R; ++i) {
       const int n = j + R * i;
       const long long gi = gidx(i);
       if constexpr (MODE == YFWD5) {
-        const C a5 = v[i], a4 = opA[i];
+        const C a5 = v[i], a4 = s1[sidx(i)];
         const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
         const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
         red = (d > red || d != d) ? d : red;
@@ -1278,7 +1316,7 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
       }
       if constexpr (MODE == YMID4) {
         const C a4 = v[i];
-        const C A4 = cadd(opB[i], cscale(a4, h6R));
+        const C A4 = cadd(s1[sidx(i)], cscale(a4, h6R));
         a4p[gi] = a4;
         const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
         red = (m > red || m != m) ? m : red;
@@ -1287,9 +1325,9 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
       }
       const C Ef = IPFactor<Rl>::get(a.tb, oc, w0 + w, qrow[n], h2);
       C u;
-      if constexpr (MODE == YMID1R) {   // v = A, opB = k1
+      if constexpr (MODE == YMID1R) {   // v = A, slot 1 = k1
         const C vv = cmul(v[i], Ef);
-        const C a1 = cmul(opB[i], Ef);
+        const C a1 = cmul(s1[sidx(i)], Ef);
         tsum[gi] = a1;
         u = cadd(vv, cscale(a1, h2R));
       } else if constexpr (MODE == YMID1) {   // v = k1 = N(A), v2 = A
@@ -1300,15 +1338,15 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
         const C a1 = cmul(k1, Ef);
         tsum[gi] = a1;
         u = cadd(vv, cscale(a1, h2R));
-      } else if constexpr (MODE == YMID2) {
+      } else if constexpr (MODE == YMID2) {   // slot 1 = A, slot 2 = term sum
         const C a2 = v[i];
-        const C vv = cmul(opA[i], Ef);
-        tsum[gi] = cadd(opB[i], cscale(a2, (Rl)2));
+        const C vv = cmul(s1[sidx(i)], Ef);
+        tsum[gi] = cadd(s2[sidx(i)], cscale(a2, (Rl)2));
         u = cadd(vv, cscale(a2, h2R));
       } else {   // YMID3
         const C a3 = v[i];
-        const C vv = cmul(opA[i], Ef);
-        const C ts = cadd(opB[i], cscale(a3, (Rl)2));
+        const C vv = cmul(s1[sidx(i)], Ef);
+        const C ts = cadd(s2[sidx(i)], cscale(a3, (Rl)2));
         tsum[gi] = cmul(cadd(vv, cscale(ts, h6R)), Ef);
         u = cmul(cadd(vv, cscale(a3, hR)), Ef);
       }
@@ -1316,11 +1354,11 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
       if (su) su[gi] = u;
     }
     if constexpr (MODE != YFWD5) {
-      fft_sq<R, +1>(v, s, tw, j, w);
+      fft_sq<R, +1>(v, s0, tw, j, w);
 #pragma unroll
       for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
     }
-    // buffer b is refilled by the copy issued at iteration k + 1: order this
+    // slot b is refilled by the copy issued at iteration k + 1: order this
     // iteration's shared-memory accesses before that async-proxy write
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     __syncthreads();
@@ -1329,10 +1367,6 @@ k_ypass_tq(SpaceArgs a, const __grid_constant__ YMaps maps) {
     red = warp_max<32>(red);
     if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
   }
-}
-
-static constexpr size_t ytq_smem() {
-  return sizeof(float2) * (size_t)(2 * 256 * kW + 256) + 2 * sizeof(unsigned long long) + 256 * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -1353,37 +1387,49 @@ template <int E> struct WarpFFT {
   __device__ __forceinline__ static int out_index(int lane, int k) {
     return (lane / G) + E * (k + E * (lane % G));
   }
-  template <int DIR, typename C>
-  __device__ __forceinline__ static void pair_fwd(C (&v)[E], const C* tw, int lane) {
-    if constexpr (G == 2) {
-      const bool r0 = (lane & 1) == 0;
-#pragma unroll
-      for (int k = 0; k < E; ++k) {
-        C t = tw[k * 32 + E];                          // W_32^k = W_NT^(k E)
-        if (DIR > 0) t.y = -t.y;
-        const C own = v[k];
-        C oth;
-        oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
-        oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
-        v[k] = r0 ? cadd(own, cmul(t, oth)) : csub(oth, cmul(t, own));
-      }
+  // radix-2 step with the partner lane L^1 (E = 16): the factor W_32^k of register
+  // k is a compile-time constant (exact for k = 0 and 8), and the even / odd lane
+  // results are formed as b + s p with s = +-1 (an exact sign, so the same values
+  // as an add and a subtract) instead of both branches and a select per component
+  template <int K, int DIR, typename C>
+  __device__ __forceinline__ static void pair_fwd_k(C (&v)[E], bool r0) {
+    using Rl = decltype(v[0].x);
+    if constexpr (K < E) {
+      const C own = v[K];
+      C oth;
+      oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
+      oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
+      // even lane: own + W oth; odd lane: oth - W own
+      const C m = r0 ? oth : own, b = r0 ? own : oth;
+      const C p = rot<32, K, DIR>(m);
+      const Rl sg = r0 ? (Rl)1 : (Rl)-1;
+      v[K] = C{fma(sg, p.x, b.x), fma(sg, p.y, b.y)};
+      pair_fwd_k<K + 1, DIR>(v, r0);
+    }
+  }
+  template <int K, int DIR, typename C>
+  __device__ __forceinline__ static void pair_bwd_k(C (&v)[E], bool r0) {
+    using Rl = decltype(v[0].x);
+    if constexpr (K < E) {
+      const C own = v[K];
+      C oth;
+      oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
+      oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
+      // even lane: own + oth; odd lane: W (oth - own)
+      const Rl sg = r0 ? (Rl)1 : (Rl)-1;
+      const C d = C{fma(sg, own.x, oth.x), fma(sg, own.y, oth.y)};
+      const C p = rot<32, K, DIR>(d);
+      v[K] = r0 ? d : p;
+      pair_bwd_k<K + 1, DIR>(v, r0);
     }
   }
   template <int DIR, typename C>
-  __device__ __forceinline__ static void pair_bwd(C (&v)[E], const C* tw, int lane) {
-    if constexpr (G == 2) {
-      const bool r0 = (lane & 1) == 0;
-#pragma unroll
-      for (int k = 0; k < E; ++k) {
-        C t = tw[k * 32 + E];
-        if (DIR > 0) t.y = -t.y;
-        const C own = v[k];
-        C oth;
-        oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
-        oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
-        v[k] = r0 ? cadd(own, oth) : cmul(t, csub(oth, own));
-      }
-    }
+  __device__ __forceinline__ static void pair_fwd(C (&v)[E], const C*, int lane) {
+    if constexpr (G == 2) pair_fwd_k<0, DIR>(v, (lane & 1) == 0);
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void pair_bwd(C (&v)[E], const C*, int lane) {
+    if constexpr (G == 2) pair_bwd_k<0, DIR>(v, (lane & 1) == 0);
   }
   template <int DIR, typename C>
   __device__ __forceinline__ static void fwd_like(C (&v)[E], C* S, const C* tw, int lane) {
@@ -1836,7 +1882,7 @@ struct uppe3d_plan {
   int nsm = 148;
   // launch configuration picked per shape by the tuner (uppe3d_tuning): every
   // candidate computes the same bits, only the time differs
-  int y_tma = 1;                  // y passes on k_ypass_tma (1), k_ypass_rq (2), k_ypass_tq (3) or k_space (0)
+  int y_tma = 1;                  // y passes on k_ypass_tma (1), k_ypass_rq (2), k_ypass_ring (3) or k_space (0)
   int y_ctas = 2;                 // k_ypass_tma CTAs per SM (1..6; k_ypass_rq: 2 or 3, fixed by LATE)
   int y_late = 0;                 // the y kernel loads the stage operands where used (1)
   int y_kw = kW;                  // k_ypass_tma omega columns per tile (16 or 8)
@@ -1919,28 +1965,31 @@ static bool use_ytq(const uppe3d_plan* p, int mode, const void* in) {
 }
 
 static void launch_ytq(const uppe3d_plan* p, const SpaceArgs& a, cudaStream_t s) {
-  const dim3 g((unsigned)(2 * p->nsm));
+  const long long total = (long long)p->g.Nx * (p->g.Nt / kW);
+  const dim3 g((unsigned)(total < p->nsm ? total : p->nsm));
   constexpr unsigned T = kW * 16;
-  constexpr size_t sm = ytq_smem();
   const YMaps& mp = p->ymaps;
   switch (a.mode) {
-    case YMID1: k_ypass_tq<YMID1><<<g, T, sm, s>>>(a, mp); break;
-    case YMID1R: k_ypass_tq<YMID1R><<<g, T, sm, s>>>(a, mp); break;
-    case YMID2: k_ypass_tq<YMID2><<<g, T, sm, s>>>(a, mp); break;
-    case YMID3: k_ypass_tq<YMID3><<<g, T, sm, s>>>(a, mp); break;
-    case YMID4: k_ypass_tq<YMID4><<<g, T, sm, s>>>(a, mp); break;
-    default: k_ypass_tq<YFWD5><<<g, T, sm, s>>>(a, mp); break;
+    case YMID1: k_ypass_ring<YMID1><<<g, T, YRing<YMID1>::bytes(), s>>>(a, mp); break;
+    case YMID1R: k_ypass_ring<YMID1R><<<g, T, YRing<YMID1R>::bytes(), s>>>(a, mp); break;
+    case YMID2: k_ypass_ring<YMID2><<<g, T, YRing<YMID2>::bytes(), s>>>(a, mp); break;
+    case YMID3: k_ypass_ring<YMID3><<<g, T, YRing<YMID3>::bytes(), s>>>(a, mp); break;
+    case YMID4: k_ypass_ring<YMID4><<<g, T, YRing<YMID4>::bytes(), s>>>(a, mp); break;
+    default: k_ypass_ring<YFWD5><<<g, T, YRing<YFWD5>::bytes(), s>>>(a, mp); break;
   }
 }
 
+template <int MODE> static cudaError_t set_yring_attr_m() {
+  return cudaFuncSetAttribute(k_ypass_ring<MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              (int)YRing<MODE>::bytes());
+}
 static cudaError_t set_ytq_attr() {
-  const int sm = (int)ytq_smem();
-  cudaError_t e = cudaFuncSetAttribute(k_ypass_tq<YMID1>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID1R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID2>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID3>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YMID4>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(k_ypass_tq<YFWD5>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+  cudaError_t e = set_yring_attr_m<YMID1>();
+  if (e == cudaSuccess) e = set_yring_attr_m<YMID1R>();
+  if (e == cudaSuccess) e = set_yring_attr_m<YMID2>();
+  if (e == cudaSuccess) e = set_yring_attr_m<YMID3>();
+  if (e == cudaSuccess) e = set_yring_attr_m<YMID4>();
+  if (e == cudaSuccess) e = set_yring_attr_m<YFWD5>();
   return e;
 }
 
@@ -2347,7 +2396,7 @@ static int tune(uppe3d_plan* p) {
   // serve Ny = 256
   struct YC { int tma, ctas, late, kw; } yc[9] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
                                                 {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW},
-                                                {3, 2, 0, kW}};
+                                                {3, 1, 0, kW}};
   const int ny = p->ytma ? (yrq_ok(p) ? 9 : 6) : 1;
   if (!p->ytma) yc[0] = YC{0, 2, 0, kW};
   const int tw_n = (p->g.Nt == 512 || (p->g.Nt == 1024 && !p->dbl)) ? 2 : 1;
@@ -2724,8 +2773,8 @@ extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_la
     return UPPE_ERR_ARG;
   p->y_tma = y_tma;
   p->y_late = y_late ? 1 : 0;
-  // k_ypass_rq / k_ypass_tq: CTAs per SM fixed by their launch bounds
-  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_tma == 3 ? 2 : y_ctas;
+  // k_ypass_rq / k_ypass_ring: CTAs per SM fixed by their launch bounds
+  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_tma == 3 ? 1 : y_ctas;
   p->y_kw = y_kw;
   p->t_wpb = t_wpb;
   if (p->g_attempt) { cudaGraphExecDestroy(p->g_attempt); p->g_attempt = nullptr; }
@@ -3789,10 +3838,11 @@ k_rf_line(int mode, RfTables tb, RfConst rc, Geom g, int Nw, const void* in, voi
     mj = fmax(mj, __shfl_xor_sync(0xffffffffu, mj, off));
   }
   const Rl sP = mp > (Rl)0 ? mp : (Rl)1, sJ = mj > (Rl)0 ? mj : (Rl)1;
-  const Rl isP = (Rl)1 / sP, isJ = (Rl)1 / sJ;
+  // divisions, not reciprocals: on weakly ionising lines the current's maximum is
+  // a float32 subnormal whose reciprocal overflows
   for (int t = lane; t < NT; t += 32) {
     const C pj = S[tpad(t)];
-    S[tpad(t)] = C{pj.x * isP, pj.y * isJ};
+    S[tpad(t)] = C{pj.x / sP, pj.y / sJ};
   }
   __syncwarp();
   stockham<NT, 1, TCfg<NT>::FT, -1, 1, C>(S, tw, lane, LineIdx(), WarpSync());    // F(P/sP + i J/sJ)
@@ -3903,8 +3953,9 @@ k_rf_ypass(int mode, RfTables tb, RfBufs b, int Nw, int NR, const void* in, void
     s[idx(w, n)] = u;
   }
   if (mode == RS_4) {
-    mdiff = warp_max<32>(mdiff);
-    mnorm = warp_max<32>(mnorm);
+    // blocks of fewer than 32 threads (Ny = 16) reduce over their own lanes only
+    mdiff = warp_max<(NTHR < 32 ? NTHR : 32)>(mdiff);
+    mnorm = warp_max<(NTHR < 32 ? NTHR : 32)>(mnorm);
     if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(&red[0], mdiff); atomic_max_nonneg(&red[1], mnorm); }
   }
   __syncthreads();
