@@ -801,12 +801,14 @@ def plan_tuning(sol):
     ms = (ctypes.c_float * _lib.UPPE3D_TUNE_SLOTS)()
     _lib.check(sol._lib.uppe3d_tuning(sol._plan, cfg, ms), 'uppe3d_tuning')
     names = ['tma16 2/SM', 'tma16 1/SM', 'tma16 late 3/SM', 'tma16 late 2/SM', 'tma8 4/SM', 'tma8 late 6/SM',
-             'reg4step 2/SM', 'reg4step late 3/SM', 'reg4step tma ring 1/SM']
-    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step', 3: 'reg4step tma ring'}[cfg[0]]
+             'reg4step 2/SM', 'reg4step late 3/SM', 'reg4step tma ring 1/SM', 'reg4step8 4/SM',
+             'reg4step8 late 6/SM']
+    kind = {0: 'plain', 1: f'tma{cfg[3]}', 2: 'reg4step' if cfg[3] == 16 else 'reg4step8',
+            3: 'reg4step tma ring'}[cfg[0]]
     y = kind if not cfg[0] else f"{kind}{' late' if cfg[2] else ''} {cfg[1]}/SM"
     return {'y_pass': y, 't_lines_per_block': cfg[4], 'source': {0: 'defaults', 1: 'timed', 2: 'cache'}[cfg[5]],
-            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:9]) if v > 0},
-            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[9:11]) if v > 0}}
+            'y_candidates_ms': {n: round(float(v), 4) for n, v in zip(names, ms[:11]) if v > 0},
+            't_candidates_ms': {w: round(float(v), 4) for w, v in zip((8, 4), ms[11:13]) if v > 0}}
 
 
 def run_b200(args, rank, world, local_rank):

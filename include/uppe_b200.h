@@ -424,23 +424,25 @@ int uppe3d_transform_t(uppe3d_plan* plan, const void* in, void* out, int dir, do
  * omega columns (stage operands loaded before the tile's wait with 2 or 1 CTAs
  * per SM, or where they are used with 3 or 2) or of 8 columns (early with 4,
  * late with 6 CTAs per SM) -- complex64 plans with 64 <= Ny <= 256 -- then, for
- * Ny = 256, on the register four-step kernel (operands loaded with the tile, 2
- * CTAs per SM, or where used, 3) and on the register four-step kernel with
- * every operand tile on a TMA ring (persistent, 1 CTA per SM), and 8 or 4 t-lines per block of the
- * warp t-line kernel.  All candidates compute identical bits (the plain tile
+ * Ny = 256, on the register four-step kernel (tiles of 16 columns: operands
+ * loaded with the tile, 2 CTAs per SM, or where used, 3), on the register
+ * four-step kernel with every operand tile on a TMA ring (persistent, 1 CTA per
+ * SM) and on the register four-step kernel with tiles of 8 columns (early, 4 CTAs
+ * per SM, or late, 6), and 8 or 4 t-lines per block of the warp t-line kernel.  All candidates compute identical bits (the plain tile
  * kernel, which rounds differently, serves the other shapes).  cfg6 = {y kernel
  * (1 TMA-fed, 2 register four-step, 3 register four-step on a TMA ring, 0 plain
  * tile), CTAs per SM, late operand loads, omega columns per tile, t-lines per
  * block, 1 timed / 2 from the process cache / 0 defaults (UPPE_TUNE=0)}; ms (may
  * be NULL, UPPE3D_TUNE_SLOTS floats): per-attempt time of the y passes for the
- * nine y candidates in that order [0..8] and of the t passes for 8 and 4 lines
- * per block [9..10], in ms (0 when not timed). */
-#define UPPE3D_TUNE_SLOTS 11
+ * eleven y candidates in that order [0..10] and of the t passes for 8 and 4
+ * lines per block [11..12], in ms (0 when not timed). */
+#define UPPE3D_TUNE_SLOTS 13
 int uppe3d_tuning(const uppe3d_plan* plan, int* cfg6, float* ms);
 /* Force a launch configuration (y_tma 1 TMA-fed, 2 register four-step, 3
  * register four-step on a TMA ring -- 2 and 3: Ny = 256 complex64 only, 3 without
- * late loads --, 0 the plain tile kernel; y_ctas 1..6, y_kw 16 or 8, t_wpb 4 or
- * 8) and re-capture the attempt graphs; for comparing the candidates. */
+ * late loads and with 16 columns --, 0 the plain tile kernel; y_ctas 1..6, y_kw
+ * 16 or 8, t_wpb 4 or 8) and re-capture the attempt graphs; for comparing the
+ * candidates. */
 int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb);
 
 /* Kernel launches of one propagate-mode attempt (graph nodes). */

@@ -16,8 +16,8 @@ UPPE_C64, UPPE_C128 = 0, 1
 STATUS_NONFINITE, STATUS_MIN_STEP, STATUS_MAX_ATTEMPTS, STATUS_RETRIED = 1, 2, 4, 64
 # line limits of uppe1d_propagate_noalloc (its static device array)
 UPPE_NOALLOC_MAX_NT_C64, UPPE_NOALLOC_MAX_NT_C128 = 16384, 8192
-# timing slots of uppe3d_tuning: nine y-pass candidates, then two t-pass ones
-UPPE3D_TUNE_SLOTS = 11
+# timing slots of uppe3d_tuning: eleven y-pass candidates, then two t-pass ones
+UPPE3D_TUNE_SLOTS = 13
 
 _P = ctypes.c_void_p
 _D = ctypes.c_double

@@ -462,7 +462,7 @@ k_space(SpaceArgs a) {
 // One FFT = R-point DFT in registers, twiddle, one shared-memory transpose,
 // R-point DFT; the inverse is the same with conjugated roots.
 // ---------------------------------------------------------------------------
-template <int R, int DIR, typename C>
+template <int R, int DIR, typename C, int KW = kW>
 __device__ __forceinline__ void fft_sq(C (&v)[R], C* T, const C* tw, int j, int w) {
   DFT<R, DIR, C>::run(v);
 #pragma unroll
@@ -472,10 +472,10 @@ __device__ __forceinline__ void fft_sq(C (&v)[R], C* T, const C* tw, int j, int 
     v[k] = cmul(v[k], t);
   }
 #pragma unroll
-  for (int k = 0; k < R; ++k) T[(k * R + j) * kW + w] = v[k];
+  for (int k = 0; k < R; ++k) T[(k * R + j) * KW + w] = v[k];
   __syncthreads();
 #pragma unroll
-  for (int k = 0; k < R; ++k) v[k] = T[(j * R + k) * kW + w];
+  for (int k = 0; k < R; ++k) v[k] = T[(j * R + k) * KW + w];
   __syncthreads();
   DFT<R, DIR, C>::run(v);
 }
@@ -1030,25 +1030,25 @@ static size_t ytma_smem(int mode) {
 // (two CTAs per SM); LATE = 1 issues them element by element in the stage loop
 // (three CTAs per SM).  One instantiation per pass.
 // ---------------------------------------------------------------------------
-template <int MODE, int LATE>
-__global__ void __launch_bounds__(kW * 16, LATE ? 3 : 2)
+template <int MODE, int LATE, int KW = kW>
+__global__ void __launch_bounds__(KW * 16, (LATE ? 3 : 2) * (kW / KW))
 k_ypass_rq(SpaceArgs a) {
   using C = float2;
   using Rl = float;
-  constexpr int R = 16, N = R * R, NTHR = kW * R;
+  constexpr int R = 16, N = R * R, NTHR = KW * R;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   C* tw = reinterpret_cast<C*>(smem_raw);
-  C* T = tw + N;                                          // transpose buffer, N * kW
-  double* qrow = reinterpret_cast<double*>(T + N * kW);   // k_perp^2 of the tile's kx row
-  const int tid = threadIdx.x, w = tid % kW, j = tid / kW;
+  C* T = tw + N;                                          // transpose buffer, N * KW
+  double* qrow = reinterpret_cast<double*>(T + N * KW);   // k_perp^2 of the tile's kx row
+  const int tid = threadIdx.x, w = tid % KW, j = tid / KW;
   State3D* st = a.st;
   if (st->done) return;
   if (MODE == YMID1R && st->fresh) return;
   if (MODE == YMID1 && !st->fresh) return;
   const int Nt = a.g.Nt;
-  const int ntile = Nt / kW;
+  const int ntile = Nt / KW;
   const int o = blockIdx.x / ntile;            // kx index
-  const int w0 = (blockIdx.x % ntile) * kW;    // omega offset
+  const int w0 = (blockIdx.x % ntile) * KW;    // omega offset
   const long long base = (long long)o * N * Nt + w0 + w;
   auto gidx = [&](int i) { return base + (long long)(j + R * i) * Nt; };
   C* __restrict__ acur = reinterpret_cast<C*>(a.b.acur);
@@ -1086,8 +1086,8 @@ k_ypass_rq(SpaceArgs a) {
       for (int i = tid; i < N; i += NTHR) qrow[i] = __ldg(a.tb.q + (long long)o * N + i);
   }
   __syncthreads();
-  if constexpr (MODE != YMID1R) fft_sq<R, -1>(v, T, tw, j, w);
-  if constexpr (TWO) fft_sq<R, -1>(v2, T, tw, j, w);
+  if constexpr (MODE != YMID1R) fft_sq<R, -1, C, KW>(v, T, tw, j, w);
+  if constexpr (TWO) fft_sq<R, -1, C, KW>(v2, T, tw, j, w);
   const double h = st->h;
   const double h2 = 0.5 * h;
   const Rl hR = (Rl)h, h2R = (Rl)(h / 2), h6R = (Rl)(h / 6);
@@ -1151,14 +1151,14 @@ k_ypass_rq(SpaceArgs a) {
     if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
   }
   if constexpr (MODE != YFWD5) {
-    fft_sq<R, +1>(v, T, tw, j, w);
+    fft_sq<R, +1, C, KW>(v, T, tw, j, w);
 #pragma unroll
     for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
   }
 }
 
-static constexpr size_t yrq_smem() {
-  return sizeof(float2) * (size_t)(256 + 256 * kW) + 256 * sizeof(double);
+template <int KW = kW> static constexpr size_t yrq_smem() {
+  return sizeof(float2) * (size_t)(256 + 256 * KW) + 256 * sizeof(double);
 }
 
 // ---------------------------------------------------------------------------
@@ -1993,17 +1993,17 @@ static cudaError_t set_ytq_attr() {
   return e;
 }
 
-template <int LATE>
+template <int LATE, int KW>
 static void launch_yrq_l(const SpaceArgs& a, unsigned nblocks, cudaStream_t s) {
-  constexpr unsigned T = kW * 16;
-  constexpr size_t sm = yrq_smem();
+  constexpr unsigned T = KW * 16;
+  constexpr size_t sm = yrq_smem<KW>();
   switch (a.mode) {
-    case YMID1: k_ypass_rq<YMID1, LATE><<<nblocks, T, sm, s>>>(a); break;
-    case YMID1R: k_ypass_rq<YMID1R, LATE><<<nblocks, T, sm, s>>>(a); break;
-    case YMID2: k_ypass_rq<YMID2, LATE><<<nblocks, T, sm, s>>>(a); break;
-    case YMID3: k_ypass_rq<YMID3, LATE><<<nblocks, T, sm, s>>>(a); break;
-    case YMID4: k_ypass_rq<YMID4, LATE><<<nblocks, T, sm, s>>>(a); break;
-    default: k_ypass_rq<YFWD5, LATE><<<nblocks, T, sm, s>>>(a); break;
+    case YMID1: k_ypass_rq<YMID1, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
+    case YMID1R: k_ypass_rq<YMID1R, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
+    case YMID2: k_ypass_rq<YMID2, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
+    case YMID3: k_ypass_rq<YMID3, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
+    case YMID4: k_ypass_rq<YMID4, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
+    default: k_ypass_rq<YFWD5, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
   }
 }
 
@@ -2072,9 +2072,14 @@ static int launch_space(uppe3d_plan* p, int mode, const void* in, void* out, cud
     return 0;
   }
   if (sizeof(Rl) == 4 && use_yrq(p, mode, in)) {
-    const unsigned nb = (unsigned)((long long)p->g.Nx * (p->g.Nt / kW));
-    if (p->y_late) launch_yrq_l<1>(a, nb, s);
-    else launch_yrq_l<0>(a, nb, s);
+    const unsigned nb = (unsigned)((long long)p->g.Nx * (p->g.Nt / p->y_kw));
+    if (p->y_kw == 8) {
+      if (p->y_late) launch_yrq_l<1, 8>(a, nb, s);
+      else launch_yrq_l<0, 8>(a, nb, s);
+    } else {
+      if (p->y_late) launch_yrq_l<1, kW>(a, nb, s);
+      else launch_yrq_l<0, kW>(a, nb, s);
+    }
     return 0;
   }
   if (sizeof(Rl) == 4 && use_ytma(p, mode, in)) {
@@ -2394,10 +2399,10 @@ static int tune(uppe3d_plan* p) {
   // candidate only where the TMA path is unavailable; the register four-step
   // kernels (plain loads or TMA-fed tiles) give the TMA-fed kernel's bits and
   // serve Ny = 256
-  struct YC { int tma, ctas, late, kw; } yc[9] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
-                                                {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW},
-                                                {3, 1, 0, kW}};
-  const int ny = p->ytma ? (yrq_ok(p) ? 9 : 6) : 1;
+  struct YC { int tma, ctas, late, kw; } yc[11] = {{1, 2, 0, kW}, {1, 1, 0, kW}, {1, 3, 1, kW}, {1, 2, 1, kW},
+                                                 {1, 4, 0, 8}, {1, 6, 1, 8}, {2, 2, 0, kW}, {2, 3, 1, kW},
+                                                 {3, 1, 0, kW}, {2, 4, 0, 8}, {2, 6, 1, 8}};
+  const int ny = p->ytma ? (yrq_ok(p) ? 11 : 6) : 1;
   if (!p->ytma) yc[0] = YC{0, 2, 0, kW};
   const int tw_n = (p->g.Nt == 512 || (p->g.Nt == 1024 && !p->dbl)) ? 2 : 1;
   const int tw[2] = {8, 4};
@@ -2417,7 +2422,7 @@ static int tune(uppe3d_plan* p) {
   for (int i = 0; i < tw_n && !rc; ++i) {      // t candidates with the chosen y passes
     p->t_wpb = tw[i];
     rc = p->dbl ? time_attempts<double>(p, s, 3, &y_ms, &t_ms) : time_attempts<float>(p, s, 3, &y_ms, &t_ms);
-    p->tune_ms[9 + i] = t_ms;
+    p->tune_ms[11 + i] = t_ms;
     if (t_ms < best_t) { best_t = t_ms; bt = i; }
   }
   p->t_wpb = tw[bt];
@@ -2769,12 +2774,12 @@ extern "C" int uppe3d_tuning(const uppe3d_plan* p, int* cfg6, float* ms) {
 
 extern "C" int uppe3d_set_tuning(uppe3d_plan* p, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb) {
   if (!p || y_ctas < 1 || y_ctas > 6 || (y_kw != 8 && y_kw != kW) || (t_wpb != 4 && t_wpb != 8) ||
-      y_tma < 0 || y_tma > 3 || (y_tma >= 2 && (!yrq_ok(p) || y_kw != kW)) || (y_tma == 3 && y_late))
+      y_tma < 0 || y_tma > 3 || (y_tma >= 2 && !yrq_ok(p)) || (y_tma == 3 && (y_late || y_kw != kW)))
     return UPPE_ERR_ARG;
   p->y_tma = y_tma;
   p->y_late = y_late ? 1 : 0;
   // k_ypass_rq / k_ypass_ring: CTAs per SM fixed by their launch bounds
-  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) : y_tma == 3 ? 1 : y_ctas;
+  p->y_ctas = y_tma == 2 ? (p->y_late ? 3 : 2) * (kW / y_kw) : y_tma == 3 ? 1 : y_ctas;
   p->y_kw = y_kw;
   p->t_wpb = t_wpb;
   if (p->g_attempt) { cudaGraphExecDestroy(p->g_attempt); p->g_attempt = nullptr; }

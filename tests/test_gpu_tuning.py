@@ -40,7 +40,7 @@ def _tuning(sol):
 
 
 YCANDS = [(1, 2, 0, 16), (1, 1, 0, 16), (1, 3, 1, 16), (1, 2, 1, 16), (1, 4, 0, 8), (1, 6, 1, 8)]
-YCANDS_256 = YCANDS + [(2, 2, 0, 16), (2, 3, 1, 16), (3, 1, 0, 16)]   # + the register four-step kernels
+YCANDS_256 = YCANDS + [(2, 2, 0, 16), (2, 3, 1, 16), (3, 1, 0, 16), (2, 4, 0, 8), (2, 6, 1, 8)]   # + register 4-step
 
 
 @pytest.mark.parametrize('n,nt', [(64, 512), (256, 128)])
@@ -55,9 +55,9 @@ def test_tuner_runs_and_every_candidate_gives_identical_fields(n, nt):
     assert cfg[0] in (1, 2, 3) and 1 <= cfg[1] <= 6 and cfg[3] in (8, 16) and cfg[4] in (4, 8)
     ycands = YCANDS_256 if n == 256 else YCANDS
     if cfg[5] == 1:
-        assert all(v > 0 for v in ms[:len(ycands)]) and ms[9] > 0
+        assert all(v > 0 for v in ms[:len(ycands)]) and ms[11] > 0
     if n != 256:
-        assert cfg[0] == 1 and ms[6] == 0 and ms[7] == 0 and ms[8] == 0
+        assert cfg[0] == 1 and all(v == 0 for v in ms[6:11])
         assert sol._lib.uppe3d_set_tuning(sol._plan, 2, 2, 0, 16, 8) == -1   # Ny = 256 only
         assert sol._lib.uppe3d_set_tuning(sol._plan, 3, 2, 0, 16, 8) == -1
     ref = None
