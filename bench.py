@@ -609,6 +609,44 @@ def profile_kernels(sol, lib, n_attempts=3):
     return agg
 
 
+def pattern_ceilings(dev, reps=20):
+    """Copy bandwidth of the passes' access patterns alone (uppe_pattern_probe: one
+    read + one write of a 256 x 256 x 512 complex64 field, sequential, as x-pass
+    tiles or as y-pass tiles of 8, 16 or 32 omega columns), CUDA events over
+    `reps` launches after three warm-up launches; GB/s."""
+    import torch
+    from project_b200 import _lib
+    lib = _lib.load()
+    a = torch.zeros((NX, NY, NT), dtype=torch.complex64, device=dev)
+    b = torch.zeros_like(a)
+    s = _lib.stream_ptr()
+    out = {}
+    for name, pat, kw in (('sequential', 0, 16), ('x tiles kw8', 1, 8), ('x tiles kw16', 1, 16),
+                          ('x tiles kw32', 1, 32), ('y tiles kw8', 2, 8), ('y tiles kw16', 2, 16),
+                          ('y tiles kw32', 2, 32)):
+        def run():
+            _lib.check(lib.uppe_pattern_probe(pat, kw, ctypes.c_void_p(a.data_ptr()),
+                                              ctypes.c_void_p(b.data_ptr()), NT, s), 'uppe_pattern_probe')
+        for _ in range(3):
+            run()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            run()
+        e1.record()
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1) / reps
+        out[name] = 2.0 * a.numel() * 8 / (ms / 1e3) / 1e9
+    del a, b
+    return out
+
+
+# the access pattern of each pass kernel in pattern_ceilings
+PASS_PATTERN = {'k_ypass_rq': 'y tiles kw16', 'k_ypass_tma': 'y tiles kw16', 'k_ypass_ring': 'y tiles kw16',
+                'k_space': 'y tiles kw16', 'k_xpass_sq': 'x tiles kw16', 'k_tpass_w': 'sequential',
+                'k_tpass': 'sequential'}
+
+
 def _events():
     import torch
     return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -887,6 +925,12 @@ def run_b200(args, rank, world, local_rank):
             traffic = json.load(f)[dom]['measured_over_algorithmic'] * d_bytes / d_n
     except Exception:
         traffic = None
+    try:
+        patterns = pattern_ceilings(dev)
+    except Exception as e:   # reported, never fatal
+        patterns = {'error': str(e)[:200]}
+    pat_key = PASS_PATTERN.get(dom)
+    pat_gbs = patterns.get(pat_key) if pat_key else None
     step_bytes = 64.0 * (8 if prec == 'single' else 16) * npts     # 64 s N per attempt
     step_achieved = step_bytes / (ms_max / args.steps / 1e3) / 1e9
 
@@ -985,7 +1029,10 @@ def run_b200(args, rank, world, local_rank):
                          'peak_source': peak_kind, 'unit': 'GB/s', 'frac': achieved / peak,
                          'traffic': traffic, 'traffic_unit': 'bytes per launch',
                          'launches_profiled': d_n,
-                         'bytes_model': 'per launch: fields read + written x field bytes'},
+                         'bytes_model': 'per launch: fields read + written x field bytes',
+                         'access_pattern': pat_key, 'pattern_copy_gbs': pat_gbs,
+                         'frac_of_pattern_copy': (achieved / pat_gbs) if pat_gbs else None},
+            'access_pattern_copy_gbs': patterns,
             'roofline_step': {'model': '64*s*N bytes per attempt', 'achieved': step_achieved,
                               'peak': peak, 'unit': 'GB/s', 'frac': step_achieved / peak},
             'kernel_ms_per_attempt': {k: v[0] / 3 for k, v in agg.items()},
@@ -1105,6 +1152,8 @@ def main():
     ap.add_argument('--profile-table', default='adk', choices=['adk', 'mpi'])
     ap.add_argument('--profile-grid', type=int, default=NX)
     ap.add_argument('--profile-tuning', default='', help='profile case: y_tma,y_ctas,y_late,y_kw,t_wpb')
+    ap.add_argument('--pattern-probe', action='store_true',
+                    help='only the access-pattern copy bandwidths of the 3D passes (uppe_pattern_probe)')
     args = ap.parse_args()
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -1117,6 +1166,11 @@ def main():
         return run_profile_realfield(args)
     if args.profile_case:
         return run_profile_case(args)
+    if args.pattern_probe:
+        import torch
+        print(json.dumps({'access_pattern_copy_gbs': pattern_ceilings(torch.device('cuda', local_rank)),
+                          'field': [NX, NY, NT], 'dtype': 'c64'}), flush=True)
+        return 0
     import datetime
     import torch.distributed as dist
     if world > 1:

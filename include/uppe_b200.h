@@ -445,6 +445,15 @@ int uppe3d_tuning(const uppe3d_plan* plan, int* cfg6, float* ms);
  * candidates. */
 int uppe3d_set_tuning(uppe3d_plan* plan, int y_tma, int y_ctas, int y_late, int y_kw, int t_wpb);
 
+/* Access-pattern bandwidth probe (measurement hook; no reference counterpart):
+ * one read and one write of a 256 x 256 x nt complex64 field (in, out: device,
+ * distinct, 16-byte aligned; nt a power of two >= 64) with pattern 0 a sequential
+ * stream, 1 the x-pass tiles (kw omega columns from 256 rows Ny*nt elements
+ * apart), 2 the y-pass tiles (rows nt elements apart); kw 8, 16 or 32.  Each
+ * element is loaded, has 1 added to its real part and is stored: the bandwidth
+ * a pass's access pattern alone reaches, to set its achieved bandwidth against. */
+int uppe_pattern_probe(int pattern, int kw, const void* in, void* out, int nt, uppe_stream_t stream);
+
 /* Kernel launches of one propagate-mode attempt (graph nodes). */
 int uppe3d_launches_per_step(const uppe3d_plan* plan);
 /* Measurement hook: run one attempt (plus the controller) launch by launch,

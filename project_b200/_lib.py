@@ -135,6 +135,7 @@ SIGNATURES = {
     'uppe3d_transform_t': (_I, [_P, _P, _P, _I, _D, _P]),
     'uppe3d_tuning': (_I, [_P, ctypes.POINTER(_I), ctypes.POINTER(ctypes.c_float)]),
     'uppe3d_set_tuning': (_I, [_P, _I, _I, _I, _I, _I]),
+    'uppe_pattern_probe': (_I, [_I, _I, _P, _P, _I, _P]),
     'uppe3d_profile_attempt': (_I, [_P, _I, ctypes.POINTER(ctypes.c_float), ctypes.POINTER(_I),
                                     ctypes.POINTER(_D), ctypes.POINTER(_I), _P]),
 }

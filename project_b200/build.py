@@ -9,7 +9,7 @@ CSRC = os.path.join(HERE, 'csrc')
 BUILD = os.path.join(HERE, '_build')
 LIB = os.path.join(HERE, 'libuppe_b200.so')
 SOURCES = ['uppe3d.cu', 'uppe1d.cu', 'uppe1d_f32.cu', 'uppe1d_f64.cu', 'uppe1d_noalloc.cu', 'uppe1d_cl_f32.cu',
-           'uppe1d_cl_f64.cu']
+           'uppe1d_cl_f64.cu', 'uppe_probe.cu']
 HEADERS = ['common.cuh', 'uppe1d_kernel.cuh', 'uppe1d_cluster.cuh']
 NVCC_FLAGS = ['-gencode', 'arch=compute_100a,code=sm_100a', '-O3', '-lineinfo', '-std=c++17',
               '-Xcompiler', '-fPIC', '-Xcompiler', '-O2']
