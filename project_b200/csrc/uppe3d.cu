@@ -1370,66 +1370,24 @@ k_ypass_ring(SpaceArgs a, const __grid_constant__ YMaps maps) {
 }
 
 // ---------------------------------------------------------------------------
-// Warp FFT of a t-line of NT = 32*E points held in registers (E = 16 or 32).
-// Natural layout: lane l holds x[l + 32 m], m < E.  Four-step layout: lane L
-// holds X[out_index(L, k)], k < E.  fwd_like: DFT_E in registers, twiddle
-// W_NT^(l k1), transpose through a padded shared buffer S, DFT_E, then (E = 16)
-// a radix-2 combine with the partner lane L^1.  bwd_like is the transposed
-// sequence (four-step -> natural).  With DIR=-1 fwd_like is the forward FFT;
-// with DIR=+1 bwd_like is the unnormalised inverse.  tw is the four-step table
-// tw[k*32 + l] = W_NT^(l k).
+// Warp FFT of a 1024-point t-line (E = 32) held in registers.  Natural layout:
+// lane l holds x[l + 32 m], m < E.  Four-step layout: lane L holds
+// X[out_index(L, k)] = X[L + 32 k], k < E.  fwd_like: DFT_32 in registers,
+// twiddle W_NT^(l k), transpose through a padded shared buffer S, DFT_32.
+// bwd_like is the transposed sequence (four-step -> natural).  With DIR=-1
+// fwd_like is the forward FFT; with DIR=+1 bwd_like is the unnormalised
+// inverse.  tw is the four-step table tw[k*32 + l] = W_NT^(l k).
 // ---------------------------------------------------------------------------
 template <int E> struct WarpFFT {
-  static constexpr int G = 32 / E;                   // lanes per second-stage DFT
-  static constexpr int SP = 32 + (G == 2 ? 2 : 1);   // padded row stride of S
+  static_assert(E == 32, "the 512-point line has its own specialisation below");
+  static constexpr int SP = 33;                      // padded row stride of S
   static constexpr int NT = 32 * E;
   static constexpr int SBUF = E * SP;
-  __device__ __forceinline__ static int out_index(int lane, int k) {
-    return (lane / G) + E * (k + E * (lane % G));
-  }
-  // radix-2 step with the partner lane L^1 (E = 16): the factor W_32^k of register
-  // k is a compile-time constant (exact for k = 0 and 8), and the even / odd lane
-  // results are formed as b + s p with s = +-1 (an exact sign, so the same values
-  // as an add and a subtract) instead of both branches and a select per component
-  template <int K, int DIR, typename C>
-  __device__ __forceinline__ static void pair_fwd_k(C (&v)[E], bool r0) {
-    using Rl = decltype(v[0].x);
-    if constexpr (K < E) {
-      const C own = v[K];
-      C oth;
-      oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
-      oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
-      // even lane: own + W oth; odd lane: oth - W own
-      const C m = r0 ? oth : own, b = r0 ? own : oth;
-      const C p = rot<32, K, DIR>(m);
-      const Rl sg = r0 ? (Rl)1 : (Rl)-1;
-      v[K] = C{fma(sg, p.x, b.x), fma(sg, p.y, b.y)};
-      pair_fwd_k<K + 1, DIR>(v, r0);
-    }
-  }
-  template <int K, int DIR, typename C>
-  __device__ __forceinline__ static void pair_bwd_k(C (&v)[E], bool r0) {
-    using Rl = decltype(v[0].x);
-    if constexpr (K < E) {
-      const C own = v[K];
-      C oth;
-      oth.x = __shfl_xor_sync(0xffffffffu, own.x, 1);
-      oth.y = __shfl_xor_sync(0xffffffffu, own.y, 1);
-      // even lane: own + oth; odd lane: W (oth - own)
-      const Rl sg = r0 ? (Rl)1 : (Rl)-1;
-      const C d = C{fma(sg, own.x, oth.x), fma(sg, own.y, oth.y)};
-      const C p = rot<32, K, DIR>(d);
-      v[K] = r0 ? d : p;
-      pair_bwd_k<K + 1, DIR>(v, r0);
-    }
-  }
-  template <int DIR, typename C>
-  __device__ __forceinline__ static void pair_fwd(C (&v)[E], const C*, int lane) {
-    if constexpr (G == 2) pair_fwd_k<0, DIR>(v, (lane & 1) == 0);
-  }
-  template <int DIR, typename C>
-  __device__ __forceinline__ static void pair_bwd(C (&v)[E], const C*, int lane) {
-    if constexpr (G == 2) pair_bwd_k<0, DIR>(v, (lane & 1) == 0);
+  __device__ __forceinline__ static int out_index(int lane, int k) { return lane + E * k; }
+  // the twiddle table in shared memory from gtw[i] = W_NT^i
+  template <typename C>
+  __device__ __forceinline__ static void fill_twiddles(C* tw, const C* gtw, int tid, int nthr) {
+    for (int i = tid; i < NT; i += nthr) tw[i] = gtw[(i & 31) * (i >> 5)];
   }
   template <int DIR, typename C>
   __device__ __forceinline__ static void fwd_like(C (&v)[E], C* S, const C* tw, int lane) {
@@ -1443,20 +1401,16 @@ template <int E> struct WarpFFT {
 #pragma unroll
     for (int k = 0; k < E; ++k) S[k * SP + lane] = v[k];
     __syncwarp();
-    const int d = lane / G, r = lane % G;
 #pragma unroll
-    for (int i = 0; i < E; ++i) v[i] = S[d * SP + r + G * i];
+    for (int i = 0; i < E; ++i) v[i] = S[lane * SP + i];
     __syncwarp();
     DFT<E, DIR, C>::run(v);
-    pair_fwd<DIR>(v, tw, lane);
   }
   template <int DIR, typename C>
   __device__ __forceinline__ static void bwd_like(C (&v)[E], C* S, const C* tw, int lane) {
-    pair_bwd<DIR>(v, tw, lane);
     DFT<E, DIR, C>::run(v);
-    const int d = lane / G, r = lane % G;
 #pragma unroll
-    for (int i = 0; i < E; ++i) S[d * SP + r + G * i] = v[i];
+    for (int i = 0; i < E; ++i) S[lane * SP + i] = v[i];
     __syncwarp();
 #pragma unroll
     for (int k = 0; k < E; ++k) v[k] = S[k * SP + lane];
@@ -1471,11 +1425,103 @@ template <int E> struct WarpFFT {
   }
 };
 
+// ---------------------------------------------------------------------------
+// Warp FFT of a 512-point t-line (E = 16) as three radix-8 stages, natural order
+// in and out: lane l holds x[l + 32 m], m < 16, and afterwards X[l + 32 m].
+// With n = j + 64 n3 (j < 64) and k = 8 q + r:
+//   X[8 q + r] = sum_j W_64^(j q) W_512^(j r) sum_n3 x[j + 64 n3] W_8^(n3 r);
+// lane l owns j = l and l + 32 (registers m = 2 n3 + p, j = l + 32 p), so stage
+// 1 is two 8-point DFTs in registers and the W_512^(j r) twiddle.  With j = j1 + 8
+// j2 and q = 8 s + t the 64-point transform over j is stage 2 (8-point DFTs over
+// j2 of the groups (r, j1), twiddle W_64^(j1 t)) and stage 3 (8-point DFTs over
+// j1 of the groups (r, t)), and k = 64 s + 8 t + r.  Lane L takes the groups with
+// r = L % 8 and j1 (stage 2) or t (stage 3) = L / 8 + 4 g, g < 2, so stage 3
+// leaves X[L + 32 (2 s + g)] in register 2 s + g: the natural layout, stored with
+// 256-byte warp rows.  Two exchanges through S (padded row strides 66 and 72:
+// conflict-free for the 64-bit accesses of both sides).  The same routine with
+// DIR = +1 and conjugate twiddles is the unnormalised inverse, so bwd_like =
+// fwd_like.  tw: W_512^(j r) at (r - 1) 64 + j, then W_64^(j1 t) at 448 + (t - 1) 8
+// + j1.  Against the four-step form with a radix-2 lane-pair step this needs no
+// shuffles and about a quarter fewer instructions per point.
+// ---------------------------------------------------------------------------
+template <> struct WarpFFT<16> {
+  static constexpr int E = 16, NT = 512;
+  static constexpr int P1 = 66, P2 = 72;             // row strides of the two exchanges
+  static constexpr int SBUF = 8 * P2;
+  __device__ __forceinline__ static int out_index(int lane, int k) { return lane + 32 * k; }
+  template <typename C>
+  __device__ __forceinline__ static void fill_twiddles(C* tw, const C* gtw, int tid, int nthr) {
+    for (int i = tid; i < 448; i += nthr) tw[i] = gtw[(i & 63) * ((i >> 6) + 1)];
+    for (int i = tid; i < 56; i += nthr) tw[448 + i] = gtw[8 * (i & 7) * ((i >> 3) + 1)];
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void fwd_like(C (&v)[E], C* S, const C* tw, int lane) {
+    // stage 1: j = lane + 32 p, 8-point DFT over n3, twiddle W_512^(j r), Z[j][r] -> S[r P1 + j]
+#pragma unroll
+    for (int p = 0; p < 2; ++p) {
+      C e[8];
+#pragma unroll
+      for (int n3 = 0; n3 < 8; ++n3) e[n3] = v[2 * n3 + p];
+      DFT<8, DIR, C>::run(e);
+      const int j = lane + 32 * p;
+#pragma unroll
+      for (int r = 1; r < 8; ++r) {
+        C t = tw[(r - 1) * 64 + j];
+        if (DIR > 0) t.y = -t.y;
+        e[r] = cmul(e[r], t);
+      }
+#pragma unroll
+      for (int r = 0; r < 8; ++r) S[r * P1 + j] = e[r];
+    }
+    __syncwarp();
+    // stage 2: groups (r, j1 = L / 8 + 4 g): 8-point DFT over j2, twiddle W_64^(j1 t)
+    const int r = lane & 7, jq = lane >> 3;
+    C w[2][8];
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+#pragma unroll
+      for (int j2 = 0; j2 < 8; ++j2) w[g][j2] = S[r * P1 + jq + 4 * g + 8 * j2];
+    }
+    __syncwarp();
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      const int j1 = jq + 4 * g;
+      DFT<8, DIR, C>::run(w[g]);
+#pragma unroll
+      for (int t = 1; t < 8; ++t) {
+        C tt = tw[448 + (t - 1) * 8 + j1];
+        if (DIR > 0) tt.y = -tt.y;
+        w[g][t] = cmul(w[g][t], tt);
+      }
+      // element t of group (r, j1) at S[t P2 + 8 j1 + r] = S[t P2 + lane + 32 g]
+#pragma unroll
+      for (int t = 0; t < 8; ++t) S[t * P2 + lane + 32 * g] = w[g][t];
+    }
+    __syncwarp();
+    // stage 3: groups (r, t = L / 8 + 4 g): 8-point DFT over j1 -> X[L + 32 g + 64 s]
+#pragma unroll
+    for (int g = 0; g < 2; ++g) {
+      C u[8];
+#pragma unroll
+      for (int j1 = 0; j1 < 8; ++j1) u[j1] = S[(jq + 4 * g) * P2 + 8 * j1 + r];
+      DFT<8, DIR, C>::run(u);
+#pragma unroll
+      for (int s = 0; s < 8; ++s) v[2 * s + g] = u[s];
+    }
+    __syncwarp();
+  }
+  template <int DIR, typename C>
+  __device__ __forceinline__ static void bwd_like(C (&v)[E], C* S, const C* tw, int lane) {
+    fwd_like<DIR>(v, S, tw, lane);
+  }
+};
+
 // t-line nonlinear pass with the register warp FFT (NT = 512, and NT = 1024 in
 // complex64).  Same physics and operation order as k_tpass; the frequency-domain
-// line is read and written in the four-step order (coalesced: each half-warp
-// covers 16 consecutive omega), the time-domain samples stay in registers, and
-// only lines that ionise go through shared memory in time order for the scan.
+// line is read and written in the transform's output order, X[lane + 32 k] in
+// register k (coalesced: a warp covers 32 consecutive omega), the time-domain
+// samples stay in registers, and only lines that ionise go through shared memory
+// in time order for the scan.
 template <typename Rl, int E, int WPB>
 __global__ void __launch_bounds__(WPB * 32, (sizeof(Rl) == 4 && E == 16) ? 3 : 1)
 k_tpass_w(TArgs a) {
@@ -1496,13 +1542,10 @@ k_tpass_w(TArgs a) {
   Rl* shm = reinterpret_cast<Rl*>(sW0 + WPB * (NT + NT / 32));
   auto wpad = [](int t) { return t + (t >> 5); };
   {
-    // four-step twiddles tw[k*32 + l] = W_NT^(l k) (l < 32, k < E; l k < NT): the
-    // per-lane factors of a column k are consecutive (conflict-free loads)
-    const C* gtw = reinterpret_cast<const C*>(a.tb.twt);
-    for (int i = threadIdx.x; i < NT; i += WPB * 32) {
-      tw[i] = gtw[(i & 31) * (i >> 5)];
-      shm[i] = a.tb.valid[i] ? (Rl)a.tb.shock[i] : (Rl)-1;
-    }
+    // the transform's twiddle table (per-lane factors consecutive: conflict-free
+    // loads) and the output factor per omega bin
+    W::fill_twiddles(tw, reinterpret_cast<const C*>(a.tb.twt), threadIdx.x, WPB * 32);
+    for (int i = threadIdx.x; i < NT; i += WPB * 32) shm[i] = a.tb.valid[i] ? (Rl)a.tb.shock[i] : (Rl)-1;
   }
   __syncthreads();
   State3D* st = a.st;
