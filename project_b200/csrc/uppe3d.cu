@@ -480,7 +480,10 @@ __device__ __forceinline__ void fft_sq(C (&v)[R], C* T, const C* tw, int j, int 
   DFT<R, DIR, C>::run(v);
 }
 
-template <typename Rl, int R>
+// XM: the pass (XINV, XINV_Z, XFWD, XFWD_Z) as a compile-time constant, so that
+// each instantiation holds only its own path (fewer live registers for the plain
+// transforms, which are seven of an attempt's nine x passes).
+template <typename Rl, int R, int XM>
 __global__ void __launch_bounds__(kW * R, (sizeof(Rl) == 4 && R == 16) ? 3 : 1)
 k_xpass_sq(SpaceArgs a) {
   using C = typename CT<Rl>::T;
@@ -491,14 +494,14 @@ k_xpass_sq(SpaceArgs a) {
   C* T = tw + N;
   const int tid = threadIdx.x, w = tid % kW, j = tid / kW;
   State3D* st = a.st;
-  const int mode = a.mode;
+  constexpr int mode = XM;
   {
     const C* gtw = reinterpret_cast<const C*>(a.tb.twx);
     for (int i = tid; i < N; i += NTHR) tw[i] = gtw[i];
   }
   __syncthreads();
   if (st->done) return;
-  if (mode == XFWD_Z && !st->fresh) return;
+  if constexpr (mode == XFWD_Z) if (!st->fresh) return;
   const int Nt = a.g.Nt, Ny = a.g.Ny;
   const int ntile = Nt / kW;
   const int o = blockIdx.x / ntile;          // y index
@@ -510,14 +513,14 @@ k_xpass_sq(SpaceArgs a) {
   C* __restrict__ out = reinterpret_cast<C*>(a.out);
   C v[R];
   auto gidx = [&](int i) { return base + (long long)(j + R * i) * stride; };
-  const bool inv = (mode == XINV || mode == XINV_Z);
+  constexpr bool inv = (mode == XINV || mode == XINV_Z);
 #pragma unroll
   for (int i = 0; i < R; ++i) v[i] = __ldg(in + gidx(i));
-  if (inv) fft_sq<R, +1>(v, T, tw, j, w);
+  if constexpr (inv) fft_sq<R, +1>(v, T, tw, j, w);
   else fft_sq<R, -1>(v, T, tw, j, w);
 #pragma unroll
   for (int i = 0; i < R; ++i) out[gidx(i)] = v[i];
-  if (mode == XINV_Z) {
+  if constexpr (mode == XINV_Z) {
     // candidate state Z = ifft2(A4) * filter(omega) * exp(-damp(x,y) h); one
     // absorber factor per x of this y (exp(-0 h) = 1 exactly), kept in the
     // transpose buffer, which fft_sq has released
@@ -536,7 +539,7 @@ k_xpass_sq(SpaceArgs a) {
       zc[gidx(i)] = cscale(cscale(cscale(v[i], nrm), f), absx[x]);
     }
   }
-  if (mode == XFWD_Z) {
+  if constexpr (mode == XFWD_Z) {
     const C* __restrict__ zin = reinterpret_cast<const C*>(a.b.z[st->zidx]);
     C* __restrict__ zout = reinterpret_cast<C*>(a.b.tmp[2]);
 #pragma unroll
@@ -1982,7 +1985,13 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
     if (a.mode <= XFWD_Z) {   // x passes of square sizes: register four-step kernel
       using C = typename CT<Rl>::T;
       const size_t sm = sizeof(C) * (size_t)(N + N * kW);
-      k_xpass_sq<Rl, R><<<(unsigned)nblocks, kW * R, sm, s>>>(a);
+      const unsigned nb = (unsigned)nblocks;
+      switch (a.mode) {
+        case XINV: k_xpass_sq<Rl, R, XINV><<<nb, kW * R, sm, s>>>(a); break;
+        case XINV_Z: k_xpass_sq<Rl, R, XINV_Z><<<nb, kW * R, sm, s>>>(a); break;
+        case XFWD: k_xpass_sq<Rl, R, XFWD><<<nb, kW * R, sm, s>>>(a); break;
+        default: k_xpass_sq<Rl, R, XFWD_Z><<<nb, kW * R, sm, s>>>(a); break;
+      }
       return;
     }
   }
@@ -2199,7 +2208,10 @@ static cudaError_t set_space_attr() {
   constexpr int R = SqRoot<N>::v;
   if constexpr (R > 0) {
     const int sm = (int)(sizeof(typename CT<Rl>::T) * (N + N * kW));
-    const cudaError_t e = cudaFuncSetAttribute(k_xpass_sq<Rl, R>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaError_t e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XINV>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XINV_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e != cudaSuccess) return e;
   }
   const int smem = (int)(sizeof(typename CT<Rl>::T) * (N + 2 * N * kW));
