@@ -1033,7 +1033,9 @@ static size_t ytma_smem(int mode) {
 // (two CTAs per SM); LATE = 1 issues them element by element in the stage loop
 // (three CTAs per SM).  One instantiation per pass.
 // ---------------------------------------------------------------------------
-template <int MODE, int LATE, int KW = kW>
+// NTC > 0: the omega extent Nt as a compile-time constant (row offsets become
+// immediates, which frees the registers of sixteen 64-bit addresses); 0: runtime.
+template <int MODE, int LATE, int KW = kW, int NTC = 0>
 __global__ void __launch_bounds__(KW * 16, (LATE ? 3 : 2) * (kW / KW))
 k_ypass_rq(SpaceArgs a) {
   using C = float2;
@@ -1048,7 +1050,7 @@ k_ypass_rq(SpaceArgs a) {
   if (st->done) return;
   if (MODE == YMID1R && st->fresh) return;
   if (MODE == YMID1 && !st->fresh) return;
-  const int Nt = a.g.Nt;
+  const int Nt = NTC > 0 ? NTC : a.g.Nt;
   const int ntile = Nt / KW;
   const int o = blockIdx.x / ntile;            // kx index
   const int w0 = (blockIdx.x % ntile) * KW;    // omega offset
@@ -2049,6 +2051,17 @@ template <int LATE, int KW>
 static void launch_yrq_l(const SpaceArgs& a, unsigned nblocks, cudaStream_t s) {
   constexpr unsigned T = KW * 16;
   constexpr size_t sm = yrq_smem<KW>();
+  if (LATE == 0 && KW == kW && a.g.Nt == 512) {   // the tuned configuration at Nt = 512
+    switch (a.mode) {
+      case YMID1: k_ypass_rq<YMID1, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+      case YMID1R: k_ypass_rq<YMID1R, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+      case YMID2: k_ypass_rq<YMID2, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+      case YMID3: k_ypass_rq<YMID3, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+      case YMID4: k_ypass_rq<YMID4, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+      default: k_ypass_rq<YFWD5, 0, kW, 512><<<nblocks, T, sm, s>>>(a); break;
+    }
+    return;
+  }
   switch (a.mode) {
     case YMID1: k_ypass_rq<YMID1, LATE, KW><<<nblocks, T, sm, s>>>(a); break;
     case YMID1R: k_ypass_rq<YMID1R, LATE, KW><<<nblocks, T, sm, s>>>(a); break;

@@ -43,7 +43,7 @@ YCANDS = [(1, 2, 0, 16), (1, 1, 0, 16), (1, 3, 1, 16), (1, 2, 1, 16), (1, 4, 0, 
 YCANDS_256 = YCANDS + [(2, 2, 0, 16), (2, 3, 1, 16), (3, 1, 0, 16), (2, 4, 0, 8), (2, 6, 1, 8)]   # + register 4-step
 
 
-@pytest.mark.parametrize('n,nt', [(64, 512), (256, 128)])
+@pytest.mark.parametrize('n,nt', [(64, 512), (256, 128), (256, 512)])
 def test_tuner_runs_and_every_candidate_gives_identical_fields(n, nt):
     import torch
     from project_b200 import _lib
