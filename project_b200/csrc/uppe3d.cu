@@ -483,7 +483,9 @@ __device__ __forceinline__ void fft_sq(C (&v)[R], C* T, const C* tw, int j, int 
 // XM: the pass (XINV, XINV_Z, XFWD, XFWD_Z) as a compile-time constant, so that
 // each instantiation holds only its own path (fewer live registers for the plain
 // transforms, which are seven of an attempt's nine x passes).
-template <typename Rl, int R, int XM>
+// NTC > 0: the omega extent Nt (and Ny = Nx) as compile-time constants, so the
+// row stride Ny Nt and the row offsets fold into the address arithmetic.
+template <typename Rl, int R, int XM, int NTC = 0>
 __global__ void __launch_bounds__(kW * R, (sizeof(Rl) == 4 && R == 16) ? 3 : 1)
 k_xpass_sq(SpaceArgs a) {
   using C = typename CT<Rl>::T;
@@ -502,7 +504,7 @@ k_xpass_sq(SpaceArgs a) {
   __syncthreads();
   if (st->done) return;
   if constexpr (mode == XFWD_Z) if (!st->fresh) return;
-  const int Nt = a.g.Nt, Ny = a.g.Ny;
+  const int Nt = NTC > 0 ? NTC : a.g.Nt, Ny = NTC > 0 ? N : a.g.Ny;
   const int ntile = Nt / kW;
   const int o = blockIdx.x / ntile;          // y index
   const int w0 = (blockIdx.x % ntile) * kW;  // omega offset
@@ -1988,6 +1990,15 @@ static void launch_space_n(const SpaceArgs& a, long long nblocks, size_t smem, c
       using C = typename CT<Rl>::T;
       const size_t sm = sizeof(C) * (size_t)(N + N * kW);
       const unsigned nb = (unsigned)nblocks;
+      if (sizeof(Rl) == 4 && N == 256 && a.g.Nt == 512 && a.g.Ny == 256) {   // 256 x 256 x 512 complex64
+        switch (a.mode) {
+          case XINV: k_xpass_sq<Rl, R, XINV, 512><<<nb, kW * R, sm, s>>>(a); break;
+          case XINV_Z: k_xpass_sq<Rl, R, XINV_Z, 512><<<nb, kW * R, sm, s>>>(a); break;
+          case XFWD: k_xpass_sq<Rl, R, XFWD, 512><<<nb, kW * R, sm, s>>>(a); break;
+          default: k_xpass_sq<Rl, R, XFWD_Z, 512><<<nb, kW * R, sm, s>>>(a); break;
+        }
+        return;
+      }
       switch (a.mode) {
         case XINV: k_xpass_sq<Rl, R, XINV><<<nb, kW * R, sm, s>>>(a); break;
         case XINV_Z: k_xpass_sq<Rl, R, XINV_Z><<<nb, kW * R, sm, s>>>(a); break;
@@ -2225,6 +2236,12 @@ static cudaError_t set_space_attr() {
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XINV_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD_Z>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if constexpr (sizeof(Rl) == 4 && N == 256) {
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XINV, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XINV_Z, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+      if (e == cudaSuccess) e = cudaFuncSetAttribute(k_xpass_sq<Rl, R, XFWD_Z, 512>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
     if (e != cudaSuccess) return e;
   }
   const int smem = (int)(sizeof(typename CT<Rl>::T) * (N + 2 * N * kW));
