@@ -1100,6 +1100,44 @@ def run_profile_case(args):
     return 0
 
 
+def run_profile_batched(args):
+    """The batched 1D sweep's longest instance alone, for profiler commands: one
+    sweep (untimed) finds the instance with the most attempts; the same instance
+    over --profile-l metres runs --warmup times untimed, then once inside an NVTX
+    range named "timed" (one launch of the cluster kernel)."""
+    import torch
+    from project_b200.solver1d import BatchedPropagator
+    dev = torch.device('cuda')
+    insts, fields = batched1d_instances()
+    bp = BatchedPropagator(insts, precision='single', device=dev)
+    _, _, res = bp.run(fields)
+    k = int(np.argmax([r.attempts for r in res]))
+    del bp
+    insts_l, fields_l = batched1d_instances(L=args.profile_l)
+    one = BatchedPropagator([insts_l[k]], precision='single', device=dev)
+    packed0 = one.pack([fields_l[k]])
+    work = packed0.clone()
+    for _ in range(max(args.warmup, 1)):
+        work.copy_(packed0)
+        one.run_packed(work)
+    work.copy_(packed0)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push('timed')
+    e0.record()
+    r = one.run_packed(work)[0]
+    e1.record()
+    torch.cuda.nvtx.range_pop()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    print(json.dumps({'instance': k, 'Nt': int(insts_l[k]['desc'].Nt), 'energy_J': insts_l[k]['energy'],
+                      'pressure_bar': insts_l[k]['pressure'], 'L_m': args.profile_l,
+                      'attempts_full_sweep': int(res[k].attempts), 'attempts': int(r.attempts),
+                      'ms': ms, 'ms_per_attempt': ms / max(int(r.attempts), 1),
+                      'clusters': int(one._lib.uppe1d_uses_clusters(one._plan))}), flush=True)
+    return 0
+
+
 def run_profile_realfield(args):
     """Only the real-field propagator (the realfield_3d workload), for profiler
     commands: --warmup untimed attempts, then --steps attempts inside an NVTX range
@@ -1152,6 +1190,9 @@ def main():
     ap.add_argument('--profile-table', default='adk', choices=['adk', 'mpi'])
     ap.add_argument('--profile-grid', type=int, default=NX)
     ap.add_argument('--profile-tuning', default='', help='profile case: y_tma,y_ctas,y_late,y_kw,t_wpb')
+    ap.add_argument('--profile-batched', action='store_true',
+                    help='only the batched sweep\'s longest instance over --profile-l m, one timed launch')
+    ap.add_argument('--profile-l', type=float, default=0.1)
     ap.add_argument('--pattern-probe', action='store_true',
                     help='only the access-pattern copy bandwidths of the 3D passes (uppe_pattern_probe)')
     args = ap.parse_args()
@@ -1166,6 +1207,8 @@ def main():
         return run_profile_realfield(args)
     if args.profile_case:
         return run_profile_case(args)
+    if args.profile_batched:
+        return run_profile_batched(args)
     if args.pattern_probe:
         import torch
         print(json.dumps({'access_pattern_copy_gbs': pattern_ceilings(torch.device('cuda', local_rank)),
