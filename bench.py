@@ -283,7 +283,8 @@ def run_batched1d(dev, rank=0, world=1, accuracy=False):
         att = [merged[i]['attempts'] for i in range(n_all)]
         res = [type('R', (), merged[i]) for i in range(n_all)]
     return {'value': n_all / sec, 'unit': 'sims/s', 'n_instances': n_all, 'seconds': sec, 'ranks': world,
-            'kernel': 'four-CTA clusters per line' if bp._lib.uppe1d_uses_clusters(bp._plan) else 'one CTA per line',
+            'kernel': ('thread-block clusters per line: eight CTAs for the costliest lines, four for the rest'
+                       if bp._lib.uppe1d_uses_clusters(bp._plan) else 'one CTA per line'),
             'attempts_total': int(sum(att)), 'attempts_max': int(max(att)),
             'status_nonzero': int(sum(1 for r in res if r.status)), 'dtype': 'c64',
             'workload': 'batched 1D sweep, 256 argon-capillary instances, L = 1 m, tol 1e-6, '

@@ -25,9 +25,19 @@ struct uppe1d_plan {
   int nblocks;
   int nsm;
   size_t smem;
-  bool use_cl = false;    // lines run on four-CTA clusters (uppe1d_cluster.cuh)
+  bool use_cl = false;    // lines run on thread-block clusters (uppe1d_cluster.cuh)
+  int cs = kCS;           // CTAs per cluster (4, or 8 with UPPE_CLUSTER_CTAS=8)
   int ncl = 0;            // clusters of the persistent cluster launch
   size_t cl_smem = 0;
+  // mixed launch: n8 eight-CTA clusters take the costliest lines while the ncl
+  // four-CTA clusters run the rest, concurrently on a second stream
+  bool mixed = false;
+  int n8 = 0;
+  size_t cl_smem8 = 0;
+  const void* xtw8 = nullptr;
+  int* counter_head = nullptr;
+  cudaStream_t s2 = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   int last_ctas = 0;      // CTAs of the last propagation launch (activity record)
   Batch1D b;
   Inst1D* d_inst;
@@ -65,6 +75,9 @@ extern "C" int uppe1d_plan_destroy(uppe1d_plan* p) {
   if (p->d_prog) cudaFree(p->d_prog);
   if (p->d_prog_scratch) cudaFree(p->d_prog_scratch);
   if (p->h_res) cudaFreeHost(p->h_res);
+  if (p->s2) cudaStreamDestroy(p->s2);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
   delete p;
   return 0;
 }
@@ -122,7 +135,8 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   if (any_raman && !d->H) { delete p; return UPPE_ERR_ARG; }
   // The cluster kernel serves plans whose lines are all 2048..16384 points without
   // Raman or history and at least one of them long (>= 8192): one line then runs
-  // on four SMs.  UPPE_1D_CLUSTER=0 keeps the single-CTA kernel where it can serve.
+  // on four SMs (eight for the costliest lines of a large batch, below).
+  // UPPE_1D_CLUSTER=0 keeps the single-CTA kernel where it can serve.
   {
     bool ok = true, longer = false;
     for (int i = 0; i < d->n_inst; ++i) {
@@ -234,32 +248,72 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   p->b.xtw = nullptr;
   p->b.cl_scratch = nullptr;
   p->b.cl_scratch_bytes = 0;
+  p->b.counter_head = nullptr;
+  p->b.nhead = 0;
+  p->b.cl_off = 0;
+  p->b.busy_off = 0;
   if (p->use_cl) {
-    // cross-CTA twiddles W_N^(m r) (r = 1..3, m < M = N/4) for M = 512 .. nmax/4
-    const int mmax = nmax / kCS;
-    std::vector<unsigned char> xt(p->csz * (size_t)(cl_xtw_offset(mmax) + 3LL * mmax));
-    for (int M = 512; M <= mmax; M *= 2) {
-      const long long o = cl_xtw_offset(M);
-      for (int r = 1; r < kCS; ++r)
-        for (int m = 0; m < M; ++m) {
-          const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * r) /
-                                  (long double)(kCS * M);
-          const double cr = (double)cosl(ang), ci = (double)sinl(ang);
-          const long long e = o + (long long)(r - 1) * M + m;
-          if (dbl) ((double2*)xt.data())[e] = make_double2(cr, ci);
-          else ((float2*)xt.data())[e] = make_float2((float)cr, (float)ci);
+    // CTAs per line: UPPE_CLUSTER_CTAS=4 or 8 forces one size; otherwise a batch of
+    // many lines with 16384-point ones runs its costliest lines on eight-CTA
+    // clusters next to four-CTA clusters for the rest (mixed launch)
+    const char* env_cs = getenv("UPPE_CLUSTER_CTAS");
+    const int force = env_cs ? atoi(env_cs) : 0;
+    p->cs = force == 8 ? 8 : 4;
+    int n16 = 0;
+    for (int i = 0; i < p->ninst; ++i) n16 += p->h_inst[i].Nt == 16384;
+    p->mixed = force == 0 && nmax == 16384 && p->ninst >= 16;
+    // cross-CTA twiddles W_N^(m r) (r = 1..cs-1, m < M = N/cs) for M = 2048/cs .. nmax/cs
+    auto xtw_table = [&](int cs, const void** dst) -> int {
+      const int mmax = nmax / cs;
+      std::vector<unsigned char> xt(p->csz * (size_t)(cl_xtw_offset(mmax, cs) + (long long)(cs - 1) * mmax));
+      for (int M = 2048 / cs; M <= mmax; M *= 2) {
+        const long long o = cl_xtw_offset(M, cs);
+        for (int r = 1; r < cs; ++r)
+          for (int m = 0; m < M; ++m) {
+            const long double ang = -2.0L * 3.141592653589793238462643383279502884L * (long double)(m * r) /
+                                    (long double)(cs * M);
+            const double cr = (double)cosl(ang), ci = (double)sinl(ang);
+            const long long e = o + (long long)(r - 1) * M + m;
+            if (dbl) ((double2*)xt.data())[e] = make_double2(cr, ci);
+            else ((float2*)xt.data())[e] = make_float2((float)cr, (float)ci);
+          }
+      }
+      void* q = nullptr;
+      const int r = up1(p, &q, xt.data(), xt.size());
+      *dst = q;
+      return r;
+    };
+    TRY1(xtw_table(p->cs, &p->b.xtw));
+    p->cl_smem = dbl ? cl_smem<double>(nmax, p->cs) : cl_smem<float>(nmax, p->cs);
+    const int maxcl = dbl ? uppe1d_cl_max_clusters<double>(p->cl_smem, p->cs)
+                          : uppe1d_cl_max_clusters<float>(p->cl_smem, p->cs);
+    p->ncl = std::min(p->ninst, maxcl > 0 ? maxcl : nsm / p->cs);
+    if (p->mixed) {
+      p->cl_smem8 = dbl ? cl_smem<double>(nmax, 8) : cl_smem<float>(nmax, 8);
+      const int max8 = dbl ? uppe1d_cl_max_clusters<double>(p->cl_smem8, 8)
+                           : uppe1d_cl_max_clusters<float>(p->cl_smem8, 8);
+      p->n8 = std::min(std::min(4, n16), max8);
+      if (p->n8 <= 0) {
+        p->mixed = false;
+      } else {
+        TRY1(xtw_table(8, &p->xtw8));
+        p->ncl = std::max(1, std::min(p->ninst - p->n8, std::min(maxcl > 0 ? maxcl : nsm / 4,
+                                                                   (nsm - 8 * p->n8) / 4)));
+        TRY1(up1(p, &ptr, nullptr, sizeof(int))); p->counter_head = (int*)ptr;
+        if (cudaStreamCreateWithFlags(&p->s2, cudaStreamNonBlocking) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&p->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+          uppe1d_plan_destroy(p);
+          return UPPE_ERR_CUDA;
         }
+      }
     }
-    TRY1(up1(p, &ptr, xt.data(), xt.size())); p->b.xtw = ptr;
-    p->cl_smem = dbl ? cl_smem<double>(nmax) : cl_smem<float>(nmax);
-    const int maxcl = dbl ? uppe1d_cl_max_clusters<double>(p->cl_smem) : uppe1d_cl_max_clusters<float>(p->cl_smem);
-    p->ncl = std::min(p->ninst, maxcl > 0 ? maxcl : nsm / kCS);
     p->b.cl_scratch_bytes = (long long)(dbl ? cl_scratch_bytes<double>(nmax) : cl_scratch_bytes<float>(nmax));
-    TRY1(up1(p, &ptr, nullptr, (size_t)p->b.cl_scratch_bytes * p->ncl)); p->b.cl_scratch = ptr;
+    TRY1(up1(p, &ptr, nullptr, (size_t)p->b.cl_scratch_bytes * (p->ncl + p->n8))); p->b.cl_scratch = ptr;
   }
   {
     // activity record: two timer values per CTA of the widest launch
-    const int ctas = std::max(p->nblocks, kCS * p->ncl);
+    const int ctas = std::max(p->nblocks, p->cs * p->ncl + 8 * p->n8);
     TRY1(up1(p, &ptr, nullptr, 2 * sizeof(unsigned long long) * (size_t)ctas));
     p->b.busy = static_cast<unsigned long long*>(ptr);
   }
@@ -268,11 +322,40 @@ extern "C" int uppe1d_plan_create(const uppe1d_desc* d, uppe1d_plan** out) {
   return 0;
 }
 
-// the propagation kernel of the plan: four-CTA clusters per line, or one CTA per line
+__global__ void k_queue_head(int* counter, int* counter_head, int nhead) {
+  *counter = nhead;
+  *counter_head = 0;
+}
+
+// the propagation kernel of the plan: thread-block clusters per line (one size, or
+// the mixed launch), or one CTA per line
 static cudaError_t launch_lines(uppe1d_plan* p, const Batch1D& b, cudaStream_t s) {
-  p->last_ctas = p->use_cl ? kCS * p->ncl : p->nblocks;
+  if (p->use_cl && p->mixed) {
+    // eight-CTA clusters take queue positions [0, n8), on a second stream forked
+    // from and joined back into s; the four-CTA clusters take the rest from n8
+    p->last_ctas = 8 * p->n8 + 4 * p->ncl;
+    k_queue_head<<<1, 1, 0, s>>>(b.counter, p->counter_head, p->n8);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev_fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(p->s2, p->ev_fork, 0);
+    if (e != cudaSuccess) return e;
+    Batch1D b8 = b;
+    b8.xtw = p->xtw8; b8.counter_head = p->counter_head; b8.nhead = p->n8; b8.cl_off = 0; b8.busy_off = 0;
+    e = p->dbl ? launch_uppe1d_cl<double>(b8, p->n8, p->cl_smem8, p->s2, 8)
+               : launch_uppe1d_cl<float>(b8, p->n8, p->cl_smem8, p->s2, 8);
+    if (e != cudaSuccess) return e;
+    Batch1D b4 = b;
+    b4.nhead = 0; b4.cl_off = p->n8; b4.busy_off = 8 * p->n8;
+    e = p->dbl ? launch_uppe1d_cl<double>(b4, p->ncl, p->cl_smem, s, 4)
+               : launch_uppe1d_cl<float>(b4, p->ncl, p->cl_smem, s, 4);
+    if (e == cudaSuccess) e = cudaEventRecord(p->ev_join, p->s2);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, p->ev_join, 0);
+    return e;
+  }
+  p->last_ctas = p->use_cl ? p->cs * p->ncl : p->nblocks;
   if (p->use_cl)
-    return p->dbl ? launch_uppe1d_cl<double>(b, p->ncl, p->cl_smem, s) : launch_uppe1d_cl<float>(b, p->ncl, p->cl_smem, s);
+    return p->dbl ? launch_uppe1d_cl<double>(b, p->ncl, p->cl_smem, s, p->cs)
+                  : launch_uppe1d_cl<float>(b, p->ncl, p->cl_smem, s, p->cs);
   return p->dbl ? launch_uppe1d<double>(b, p->nblocks, p->smem, s) : launch_uppe1d<float>(b, p->nblocks, p->smem, s);
 }
 

@@ -1,10 +1,11 @@
 #pragma once
-// 1D ERK4(3)-IP propagation of one instance by a thread-block cluster of four
-// CTAs (long lines, sm_100a distributed shared memory).
+// 1D ERK4(3)-IP propagation of one instance by a thread-block cluster of CS = 4
+// or 8 CTAs (long lines, sm_100a distributed shared memory).
 //
 // The single-CTA kernel (uppe1d_kernel.cuh) runs a whole instance on one SM, so a
-// batch takes as long as its longest line.  Here the four CTAs of a cluster share
-// one line of N = 4 M points:
+// batch takes as long as its longest line.  Here the CTAs of a cluster share one
+// line of N = CS M points (written below for CS = 4; with eight CTAs the cross
+// step is radix 8):
 //   * time domain: CTA r holds samples n = r M + m (m < M) in its shared line;
 //   * omega domain: CTA r holds the bins k = r + 4 j (j < M), at index j;
 //   * a forward transform is one radix-4 step across the cluster (each CTA reads
@@ -28,11 +29,14 @@
 namespace uppe {
 namespace cg = cooperative_groups;
 
-constexpr int kCS = 4;   // CTAs per line
+constexpr int kCS = 4;   // CTAs per line by default (8 is the other supported size)
 
 // offset (elements) of the cross-CTA twiddles W_N^(m r), r = 1..3, m < M = N/4,
 // for every M = 512 .. 4096: 3 (M - 512), entry (r - 1) M + m
-__host__ __device__ constexpr long long cl_xtw_offset(int M) { return 3LL * (M - 512); }
+// (for CS CTAs per line: (CS - 1) entries per M, M = 2048 / CS .. 16384 / CS)
+__host__ __device__ constexpr long long cl_xtw_offset(int M, int CS = kCS) {
+  return (long long)(CS - 1) * (M - 2048 / CS);
+}
 
 template <typename Rl> struct ClCtx {
   using C = typename CT<Rl>::T;
@@ -60,33 +64,46 @@ template <typename Rl> struct ClCtx {
   int r;                 // rank in the cluster
 };
 
-// x * W_4^e (DIR = -1: exp(-2 pi i e / 4); +1: exp(+2 pi i e / 4))
-template <int DIR, typename C> __device__ __forceinline__ C w4(C x, int e) {
-  switch (e & 3) {
-    case 0: return x;
-    case 1: return mul_pmi<DIR>(x);
-    case 2: return C{-x.x, -x.y};
-    default: return mul_pmi<-DIR>(x);
+// x * W_CS^e (DIR = -1: exp(-2 pi i e / CS); +1: exp(+2 pi i e / CS)), CS = 4 or 8
+template <int DIR, int CS, typename C> __device__ __forceinline__ C wcs(C x, int e) {
+  if constexpr (CS == 4) {
+    switch (e & 3) {
+      case 0: return x;
+      case 1: return mul_pmi<DIR>(x);
+      case 2: return C{-x.x, -x.y};
+      default: return mul_pmi<-DIR>(x);
+    }
+  } else {
+    switch (e & 7) {
+      case 0: return x;
+      case 1: return rot<8, 1, DIR>(x);
+      case 2: return rot<8, 2, DIR>(x);
+      case 3: return rot<8, 3, DIR>(x);
+      case 4: return rot<8, 4, DIR>(x);
+      case 5: return rot<8, 5, DIR>(x);
+      case 6: return rot<8, 6, DIR>(x);
+      default: return rot<8, 7, DIR>(x);
+    }
   }
 }
 
 // radix-4 step across the cluster into buf, then swap line/buf.  DIR = -1: out[m]
 // = W_N^(m r) sum_q W_4^(q r) line_q[m]; DIR = +1: out[m] = sum_q W_4^(-q r)
 // line_q[m] (the caller has applied the conjugate twiddles to line_q).
-template <typename Rl, int M, int DIR>
+template <typename Rl, int M, int DIR, int CS>
 __device__ __forceinline__ void cl_cross(ClCtx<Rl>& c, cg::cluster_group& cl) {
   using C = typename CT<Rl>::T;
   cl.sync();                                   // every CTA's line is complete
-  C* rem[kCS];
+  C* rem[CS];
 #pragma unroll
-  for (int q = 0; q < kCS; ++q) rem[q] = cl.map_shared_rank(c.line(), q);
+  for (int q = 0; q < CS; ++q) rem[q] = cl.map_shared_rank(c.line(), q);
   const int r = c.r;
   // all of a thread's remote loads in flight together (M / T1 <= 8 iterations)
 #pragma unroll
   for (int m = threadIdx.x; m < M; m += T1) {
     C acc = rem[0][pad1(m)];
 #pragma unroll
-    for (int q = 1; q < kCS; ++q) acc = cadd(acc, w4<DIR>(rem[q][pad1(m)], q * r));
+    for (int q = 1; q < CS; ++q) acc = cadd(acc, wcs<DIR, CS>(rem[q][pad1(m)], q * r));
     if (DIR < 0 && r > 0) acc = cmul(acc, c.xtw[(r - 1) * M + m]);
     c.buf()[pad1(m)] = acc;
   }
@@ -95,37 +112,37 @@ __device__ __forceinline__ void cl_cross(ClCtx<Rl>& c, cg::cluster_group& cl) {
 }
 
 // time domain (CTA r: samples r M + m) -> omega domain (CTA r: bins r + 4 j)
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ __forceinline__ void cl_fft_fwd(ClCtx<Rl>& c, cg::cluster_group& cl) {
-  cl_cross<Rl, M, -1>(c, cl);
+  cl_cross<Rl, M, -1, CS>(c, cl);
   line_fft<M, -1>(c.line(), c.tw, threadIdx.x);
 }
 
 // omega domain -> time domain, unnormalised
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ __forceinline__ void cl_fft_inv(ClCtx<Rl>& c, cg::cluster_group& cl) {
   using C = typename CT<Rl>::T;
   line_fft<M, +1>(c.line(), c.tw, threadIdx.x);
   if (c.r > 0) {
     for (int m = threadIdx.x; m < M; m += T1) c.line()[pad1(m)] = cmul(c.line()[pad1(m)], cconj(c.xtw[(c.r - 1) * M + m]));
   }
-  cl_cross<Rl, M, +1>(c, cl);
+  cl_cross<Rl, M, +1, CS>(c, cl);
 }
 
 // sum over the cluster (every thread of every CTA gets the same value)
-template <typename Rl>
+template <typename Rl, int CS>
 __device__ __forceinline__ double cl_sum(ClCtx<Rl>& c, cg::cluster_group& cl, double v) {
   v = block_sum(v, c.red);
   if (threadIdx.x == 0) c.slot[0] = v;
   cl.sync();
   double s = 0.0;
 #pragma unroll
-  for (int q = 0; q < kCS; ++q) s += *cl.map_shared_rank(&c.slot[0], q);
+  for (int q = 0; q < CS; ++q) s += *cl.map_shared_rank(&c.slot[0], q);
   cl.sync();
   return s;
 }
 
-template <typename Rl>
+template <typename Rl, int CS>
 __device__ __forceinline__ double cl_max(ClCtx<Rl>& c, cg::cluster_group& cl, double v) {
   v = warp_max(v);
   if ((threadIdx.x & 31) == 0) c.red[threadIdx.x >> 5] = v;
@@ -138,7 +155,7 @@ __device__ __forceinline__ double cl_max(ClCtx<Rl>& c, cg::cluster_group& cl, do
   cl.sync();
   double mx = 0.0;
 #pragma unroll
-  for (int q = 0; q < kCS; ++q) mx = fmax(mx, *cl.map_shared_rank(&c.slot[1], q));
+  for (int q = 0; q < CS; ++q) mx = fmax(mx, *cl.map_shared_rank(&c.slot[1], q));
   cl.sync();
   return mx;
 }
@@ -149,7 +166,7 @@ __device__ __forceinline__ double cl_max(ClCtx<Rl>& c, cg::cluster_group& cl, do
 // preceding CTAs' affine maps; when a clamp binds anywhere the exact serial
 // update runs CTA by CTA.  Returns false on every CTA when the whole line has
 // W_ion = 0 and no avalanche.
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) {
   using C = typename CT<Rl>::T;
   constexpr int CH = Cfg1<M>::CH, NA = Cfg1<M>::NA;
@@ -203,7 +220,7 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
   bool all_any = m.ava != 0.0, all_ok = true;
   double rho_in = 0.0;
 #pragma unroll
-  for (int q = 0; q < kCS; ++q) {
+  for (int q = 0; q < CS; ++q) {
     const double* sq = cl.map_shared_rank(c.slot, q);
     all_any |= sq[4] != 0.0;
     all_ok &= sq[5] != 0.0;
@@ -220,7 +237,7 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
     __syncthreads();
   } else {
     // exact serial update: CTA q continues from CTA q-1's final density
-    for (int q = 0; q < kCS; ++q) {
+    for (int q = 0; q < CS; ++q) {
       if (c.r == q && tid == 0) {
         double rho = q == 0 ? 0.0 : *cl.map_shared_rank(&c.slot[6], q - 1);
         for (int t = 0; t < M; ++t) {
@@ -257,18 +274,18 @@ __device__ bool cl_plasma(ClCtx<Rl>& c, cg::cluster_group& cl, double* ion_out) 
       c.line()[pad1(t)] = C{(Rl)(cr * a.x - ci * a.y), (Rl)(cr * a.y + ci * a.x)};
     }
   }
-  const double mx = cl_max(c, cl, ion / m.rho_nt);
+  const double mx = cl_max<Rl, CS>(c, cl, ion / m.rho_nt);
   if (ion_out) *ion_out = fmax(*ion_out, mx);
   return true;
 }
 
 // N(u) for this CTA's bins (erk43ip_method.py:197-255 plus the plasma term),
 // the stage input u formed on the fly; returns sum |u|^2 over the line for IN_5.
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, int mode, double h,
                                           typename CT<Rl>::T* out, double* ion_out = nullptr) {
   using C = typename CT<Rl>::T;
-  constexpr int N = kCS * M;
+  constexpr int N = CS * M;
   const int tid = threadIdx.x;
   const Rl hR = (Rl)h, h2 = (Rl)(h / 2), h6 = (Rl)(h / 6);
   double nrm = 0.0;
@@ -304,7 +321,7 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
     }
   }
   __syncthreads();
-  cl_fft_inv<Rl, M>(c, cl);
+  cl_fft_inv<Rl, M, CS>(c, cl);
   const Rl invN = (Rl)(1.0 / N);
   const bool plasma = c.in->plasma;
   for (int t = tid; t < M; t += T1) {
@@ -314,32 +331,32 @@ __device__ __noinline__ double cl_nl_eval(ClCtx<Rl>& c, cg::cluster_group& cl, i
     c.line()[pad1(t)] = cscale(a, I);
   }
   __syncthreads();
-  cl_fft_fwd<Rl, M>(c, cl);
+  cl_fft_fwd<Rl, M, CS>(c, cl);
   for (int w = tid; w < M; w += T1) {
     const C p = c.line()[pad1(w)];
     const Rl gr = (Rl)c.G[w];
     out[w] = C{-gr * p.y, gr * p.x};     // i gamma U(w) P_NL(w)
   }
   __syncthreads();
-  if (plasma && cl_plasma<Rl, M>(c, cl, ion_out)) {
+  if (plasma && cl_plasma<Rl, M, CS>(c, cl, ion_out)) {
     __syncthreads();
-    cl_fft_fwd<Rl, M>(c, cl);
+    cl_fft_fwd<Rl, M, CS>(c, cl);
     for (int w = tid; w < M; w += T1) out[w] = cadd(out[w], c.line()[pad1(w)]);
     __syncthreads();
   }
-  return mode == IN_5 ? cl_sum(c, cl, nrm) : 0.0;
+  return mode == IN_5 ? cl_sum<Rl, CS>(c, cl, nrm) : 0.0;
 }
 
 // one erk43_step from (A, K1); the error of erk43ip_method.py:279-284
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ __noinline__ double cl_attempt(ClCtx<Rl>& c, cg::cluster_group& cl, double h, double* ion_cand) {
   using C = typename CT<Rl>::T;
-  constexpr int N = kCS * M;
+  constexpr int N = CS * M;
   const int tid = threadIdx.x;
-  cl_nl_eval<Rl, M>(c, cl, IN_2, h, c.O);
-  cl_nl_eval<Rl, M>(c, cl, IN_3, h, c.O);
-  cl_nl_eval<Rl, M>(c, cl, IN_4, h, c.A4P);
-  const double nrm = cl_nl_eval<Rl, M>(c, cl, IN_5, h, c.O, ion_cand);
+  cl_nl_eval<Rl, M, CS>(c, cl, IN_2, h, c.O);
+  cl_nl_eval<Rl, M, CS>(c, cl, IN_3, h, c.O);
+  cl_nl_eval<Rl, M, CS>(c, cl, IN_4, h, c.A4P);
+  const double nrm = cl_nl_eval<Rl, M, CS>(c, cl, IN_5, h, c.O, ion_cand);
   double acc = 0.0;
   const Rl h30 = (Rl)(h / 30);
   for (int w = tid; w < M; w += T1) {
@@ -353,7 +370,7 @@ __device__ __noinline__ double cl_attempt(ClCtx<Rl>& c, cg::cluster_group& cl, d
       acc += dx * dx + dy * dy;
     }
   }
-  double num = cl_sum(c, cl, acc);
+  double num = cl_sum<Rl, CS>(c, cl, acc);
   if (sizeof(Rl) != 8) num *= (h / 10.0) * (h / 10.0);
   double normA = sqrt(nrm / N);
   if (normA < 1e-20) normA = 1.0;
@@ -361,10 +378,10 @@ __device__ __noinline__ double cl_attempt(ClCtx<Rl>& c, cg::cluster_group& cl, d
 }
 
 // The whole propagation of instance i by this cluster (erk43ip_method.py:288-369).
-template <typename Rl, int M>
+template <typename Rl, int M, int CS>
 __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg::cluster_group& cl) {
   using C = typename CT<Rl>::T;
-  constexpr int N = kCS * M;
+  constexpr int N = CS * M;
   const int tid = threadIdx.x;
   const Inst1D& in = b.inst[i];
   ClCtx<Rl> c;
@@ -375,9 +392,9 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   c.starts = c.red + 64;
   c.slot = c.starts + T1;
   c.tw = reinterpret_cast<const C*>(b.tw) + (M - 1);
-  c.xtw = reinterpret_cast<const C*>(b.xtw) + cl_xtw_offset(M);
+  c.xtw = reinterpret_cast<const C*>(b.xtw) + cl_xtw_offset(M, CS);
   // per-cluster scratch: 7 stage arrays of N (CTA r's slice at r M), then D and G copies
-  const long long cid = blockIdx.x / kCS;
+  const long long cid = b.cl_off + blockIdx.x / CS;
   unsigned char* base = reinterpret_cast<unsigned char*>(b.cl_scratch) + cid * b.cl_scratch_bytes;
   C* sc = reinterpret_cast<C*>(base) + (long long)c.r * M;
   c.A = sc; c.K1 = sc + N; c.T = sc + 2 * N; c.O = sc + 3 * N;
@@ -386,7 +403,7 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   double* Gp = reinterpret_cast<double*>(reinterpret_cast<double2*>(reinterpret_cast<C*>(base) + 7LL * N) + N) +
                (long long)c.r * M;
   for (int j = tid; j < M; j += T1) {
-    const long long k = in.off + c.r + (long long)kCS * j;
+    const long long k = in.off + c.r + (long long)CS * j;
     Dp[j] = b.D[k];
     Gp[j] = b.G[k];
   }
@@ -397,11 +414,11 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   C* field = reinterpret_cast<C*>(b.field) + in.off + (long long)c.r * M;
   for (int t = tid; t < M; t += T1) c.line()[pad1(t)] = field[t];
   __syncthreads();
-  cl_fft_fwd<Rl, M>(c, cl);
+  cl_fft_fwd<Rl, M, CS>(c, cl);
   for (int w = tid; w < M; w += T1) c.A[w] = c.line()[pad1(w)];
   __syncthreads();
   double ion_peak = 0.0, ion_cand = 0.0;
-  cl_nl_eval<Rl, M>(c, cl, IN_A, 0.0, c.K1, &ion_peak);
+  cl_nl_eval<Rl, M, CS>(c, cl, IN_A, 0.0, c.K1, &ion_peak);
 
   // the adaptive loop of run_instance (every CTA takes the same decisions)
   const double L = in.L, tol = in.tol, max_step = in.max_step, min_step = in.min_step;
@@ -425,7 +442,7 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
     for (int k = 0; k < b.nsched; ++k) {
       const double hh = hs[k];
       ion_cand = 0.0;
-      err = cl_attempt<Rl, M>(c, cl, hh, &ion_cand);
+      err = cl_attempt<Rl, M, CS>(c, cl, hh, &ion_cand);
       attempts += 1;
       if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
       accept(hh);
@@ -434,7 +451,7 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   while (!b.hsched && z < L) {
     if (z + h > L) h = L - z;
     ion_cand = 0.0;
-    err = cl_attempt<Rl, M>(c, cl, h, &ion_cand);
+    err = cl_attempt<Rl, M, CS>(c, cl, h, &ion_cand);
     attempts += 1;
     if (!isfinite(h) || (!isfinite(err) && h <= min_step)) { status |= UPPE_STATUS_NONFINITE; break; }
     if (!isfinite(err)) {
@@ -451,7 +468,7 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
       h = fmax(h * fmax(factor, 0.1), min_step);
       if (h <= min_step) {   // forced step (:345-367)
         ion_cand = 0.0;
-        err = cl_attempt<Rl, M>(c, cl, h, &ion_cand);
+        err = cl_attempt<Rl, M, CS>(c, cl, h, &ion_cand);
         attempts += 1;
         status |= UPPE_STATUS_MIN_STEP;
         if (!isfinite(err)) { status |= UPPE_STATUS_NONFINITE; break; }
@@ -469,19 +486,19 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
   {
     const double dw = 6.283185307179586476925286766559 / (N * in.dt);
     for (int w = tid; w < M; w += T1) {
-      const int k = c.r + kCS * w;
+      const int k = c.r + CS * w;
       const C v = c.A[w];
       const double a2 = (double)v.x * v.x + (double)v.y * v.y;
       en += a2;
       const double wa = in.omega0 + dw * (k < (N + 1) / 2 ? k : k - N);
       if (wa > 0.0) ph += a2 / (1.054571817e-34 * wa);
     }
-    en = cl_sum(c, cl, en) * in.dt / N;
-    ph = cl_sum(c, cl, ph) * in.dt / N;
+    en = cl_sum<Rl, CS>(c, cl, en) * in.dt / N;
+    ph = cl_sum<Rl, CS>(c, cl, ph) * in.dt / N;
   }
   for (int w = tid; w < M; w += T1) c.line()[pad1(w)] = c.A[w];
   __syncthreads();
-  cl_fft_inv<Rl, M>(c, cl);
+  cl_fft_inv<Rl, M, CS>(c, cl);
   const Rl invN = (Rl)(1.0 / N);
   for (int t = tid; t < M; t += T1) field[t] = cscale(c.line()[pad1(t)], invN);
   if (lead) {
@@ -496,32 +513,42 @@ __device__ void cl_run_instance(const Batch1D& b, int i, unsigned char* smem, cg
 
 // Persistent cluster kernel: each cluster takes instances from the work queue
 // (longest expected first) and propagates them one at a time.
-template <typename Rl>
-__global__ void __cluster_dims__(kCS, 1, 1) __launch_bounds__(T1, 1) k_uppe1d_cl(Batch1D b) {
+template <typename Rl, int CS>
+__global__ void __cluster_dims__(CS, 1, 1) __launch_bounds__(T1, 1) k_uppe1d_cl(Batch1D b) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ int s_k;
   cg::cluster_group cl = cg::this_cluster();
-  mark_busy(b.busy, 0);
+  mark_busy(b.busy, 0, b.busy_off);
   for (;;) {
-    if (cl.block_rank() == 0 && threadIdx.x == 0) s_k = atomicAdd(b.counter, 1);
+    if (cl.block_rank() == 0 && threadIdx.x == 0) {
+      if (CS == 8 && b.nhead > 0) {
+        // the eight-CTA clusters of a mixed launch take the head of the queue (the
+        // costliest lines) and nothing else, so every line's cluster size, hence
+        // its result, is fixed by the plan
+        const int k = atomicAdd(b.counter_head, 1);
+        s_k = k < b.nhead ? k : b.ninst;
+      } else {
+        s_k = atomicAdd(b.counter, 1);
+      }
+    }
     cl.sync();
     const int k = *cl.map_shared_rank(&s_k, 0);
     cl.sync();
-    if (k >= b.ninst) { mark_busy(b.busy, 1); return; }
+    if (k >= b.ninst) { mark_busy(b.busy, 1, b.busy_off); return; }
     const int i = b.order[k];
     switch (b.inst[i].log2n) {
-      case 11: cl_run_instance<Rl, 512>(b, i, smem, cl); break;
-      case 12: cl_run_instance<Rl, 1024>(b, i, smem, cl); break;
-      case 13: cl_run_instance<Rl, 2048>(b, i, smem, cl); break;
-      case 14: cl_run_instance<Rl, 4096>(b, i, smem, cl); break;
+      case 11: cl_run_instance<Rl, 2048 / CS, CS>(b, i, smem, cl); break;
+      case 12: cl_run_instance<Rl, 4096 / CS, CS>(b, i, smem, cl); break;
+      case 13: cl_run_instance<Rl, 8192 / CS, CS>(b, i, smem, cl); break;
+      case 14: cl_run_instance<Rl, 16384 / CS, CS>(b, i, smem, cl); break;
       default: break;
     }
   }
 }
 
 // shared memory of the cluster kernel for lines up to nmax points
-template <typename Rl> inline size_t cl_smem(int nmax) {
-  const int M = nmax / kCS;
+template <typename Rl> inline size_t cl_smem(int nmax, int cs = kCS) {
+  const int M = nmax / cs;
   return 2 * sizeof(typename CT<Rl>::T) * (size_t)(M + M / 32) + sizeof(double) * (64 + T1 + 8);
 }
 // per-cluster scratch bytes for lines up to nmax points
@@ -530,7 +557,8 @@ template <typename Rl> inline size_t cl_scratch_bytes(int nmax) {
   return (b + 255) & ~(size_t)255;
 }
 
-template <typename Rl> cudaError_t launch_uppe1d_cl(const Batch1D& b, int nclusters, size_t smem, cudaStream_t s);
-template <typename Rl> int uppe1d_cl_max_clusters(size_t smem);
+template <typename Rl> cudaError_t launch_uppe1d_cl(const Batch1D& b, int nclusters, size_t smem, cudaStream_t s,
+                                                   int cs);
+template <typename Rl> int uppe1d_cl_max_clusters(size_t smem, int cs);
 
 }  // namespace uppe

@@ -94,14 +94,22 @@ struct Batch1D {
   void* cl_scratch;              // cluster kernel: per-cluster scratch
   long long cl_scratch_bytes;
   unsigned long long* busy;      // per CTA: globaltimer at start and at exit (or null)
+  // cluster kernel, eight-CTA launch next to a four-CTA one: its clusters take the
+  // queue positions [0, nhead) from counter_head (the four-CTA clusters start at
+  // nhead); cl_off and busy_off offset the cluster scratch index and the activity
+  // slots of a launch
+  int* counter_head;
+  int nhead;
+  int cl_off;
+  int busy_off;
 };
 
 // activity record of a persistent CTA (ns of the global timer)
-static __device__ __forceinline__ void mark_busy(unsigned long long* busy, int slot) {
+static __device__ __forceinline__ void mark_busy(unsigned long long* busy, int slot, int off = 0) {
   if (busy && threadIdx.x == 0) {
     unsigned long long t;
     asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    busy[2 * blockIdx.x + slot] = t;
+    busy[2 * (off + (int)blockIdx.x) + slot] = t;
   }
 }
 

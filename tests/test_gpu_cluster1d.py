@@ -1,13 +1,17 @@
-"""1D lines on four-CTA thread-block clusters (GPU).
+"""1D lines on thread-block clusters (GPU).
 
 A plan whose lines are all 2048..16384 points (no Raman, no history) with at
-least one of 8192 or more runs every line on a cluster of four CTAs sharing the
-line through distributed shared memory (uppe1d_cluster.cuh).  Checks: the
+least one of 8192 or more runs every line on a cluster of four CTAs (or eight;
+a batch of 16 or more lines with 16384-point ones runs its costliest lines on
+eight-CTA clusters next to four-CTA ones) sharing the line through distributed
+shared memory (uppe1d_cluster.cuh).  Checks: the
 reference-derived oracle in complex128 (attempt for attempt), the single-CTA
 kernel on the same batch (UPPE_1D_CLUSTER=0) with the plasma term, complex128 at
 16384 points (which only the cluster kernel holds), and the logged / replayed
 step sequence.
 """
+import os
+
 import numpy as np
 import pytest
 
@@ -151,5 +155,42 @@ def test_activity_record_of_the_persistent_launch(monkeypatch, cluster):
     _lib.check(bp._lib.uppe1d_last_activity(bp._plan, ctypes.byref(busy), ctypes.byref(span), _lib.stream_ptr()),
                'uppe1d_last_activity')
     assert 0.0 < busy.value <= 1.0 and span.value > 0.0
-    # four instances on a 148-SM GPU: at most 16 of the SMs can be busy
-    assert busy.value <= 16 / 148 + 1e-9
+    # four instances on a 148-SM GPU: at most 4 x (CTAs per cluster) of the SMs can be busy
+    ctas = 8 if os.environ.get('UPPE_CLUSTER_CTAS') == '8' else 4
+    assert busy.value <= 4 * ctas / 148 + 1e-9
+
+
+def test_mixed_launch_runs_each_line_as_one_of_the_two_cluster_sizes(monkeypatch):
+    """A batch of 16 or more lines with 16384-point ones runs its costliest lines on
+    eight-CTA clusters next to four-CTA clusters for the rest (two concurrent
+    launches; the eight-CTA clusters take the head of the cost-ordered queue).  The
+    costliest four lines' results are then bit for bit those of the forced
+    eight-CTA run and every other line's those of the forced four-CTA run."""
+    import torch
+    from project_b200.solver1d import BatchedPropagator
+    s = _argon(precision='single')
+    insts, fields = [], []
+    for k, Nt in enumerate([16384, 8192, 4096, 2048] * 5):
+        t = np.linspace(-1e-12, 1e-12, Nt)
+        inst = s.instance(t, 0.02, tol=1e-6)
+        inst['desc'].cost = float(Nt) * (1.0 + 0.01 * k)
+        insts.append(inst)
+        fields.append(_pulse(t, 40e-6 + 2e-6 * k))
+
+    def run(cs):
+        if cs:
+            monkeypatch.setenv('UPPE_CLUSTER_CTAS', cs)
+        else:
+            monkeypatch.delenv('UPPE_CLUSTER_CTAS', raising=False)
+        bp = BatchedPropagator(insts, precision='single')
+        finals, _, res = bp.run(fields)
+        assert all(r.status == 0 for r in res)
+        return finals
+
+    mixed, four, eight = run(''), run('4'), run('8')
+    costs = [i['desc'].cost for i in insts]
+    head = set(np.argsort(costs)[::-1][:4].tolist())      # four 16384-point lines
+    for k, (m, a, b) in enumerate(zip(mixed, four, eight)):
+        assert np.array_equal(m, b if k in head else a), k
+        assert rel_l2(a, b) < 1e-4        # the two cluster sizes agree to rounding
+    torch.cuda.synchronize()
