@@ -200,7 +200,10 @@ long long uppe1d_field_elems(const uppe1d_plan* plan);   /* sum Nt              
  * lines are all 2048..16384 points without Raman or history, one of them at least
  * 8192, runs each line on a cluster of four SMs sharing it through distributed
  * shared memory (no reference counterpart: the reference runs one line at a time
- * on the CPU).  UPPE_1D_CLUSTER=0 keeps one CTA per line where that can hold it. */
+ * on the CPU); a plan of 16 or more lines with 16384-point ones also runs its (up
+ * to four) costliest lines on eight-SM clusters, concurrently, on a stream of its
+ * own forked from and joined back into the caller's.  UPPE_1D_CLUSTER=0 keeps one
+ * CTA per line where that can hold it; UPPE_CLUSTER_CTAS=4 or 8 forces one size. */
 int uppe1d_uses_clusters(const uppe1d_plan* plan);
 /* SM occupancy of the plan's last propagation launch (no reference counterpart):
  * each persistent CTA records the global timer when it starts and when the work
