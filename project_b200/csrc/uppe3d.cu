@@ -390,12 +390,12 @@ k_space(SpaceArgs a) {
         const Rl h30 = (Rl)(h / 30);
         const C A3 = cadd(beta, cscale(cadd(cscale(a4, (Rl)2), cscale(a5, (Rl)3)), h30));
         const C dd = csub(A4, A3);
-        d = sqrt((double)dd.x * dd.x + (double)dd.y * dd.y);
+        d = (double)dd.x * dd.x + (double)dd.y * dd.y;
       } else {
         const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
-        d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+        d = dx * dx + dy * dy;
       }
-      red = (d > red || d != d) ? d : red;
+      red = (d > red || d != d) ? d : red;   // max of the squares (root taken once below)
       continue;
     }
     if (mode == YMID4) {
@@ -403,7 +403,7 @@ k_space(SpaceArgs a) {
       const C beta = opB[i];
       const C A4 = cadd(beta, cscale(a4, h6R));
       a4p[gi] = a4;
-      const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+      const double m = (double)A4.x * A4.x + (double)A4.y * A4.y;
       red = (m > red || m != m) ? m : red;
       s[idx(w, n)] = A4;
       continue;
@@ -445,7 +445,10 @@ k_space(SpaceArgs a) {
   }
   if (mode == YMID4 || mode == YFWD5) {
     red = warp_max<(NTHR < 32 ? NTHR : 32)>(red);
-    if ((tid & 31) == 0) atomic_max_nonneg(mode == YMID4 ? &st->red_norm : &st->red_diff, red);
+    // sqrt and the positive factor are monotone, so the root of the largest square
+    // is the largest root, bit for bit
+    const double rv = (mode == YMID4 || sizeof(Rl) == 8) ? sqrt(red) : (h / 10.0) * sqrt(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(mode == YMID4 ? &st->red_norm : &st->red_diff, rv);
     if (mode == YFWD5) return;
   }
   __syncthreads();
@@ -955,7 +958,7 @@ k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
       if constexpr (MODE == YFWD5) {
         const C a5 = s[e], a4 = oA;
         const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
-        const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+        const double d = dx * dx + dy * dy;   // max of the squares; root once per warp
         red = (d > red || d != d) ? d : red;
         continue;
       }
@@ -963,7 +966,7 @@ k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
         const C a4 = s[e];
         const C A4 = cadd(oB, cscale(a4, h6R));
         a4p[gi] = a4;
-        const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+        const double m = (double)A4.x * A4.x + (double)A4.y * A4.y;
         red = (m > red || m != m) ? m : red;
         s[e] = A4;
         continue;
@@ -1009,7 +1012,9 @@ k_ypass_tma(SpaceArgs a, const __grid_constant__ YMaps maps) {
   }
   if constexpr (MODE == YMID4 || MODE == YFWD5) {
     red = warp_max<32>(red);
-    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+    // the root of the largest square is the largest root (sqrt and h/10 > 0 are monotone)
+    const double rv = MODE == YMID4 ? sqrt(red) : (h / 10.0) * sqrt(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, rv);
   }
 }
 
@@ -1110,7 +1115,7 @@ k_ypass_rq(SpaceArgs a) {
     if constexpr (MODE == YFWD5) {
       const C a5 = v[i], a4 = oA;
       const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
-      const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+      const double d = dx * dx + dy * dy;   // max of the squares; root once per warp
       red = (d > red || d != d) ? d : red;
       continue;
     }
@@ -1118,7 +1123,7 @@ k_ypass_rq(SpaceArgs a) {
       const C a4 = v[i];
       const C A4 = cadd(oB, cscale(a4, h6R));
       a4p[gi] = a4;
-      const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+      const double m = (double)A4.x * A4.x + (double)A4.y * A4.y;
       red = (m > red || m != m) ? m : red;
       v[i] = A4;
       continue;
@@ -1155,7 +1160,9 @@ k_ypass_rq(SpaceArgs a) {
   }
   if constexpr (MODE == YMID4 || MODE == YFWD5) {
     red = warp_max<32>(red);
-    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+    // the root of the largest square is the largest root (sqrt and h/10 > 0 are monotone)
+    const double rv = MODE == YMID4 ? sqrt(red) : (h / 10.0) * sqrt(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, rv);
   }
   if constexpr (MODE != YFWD5) {
     fft_sq<R, +1, C, KW>(v, T, tw, j, w);
@@ -1317,7 +1324,7 @@ k_ypass_ring(SpaceArgs a, const __grid_constant__ YMaps maps) {
       if constexpr (MODE == YFWD5) {
         const C a5 = v[i], a4 = s1[sidx(i)];
         const double dx = (double)a4.x - (double)a5.x, dy = (double)a4.y - (double)a5.y;
-        const double d = (h / 10.0) * sqrt(dx * dx + dy * dy);
+        const double d = dx * dx + dy * dy;   // max of the squares; root once per warp
         red = (d > red || d != d) ? d : red;
         continue;
       }
@@ -1325,7 +1332,7 @@ k_ypass_ring(SpaceArgs a, const __grid_constant__ YMaps maps) {
         const C a4 = v[i];
         const C A4 = cadd(s1[sidx(i)], cscale(a4, h6R));
         a4p[gi] = a4;
-        const double m = sqrt((double)A4.x * A4.x + (double)A4.y * A4.y);
+        const double m = (double)A4.x * A4.x + (double)A4.y * A4.y;
         red = (m > red || m != m) ? m : red;
         v[i] = A4;
         continue;
@@ -1372,7 +1379,9 @@ k_ypass_ring(SpaceArgs a, const __grid_constant__ YMaps maps) {
   }
   if constexpr (MODE == YMID4 || MODE == YFWD5) {
     red = warp_max<32>(red);
-    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, red);
+    // the root of the largest square is the largest root (sqrt and h/10 > 0 are monotone)
+    const double rv = MODE == YMID4 ? sqrt(red) : (h / 10.0) * sqrt(red);
+    if ((tid & 31) == 0) atomic_max_nonneg(MODE == YMID4 ? &st->red_norm : &st->red_diff, rv);
   }
 }
 
