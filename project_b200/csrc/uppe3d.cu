@@ -4050,7 +4050,8 @@ k_rf_ypass(int mode, RfTables tb, RfBufs b, int Nw, int NR, const void* in, void
       const C E4 = cadd(cmul(cadd(v[gi], cscale(ts[gi], h6)), Ef), cscale(a, h6));
       const C El = cmul(el[gi], Ef);
       const double dx = (double)E4.x - El.x, dy = (double)E4.y - El.y;
-      const double d = sqrt(dx * dx + dy * dy), m = sqrt((double)E4.x * E4.x + (double)E4.y * E4.y);
+      // maxima of the squares; the roots are taken once per warp below
+      const double d = dx * dx + dy * dy, m = (double)E4.x * E4.x + (double)E4.y * E4.y;
       mdiff = (d > mdiff || d != d) ? d : mdiff;
       mnorm = (m > mnorm || m != m) ? m : mnorm;
       u = E4;
@@ -4059,8 +4060,8 @@ k_rf_ypass(int mode, RfTables tb, RfBufs b, int Nw, int NR, const void* in, void
   }
   if (mode == RS_4) {
     // blocks of fewer than 32 threads (Ny = 16) reduce over their own lanes only
-    mdiff = warp_max<(NTHR < 32 ? NTHR : 32)>(mdiff);
-    mnorm = warp_max<(NTHR < 32 ? NTHR : 32)>(mnorm);
+    mdiff = sqrt(warp_max<(NTHR < 32 ? NTHR : 32)>(mdiff));
+    mnorm = sqrt(warp_max<(NTHR < 32 ? NTHR : 32)>(mnorm));
     if ((threadIdx.x & 31) == 0) { atomic_max_nonneg(&red[0], mdiff); atomic_max_nonneg(&red[1], mnorm); }
   }
   __syncthreads();
