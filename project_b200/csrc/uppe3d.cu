@@ -1587,12 +1587,23 @@ k_tpass_w(TArgs a) {
 
   bool any_w = false;
   if (m.plasma) {
+    // the rates can be non-zero only where I >= I_zero (lut_eval returns 0 below):
+    // a cheap test of the whole line first, the table and the rate stores only for
+    // lines that pass it (the same rates and the same plasma_line decision)
+    bool cand = m.ava != 0.0;
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const C Ap = cscale(v[k], A_scaleR);
-      const float w = (float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
-      any_w |= (w != 0.f);
-      sW[wpad(lane + 32 * k)] = w;
+      cand |= !((double)(Ap.x * Ap.x + Ap.y * Ap.y) < a.tb.lut.I_zero);
+    }
+    if (__any_sync(0xffffffffu, cand)) {
+#pragma unroll
+      for (int k = 0; k < E; ++k) {
+        const C Ap = cscale(v[k], A_scaleR);
+        const float w = (float)lut_eval<Rl>(a.tb.lut, Ap.x * Ap.x + Ap.y * Ap.y);
+        any_w |= (w != 0.f);
+        sW[wpad(lane + 32 * k)] = w;
+      }
     }
   }
   const bool plasma_line = m.plasma && (__any_sync(0xffffffffu, any_w) || m.ava != 0.0);
