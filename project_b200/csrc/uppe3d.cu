@@ -1591,10 +1591,12 @@ k_tpass_w(TArgs a) {
     // a cheap test of the whole line first, the table and the rate stores only for
     // lines that pass it (the same rates and the same plasma_line decision)
     bool cand = m.ava != 0.0;
+    // in the field precision against I_zero rounded down: I < izr implies I < I_zero
+    const Rl izr = sizeof(Rl) == 8 ? (Rl)a.tb.lut.I_zero : (Rl)__double2float_rd(a.tb.lut.I_zero);
 #pragma unroll
     for (int k = 0; k < E; ++k) {
       const C Ap = cscale(v[k], A_scaleR);
-      cand |= !((double)(Ap.x * Ap.x + Ap.y * Ap.y) < a.tb.lut.I_zero);
+      cand |= !(Ap.x * Ap.x + Ap.y * Ap.y < izr);
     }
     if (__any_sync(0xffffffffu, cand)) {
 #pragma unroll
